@@ -1,0 +1,247 @@
+// D3Q27 lattice constants and the per-cell BGK arithmetic shared by every
+// kernel of the library (pull, in-place, L2-tile, FP64).
+//
+// Direction numbering follows the reference's VelSet3D<27>
+// (src/basic/velocity_set.hpp:189-255): d = (cx+1) + 3*(cy+1) + 9*(cz+1),
+// centre 13, opposite 26-d.  Populations are stored shifted, f_i - w_i, so
+// rho = 1 + sum(f).
+//
+// All arithmetic goes through explicit round-to-nearest intrinsics.  nvcc
+// never contracts them, so a*b + c stays two roundings exactly as in the
+// reference's routines compiled for the host with contraction disabled, and
+// only the reference's own fma() calls are fused.  Every kernel therefore
+// produces the same bits for the same cell, which is what makes the blocked
+// and in-place policies bitwise equal to the plain pull step.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace culbm {
+
+// Flag bits of the init-state flag.dat word,
+// reference src/simulator/single_dev_expt/local_config.hpp:12-22.
+constexpr uint32_t FLAG_LOAD = 1u << 0;
+constexpr uint32_t FLAG_EQU = 1u << 1;
+constexpr uint32_t FLAG_COLLIDE = 1u << 2;
+constexpr uint32_t FLAG_BOUNCE_BACK = 1u << 3;
+constexpr uint32_t FLAG_STORE = 1u << 4;
+constexpr uint32_t FLAG_DUMP_RHO = 1u << 27;
+constexpr uint32_t FLAG_DUMP_VX = 1u << 28;
+constexpr uint32_t FLAG_DUMP_VY = 1u << 29;
+constexpr uint32_t FLAG_DUMP_VZ = 1u << 30;
+constexpr uint32_t FLAG_CORRECT = 1u << 31;
+
+// Device-side compact operation byte: the five step bits keep their
+// positions; bit 5 marks a cell on the domain boundary (some neighbour is
+// outside), bit 6 marks a cell with at least one DUMP bit.
+constexpr uint8_t OP_LOAD = 1u << 0;
+constexpr uint8_t OP_EQU = 1u << 1;
+constexpr uint8_t OP_COLLIDE = 1u << 2;
+constexpr uint8_t OP_BB = 1u << 3;
+constexpr uint8_t OP_STORE = 1u << 4;
+constexpr uint8_t OP_EDGE = 1u << 5;
+constexpr uint8_t OP_SOFT = 1u << 6;   // soft-obstacle cell (adjoint model only)
+
+constexpr int Q = 27;
+
+__host__ __device__ constexpr int cx_of(int d) { return d % 3 - 1; }
+__host__ __device__ constexpr int cy_of(int d) { return (d / 3) % 3 - 1; }
+__host__ __device__ constexpr int cz_of(int d) { return d / 9 - 1; }
+__host__ __device__ constexpr int opp_of(int d) { return 26 - d; }
+
+// Lattice weights w_d (8/27 centre, 2/27 face, 1/54 edge, 1/216 corner).
+template <typename R>
+__host__ __device__ constexpr R weight(int d)
+{
+    const int k = (cx_of(d) != 0) + (cy_of(d) != 0) + (cz_of(d) != 0);
+    return k == 0 ? R(8) / R(27) : k == 1 ? R(2) / R(27) : k == 2 ? R(1) / R(54) : R(1) / R(216);
+}
+
+// Round-to-nearest arithmetic with contraction ruled out.
+template <typename R> struct Rn;
+template <> struct Rn<float> {
+    static __device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
+    static __device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
+    static __device__ __forceinline__ float sub(float a, float b) { return __fsub_rn(a, b); }
+    static __device__ __forceinline__ float fma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+    static __device__ __forceinline__ float div(float a, float b) { return __fdiv_rn(a, b); }
+};
+template <> struct Rn<double> {
+    static __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+    static __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+    static __device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+    static __device__ __forceinline__ double fma(double a, double b, double c) { return __fma_rn(a, b, c); }
+    static __device__ __forceinline__ double div(double a, double b) { return __ddiv_rn(a, b); }
+};
+
+// rho = 1 + sum f in the reference's pairing, u = (sum c f) * (1/rho).
+// Same operation order as bgk::detail::calcRhoU<27>,
+// reference src/lbm_core/device_function.hpp:439-463.
+template <typename R>
+__device__ __forceinline__ void moments(const R* f, R& rho, R& ux, R& uy, R& uz)
+{
+    using A = Rn<R>;
+    R s = A::add(R(1), f[0]);
+#pragma unroll
+    for (int k = 1; k < 27; k += 2) s = A::add(s, A::add(f[k], f[k + 1]));
+    rho = s;
+    const R inv = A::div(R(1), rho);
+    // x: pairs (3k+2, 3k); y: (9s+6+j, 9s+j); z: (18+j, j).
+    R x = A::sub(f[2], f[0]);
+#pragma unroll
+    for (int k = 1; k < 9; ++k) x = A::add(x, A::sub(f[3 * k + 2], f[3 * k]));
+    R y = A::sub(f[6], f[0]);
+#pragma unroll
+    for (int k = 1; k < 9; ++k) {
+        const int lo = 9 * (k / 3) + (k % 3);
+        y = A::add(y, A::sub(f[lo + 6], f[lo]));
+    }
+    R z = A::sub(f[18], f[0]);
+#pragma unroll
+    for (int k = 1; k < 9; ++k) z = A::add(z, A::sub(f[18 + k], f[k]));
+    ux = A::mul(x, inv);
+    uy = A::mul(y, inv);
+    uz = A::mul(z, inv);
+}
+
+// Shared intermediate terms of the shifted equilibrium.
+template <typename R>
+struct EquTerms {
+    R c3, h;
+    R v[13];   // 3u projected on the 13 direction classes (see vsel)
+    R rw[4], rm[4];
+};
+
+// Which projection and which weight class each direction uses, and whether
+// it enters with + or - sign, transcribed from the 27 expressions of
+// bgk::detail::calcEqu<27> (device_function.hpp:336-397).
+// v index: 0..2 = 3ux,3uy,3uz; 3..12 = v0..v9 of the reference.
+// weight class: 0 centre, 1 face (rhos), 2 edge (rhoe), 3 corner (rhoc).
+__host__ __device__ constexpr int equ_vsel(int d)
+{
+    constexpr int t[27] = {9, 5, 12, 4, 2, 7, 11, 8, 10,
+                           3, 1, 6, 0, 0, 0, 6, 1, 3,
+                           10, 8, 11, 7, 2, 4, 12, 5, 9};
+    return t[d];
+}
+__host__ __device__ constexpr bool equ_plus(int d)
+{
+    constexpr bool t[27] = {false, false, false, false, false, true, false, true, true,
+                            false, false, true, false, false, true, false, true, true,
+                            false, false, true, false, true, true, true, true, true};
+    return t[d];
+}
+__host__ __device__ constexpr int equ_wcls(int d)
+{
+    const int k = (cx_of(d) != 0) + (cy_of(d) != 0) + (cz_of(d) != 0);
+    return k;   // 0 centre, 1 face, 2 edge, 3 corner
+}
+
+template <typename R>
+__device__ __forceinline__ void equ_terms(R rho, R ux, R uy, R uz, EquTerms<R>& t)
+{
+    using A = Rn<R>;
+    const R WS = R(2) / R(27), WE = R(1) / R(54), WC = R(1) / R(216);
+    const R rhom1 = A::sub(rho, R(1));
+    t.c3 = A::mul(R(-3), A::add(A::add(A::mul(ux, ux), A::mul(uy, uy)), A::mul(uz, uz)));
+    t.h = R(0.5);
+    const R vx = A::mul(ux, R(3)), vy = A::mul(uy, R(3)), vz = A::mul(uz, R(3));
+    t.v[0] = vx;
+    t.v[1] = vy;
+    t.v[2] = vz;
+    t.v[3] = A::add(vx, vy);                    // v0
+    t.v[4] = A::add(vx, vz);                    // v1
+    t.v[5] = A::add(vy, vz);                    // v2
+    t.v[6] = A::sub(vx, vy);                    // v3
+    t.v[7] = A::sub(vx, vz);                    // v4
+    t.v[8] = A::sub(vy, vz);                    // v5
+    t.v[9] = A::add(A::add(vx, vy), vz);        // v6
+    t.v[10] = A::sub(A::add(vx, vy), vz);       // v7
+    t.v[11] = A::add(A::sub(vx, vy), vz);       // v8
+    t.v[12] = A::add(A::sub(vy, vx), vz);       // v9
+    t.rw[0] = rho;                              // centre uses rho directly
+    t.rw[1] = A::mul(WS, rho);
+    t.rw[2] = A::mul(WE, rho);
+    t.rw[3] = A::mul(WC, rho);
+    t.rm[0] = rhom1;
+    t.rm[1] = A::mul(WS, rhom1);
+    t.rm[2] = A::mul(WE, rhom1);
+    t.rm[3] = A::mul(WC, rhom1);
+}
+
+// feq_d - w_d for a non-centre direction: fma(rw, fma(1/2, fma(v, v, c3), +-v), rm).
+template <typename R>
+__device__ __forceinline__ R equ_dir(const EquTerms<R>& t, int d)
+{
+    using A = Rn<R>;
+    const R v = t.v[equ_vsel(d)];
+    const R sv = equ_plus(d) ? v : -v;
+    const int w = equ_wcls(d);
+    return A::fma(t.rw[w], A::fma(t.h, A::fma(v, v, t.c3), sv), t.rm[w]);
+}
+
+// Shifted equilibrium into f, bgk::detail::calcEqu<27> (device_function.hpp:305-398).
+template <typename R>
+__device__ __forceinline__ void equilibrium(R rho, R ux, R uy, R uz, R* f)
+{
+    using A = Rn<R>;
+    EquTerms<R> t;
+    equ_terms(rho, ux, uy, uz, t);
+#pragma unroll
+    for (int d = 0; d < 27; ++d) {
+        if (d == 13)
+            f[d] = A::mul(R(8) / R(27), A::fma(rho, A::mul(t.h, t.c3), t.rm[0]));
+        else
+            f[d] = equ_dir(t, d);
+    }
+}
+
+// BGK relaxation on shifted populations, bgk::detail::collision2<27>
+// (device_function.hpp:676-754): f <- invTau*feq + (1-invTau)*f, centre term
+// associated as (invTau*W0)*fma(rho, c3/2, rho-1).
+template <typename R>
+__device__ __forceinline__ void collide(R inv_tau, R* f)
+{
+    using A = Rn<R>;
+    R rho, ux, uy, uz;
+    moments(f, rho, ux, uy, uz);
+    EquTerms<R> t;
+    equ_terms(rho, ux, uy, uz, t);
+    const R om = A::sub(R(1), inv_tau);
+#pragma unroll
+    for (int d = 0; d < 27; ++d) {
+        R e;
+        if (d == 13)
+            e = A::mul(A::mul(inv_tau, R(8) / R(27)), A::fma(rho, A::mul(t.h, t.c3), t.rm[0]));
+        else
+            e = A::mul(inv_tau, equ_dir(t, d));
+        f[d] = A::add(e, A::mul(om, f[d]));
+    }
+}
+
+// Boundary and collision sequence of one cell after its populations were
+// loaded: EQU overwrite, full-way bounce-back swap d <-> 26-d, BGK.
+// Reference src/simulator/single_dev_expt/kernel.cu:2571-2600.
+template <typename R>
+__device__ __forceinline__ void cell_update(uint8_t op, R inv_tau, const float* __restrict__ rho,
+                                            const float* __restrict__ vx, const float* __restrict__ vy,
+                                            const float* __restrict__ vz, int64_t i, R* f)
+{
+    if (op & OP_EQU) {
+        equilibrium<R>(R(rho[i]), R(vx[i]), R(vy[i]), R(vz[i]), f);
+    }
+    if (op & OP_BB) {
+#pragma unroll
+        for (int d = 0; d < 13; ++d) {
+            const R tmp = f[d];
+            f[d] = f[26 - d];
+            f[26 - d] = tmp;
+        }
+    }
+    if (op & OP_COLLIDE) {
+        collide<R>(inv_tau, f);
+    }
+}
+
+}  // namespace culbm

@@ -1,0 +1,746 @@
+// Host runtime behind include/culbm.h: configuration checks, device
+// allocation, init-state loading, step dispatch, dumps and reductions.
+//
+// Replaces the reference's Simulator / Simulator::Data
+// (src/simulator/single_dev_expt/simulator_expt_platform.cu) minus argv
+// parsing, which single_dev_expt_main does on top of this ABI.
+#include <atomic>
+#include <cerrno>
+#include <cstdio>
+#include <cstring>
+#include <filesystem>
+#include <fstream>
+#include <string>
+#include <vector>
+
+#include "sim_internal.cuh"
+
+namespace culbm {
+
+namespace {
+thread_local std::string t_last_error;
+std::atomic<int> g_inject_skip{0};
+std::atomic<int> g_inject_code{0};
+}  // namespace
+
+void set_last_error(const std::string& msg) { t_last_error = msg; }
+
+culbm_status fail(culbm_status s, const std::string& msg)
+{
+    t_last_error = msg;
+    return s;
+}
+
+cudaError_t injection_gate()
+{
+    const int code = g_inject_code.load();
+    if (code == 0) return cudaSuccess;
+    const int left = g_inject_skip.fetch_sub(1);
+    if (left > 0) return cudaSuccess;
+    int expected = code;
+    if (g_inject_code.compare_exchange_strong(expected, 0)) return static_cast<cudaError_t>(code);
+    return cudaSuccess;
+}
+
+culbm_status cuda_fail(cudaError_t e, const char* what, const char* file, int line)
+{
+    char buf[512];
+    std::snprintf(buf, sizeof(buf), "CUDA error %d (%s: %s) in %s at %s:%d", static_cast<int>(e),
+                  cudaGetErrorName(e), cudaGetErrorString(e), what, file, line);
+    t_last_error = buf;
+    return e == cudaErrorMemoryAllocation ? CULBM_ERR_OUT_OF_MEMORY : CULBM_ERR_CUDA;
+}
+
+// ------------------------------------------------------------ utilities ---
+
+template <typename S>
+struct Tag {
+    using type = S;
+};
+
+// Calls f(Tag<S>{}) for the storage type of sim.
+template <class F>
+culbm_status with_storage(const culbm_sim* s, F&& f)
+{
+    switch (s->cfg.storage) {
+        case CULBM_STORAGE_F32: return f(Tag<float>{});
+        case CULBM_STORAGE_F16: return f(Tag<__half>{});
+        case CULBM_STORAGE_BF16: return f(Tag<__nv_bfloat16>{});
+        case CULBM_STORAGE_F64: return f(Tag<double>{});
+        default: return fail(CULBM_ERR_INVALID_ARGUMENT, "unknown storage format");
+    }
+}
+
+template <typename S>
+StepArgs<S, typename ArithOf<S>::type> make_args(const culbm_sim* s, int src, int dst)
+{
+    using R = typename ArithOf<S>::type;
+    StepArgs<S, R> a{};
+    a.dom = s->dom;
+    a.ops = s->d_ops;
+    a.rho = s->d_mac[0];
+    a.vx = s->d_mac[1];
+    a.vy = s->d_mac[2];
+    a.vz = s->d_mac[3];
+    a.inv_tau = static_cast<R>(s->cfg.inv_tau);
+    S* b0 = static_cast<S*>(s->d_pop[src]);
+    S* b1 = static_cast<S*>(s->d_pop[dst]);
+    for (int d = 0; d < 27; ++d) {
+        a.src.p[d] = b0 + static_cast<long long>(d) * s->n;
+        a.dst.p[d] = b1 + static_cast<long long>(d) * s->n;
+    }
+    a.edge = static_cast<S*>(s->d_edge);
+    a.el = s->el;
+    return a;
+}
+
+// Layout of the newest state and the buffer holding it.
+int current_layout(const culbm_sim* s)
+{
+    if (s->cfg.stream_policy == CULBM_STREAM_INPLACE && !is_blocked(s->cfg))
+        return s->aa_phase == 0 ? LAYOUT_AA_A : LAYOUT_AA_B;
+    return LAYOUT_PULL;
+}
+
+size_t storage_bytes(int storage)
+{
+    switch (storage) {
+        case CULBM_STORAGE_F16:
+        case CULBM_STORAGE_BF16: return 2;
+        case CULBM_STORAGE_F64: return 8;
+        default: return 4;
+    }
+}
+
+culbm_status dev_alloc(culbm_sim* s, void** p, size_t bytes, const char* what)
+{
+    cudaError_t e = injection_gate();
+    if (e == cudaSuccess) e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        cudaGetLastError();
+        char buf[256];
+        std::snprintf(buf, sizeof(buf), "device allocation of %zu bytes for %s failed: %s", bytes, what,
+                      cudaGetErrorString(e));
+        return fail(e == cudaErrorMemoryAllocation ? CULBM_ERR_OUT_OF_MEMORY : CULBM_ERR_CUDA, buf);
+    }
+    s->device_bytes += bytes;
+    return CULBM_OK;
+}
+
+// Builds the compact op bytes from the flag words: step bits plus OP_EDGE on
+// the domain boundary.
+__global__ void k_build_ops(Domain D, const uint32_t* flag, uint8_t* ops)
+{
+    const CellCoord c = cell_of_thread(D);
+    if (!c.valid) return;
+    const uint32_t fl = flag[c.i];
+    uint8_t op = static_cast<uint8_t>(fl & 0x1Fu);
+    if (c.x == 0 || c.x == D.nx - 1 || c.y == 0 || c.y == D.ny - 1 || c.z == 0 || c.z == D.nz - 1) op |= OP_EDGE;
+    ops[c.i] = op;
+}
+
+__global__ void k_fill_u32(uint32_t* p, long long n, uint32_t v)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        p[i] = v;
+}
+
+__global__ void k_fill_f32(float* p, long long n, float v)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        p[i] = v;
+}
+
+// FP64 mass/momentum partial sums, one set of 4 per block, fixed order.
+template <int LAYOUT, typename S, typename R>
+__global__ void __launch_bounds__(256) k_mass_momentum(const __grid_constant__ StepArgs<S, R> a, double* partial)
+{
+    const Domain& D = a.dom;
+    double acc[4] = {0, 0, 0, 0};
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < D.n; t += (long long)gridDim.x * blockDim.x) {
+        const int i = static_cast<int>(t);
+        const uint8_t op = a.ops[i];
+        if ((op & (OP_LOAD | OP_EQU)) == 0) continue;
+        const int x = i % D.nx, y = (i / D.nx) % D.ny, z = i / D.nxy;
+        R f[27];
+        load_pulled<LAYOUT>(a, x, y, z, i, (op & OP_EDGE) != 0, f);
+        double r = 1.0, mx = 0, my = 0, mz = 0;
+        for (int d = 0; d < 27; ++d) {
+            const double v = static_cast<double>(f[d]);
+            r += v;
+            mx += cx_of(d) * v;
+            my += cy_of(d) * v;
+            mz += cz_of(d) * v;
+        }
+        acc[0] += r;
+        acc[1] += mx;
+        acc[2] += my;
+        acc[3] += mz;
+    }
+    __shared__ double sh[4][256];
+    for (int k = 0; k < 4; ++k) sh[k][threadIdx.x] = acc[k];
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if (threadIdx.x < w)
+            for (int k = 0; k < 4; ++k) sh[k][threadIdx.x] += sh[k][threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int k = 0; k < 4; ++k) partial[4 * blockIdx.x + k] = sh[k][0];
+}
+
+__global__ void k_sum_partials(const double* partial, int nblocks, double* out)
+{
+    if (threadIdx.x < 4) {
+        double s = 0;
+        for (int b = 0; b < nblocks; ++b) s += partial[4 * b + threadIdx.x];
+        out[threadIdx.x] = s;
+    }
+}
+
+constexpr uint32_t kDefaultFlag =
+    FLAG_LOAD | FLAG_COLLIDE | FLAG_STORE | FLAG_DUMP_RHO | FLAG_DUMP_VX | FLAG_DUMP_VY | FLAG_DUMP_VZ;
+
+// Rest-equilibrium fill of the population state in its start layout.
+template <typename S>
+culbm_status fill_rest(culbm_sim* s)
+{
+    using R = typename ArithOf<S>::type;
+    const dim3 g = cell_grid(s->dom), b = cell_block();
+    for (int k = 0; k < s->npop; ++k) {
+        auto a = make_args<S>(s, k, k);
+        if (s->cfg.stream_policy == CULBM_STREAM_INPLACE && !is_blocked(s->cfg))
+            k_fill_equilibrium<LAYOUT_AA_A, S, R><<<g, b, 0, s->stream>>>(a, R(1), R(0), R(0), R(0));
+        else
+            k_fill_equilibrium<LAYOUT_PULL, S, R><<<g, b, 0, s->stream>>>(a, R(1), R(0), R(0), R(0));
+        CULBM_CUDA(cudaGetLastError());
+    }
+    s->cur = 0;
+    s->aa_phase = 0;
+    return CULBM_OK;
+}
+
+template <typename S>
+culbm_status plain_steps(culbm_sim* s, uint32_t nsteps)
+{
+    using R = typename ArithOf<S>::type;
+    const dim3 g = cell_grid(s->dom), b = cell_block();
+    for (uint32_t k = 0; k < nsteps; ++k) {
+        if (s->cfg.stream_policy == CULBM_STREAM_PULL) {
+            auto a = make_args<S>(s, s->cur, 1 - s->cur);
+            k_pull_step<S, R><<<g, b, 0, s->stream>>>(a);
+            CULBM_CUDA(cudaGetLastError());
+            s->cur ^= 1;
+        } else {
+            auto a = make_args<S>(s, 0, 0);
+            if (s->aa_phase == 0)
+                k_aa_odd<S, R><<<g, b, 0, s->stream>>>(a);
+            else
+                k_aa_even<S, R><<<g, b, 0, s->stream>>>(a);
+            CULBM_CUDA(cudaGetLastError());
+            s->aa_phase ^= 1;
+        }
+        s->launches += 1;
+    }
+    return CULBM_OK;
+}
+
+culbm_status check_sim(culbm_sim* s, bool need_loaded = false)
+{
+    if (s == nullptr) return fail(CULBM_ERR_INVALID_ARGUMENT, "culbm_sim is NULL");
+    if (need_loaded && !s->loaded) return fail(CULBM_ERR_STATE, "no state loaded");
+    CULBM_CUDA(cudaSetDevice(s->dev));
+    return CULBM_OK;
+}
+
+culbm_status validate_config(const culbm_config& c)
+{
+    for (int k = 0; k < 3; ++k) {
+        if (c.domain_dim[k] == 0) return fail(CULBM_ERR_INVALID_ARGUMENT, "domainDim must be positive");
+        if (c.block_dim[k] == 0 || c.grid_dim[k] == 0)
+            return fail(CULBM_ERR_INVALID_ARGUMENT, "blockDim and gridDim must be positive");
+    }
+    const unsigned long long n = 1ull * c.domain_dim[0] * c.domain_dim[1] * c.domain_dim[2];
+    if (n >= (1ull << 31)) return fail(CULBM_ERR_INVALID_ARGUMENT, "domain has 2^31 cells or more");
+    if (c.domain_dim[2] > 65535) return fail(CULBM_ERR_INVALID_ARGUMENT, "domainDim z above 65535");
+    if (c.vel_set != 0) return fail(CULBM_ERR_INVALID_ARGUMENT, "Unsupport Velocity Set: " + std::to_string(c.vel_set));
+    if (c.stream_policy != CULBM_STREAM_PULL && c.stream_policy != CULBM_STREAM_INPLACE)
+        return fail(CULBM_ERR_INVALID_ARGUMENT, "streamPolicy must be 0 or 1");
+    if (c.opt_policy < 0 || c.opt_policy > 3) return fail(CULBM_ERR_INVALID_ARGUMENT, "optPolicy must be 0..3");
+    if (c.storage < 0 || c.storage > 3) return fail(CULBM_ERR_INVALID_ARGUMENT, "storage must be 0..3");
+    if (!(c.inv_tau > 0.0f && c.inv_tau < 2.0f))
+        return fail(CULBM_ERR_INVALID_ARGUMENT, "invTau must lie in (0, 2)");
+    // The reference rejects the ring buffer outside in-place dynamic L2
+    // blocking (simulator_expt_platform.cu:365-368).
+    if (c.use_ring_ddf_buf && !(c.stream_policy == CULBM_STREAM_INPLACE && c.opt_policy == CULBM_OPT_DYNAMIC_L2))
+        return fail(CULBM_ERR_INVALID_ARGUMENT, "--useRingDDFBuf is unimplemented unless --streamPolicy 1 --optPolicy 3.");
+    // The reference's plain pull launches one thread per cell with the user's
+    // grid and requires it to cover the domain exactly (simulator_expt_platform.cu:962-967).
+    if (c.stream_policy == CULBM_STREAM_PULL && c.opt_policy == CULBM_OPT_NONE)
+        for (int k = 0; k < 3; ++k)
+            if (1ull * c.block_dim[k] * c.grid_dim[k] != c.domain_dim[k])
+                return fail(CULBM_ERR_INVALID_ARGUMENT, "Dimension of domain doesn't match computation grid!");
+    return CULBM_OK;
+}
+
+void release(culbm_sim* s)
+{
+    if (s == nullptr) return;
+    cudaSetDevice(s->dev);
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    tiles_destroy(s);
+    cudaFree(s->d_flag);
+    cudaFree(s->d_ops);
+    for (auto& p : s->d_mac) cudaFree(p);
+    for (auto& p : s->d_pop) cudaFree(p);
+    cudaFree(s->d_edge);
+    cudaFree(s->d_red);
+    if (s->ev0) cudaEventDestroy(s->ev0);
+    if (s->ev1) cudaEventDestroy(s->ev1);
+    if (s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+}
+
+culbm_status upload_state(culbm_sim* s, const uint32_t* flag, const float* const mac[4])
+{
+    const long long n = s->n;
+    const dim3 g1(1184), b1(256);
+    if (flag != nullptr) {
+        CULBM_CUDA(cudaMemcpyAsync(s->d_flag, flag, n * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream));
+    } else {
+        k_fill_u32<<<g1, b1, 0, s->stream>>>(s->d_flag, n, kDefaultFlag);
+        CULBM_CUDA(cudaGetLastError());
+    }
+    const float dflt[4] = {1.0f, 0.0f, 0.0f, 0.0f};
+    for (int k = 0; k < 4; ++k) {
+        if (mac[k] != nullptr) {
+            CULBM_CUDA(cudaMemcpyAsync(s->d_mac[k], mac[k], n * sizeof(float), cudaMemcpyHostToDevice, s->stream));
+        } else {
+            k_fill_f32<<<g1, b1, 0, s->stream>>>(s->d_mac[k], n, dflt[k]);
+            CULBM_CUDA(cudaGetLastError());
+        }
+    }
+    k_build_ops<<<cell_grid(s->dom), cell_block(), 0, s->stream>>>(s->dom, s->d_flag, s->d_ops);
+    CULBM_CUDA(cudaGetLastError());
+    if (is_blocked(s->cfg)) {
+        std::vector<uint32_t> host;
+        const uint32_t* hf = flag;
+        if (hf == nullptr) {
+            host.assign(static_cast<size_t>(n), kDefaultFlag);
+            hf = host.data();
+        }
+        CULBM_TRY(tiles_upload_flags(s, hf));
+    }
+    CULBM_TRY(with_storage(s, [&](auto tag) { return fill_rest<typename decltype(tag)::type>(s); }));
+    s->step = 0;
+    s->loaded = true;
+    return CULBM_OK;
+}
+
+bool read_exact(const std::string& path, void* dst, size_t bytes, bool* present, std::string* err)
+{
+    std::ifstream f(path, std::ios::binary);
+    *present = static_cast<bool>(f);
+    if (!f) return false;
+    f.read(static_cast<char*>(dst), static_cast<std::streamsize>(bytes));
+    if (static_cast<size_t>(f.gcount()) != bytes) {
+        *err = "File: " + path + " holds " + std::to_string(f.gcount()) + " bytes, expected " + std::to_string(bytes);
+        return false;
+    }
+    return true;
+}
+
+}  // namespace culbm
+
+using namespace culbm;
+
+extern "C" {
+
+culbm_status culbm_config_init(culbm_config* cfg)
+{
+    if (cfg == nullptr) return fail(CULBM_ERR_INVALID_ARGUMENT, "cfg is NULL");
+    std::memset(cfg, 0, sizeof(*cfg));
+    cfg->dev_id = 0;
+    cfg->block_dim[0] = 32;
+    cfg->block_dim[1] = 16;
+    cfg->block_dim[2] = 2;
+    cfg->grid_dim[0] = 2;
+    cfg->grid_dim[1] = 3;
+    cfg->grid_dim[2] = 19;
+    cfg->domain_dim[0] = cfg->domain_dim[1] = cfg->domain_dim[2] = 256;
+    cfg->inner_loop = 5;
+    cfg->stream_policy = CULBM_STREAM_PULL;
+    cfg->opt_policy = CULBM_OPT_NONE;
+    cfg->vel_set = 0;
+    cfg->inv_tau = 0.5f;
+    cfg->use_ring_ddf_buf = 0;
+    cfg->storage = CULBM_STORAGE_F32;
+    cfg->persist_l2 = 1;
+    cfg->cache_hints = 1;
+    cfg->use_graphs = 1;
+    return CULBM_OK;
+}
+
+culbm_status culbm_create(const culbm_config* cfg, culbm_sim** out)
+{
+    if (cfg == nullptr || out == nullptr) return fail(CULBM_ERR_INVALID_ARGUMENT, "cfg or out is NULL");
+    *out = nullptr;
+    CULBM_TRY(validate_config(*cfg));
+    culbm_sim* s = new culbm_sim();
+    s->cfg = *cfg;
+    s->dev = cfg->dev_id;
+    s->dom.nx = static_cast<int>(cfg->domain_dim[0]);
+    s->dom.ny = static_cast<int>(cfg->domain_dim[1]);
+    s->dom.nz = static_cast<int>(cfg->domain_dim[2]);
+    s->dom.nxy = s->dom.nx * s->dom.ny;
+    s->n = 1ll * s->dom.nxy * s->dom.nz;
+    s->dom.n = static_cast<int>(s->n);
+    s->esize = storage_bytes(cfg->storage);
+
+    auto body = [&]() -> culbm_status {
+        CULBM_CUDA(cudaSetDevice(s->dev));
+        CULBM_CUDA(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+        CULBM_CUDA(cudaEventCreate(&s->ev0));
+        CULBM_CUDA(cudaEventCreate(&s->ev1));
+        const long long n = s->n;
+        const bool blocked = is_blocked(s->cfg);
+        const bool inplace = s->cfg.stream_policy == CULBM_STREAM_INPLACE && !blocked;
+        s->npop = (inplace || (blocked && s->cfg.use_ring_ddf_buf)) ? 1 : 2;
+
+        // Capacity check before allocating: populations dominate.
+        size_t free_b = 0, total_b = 0;
+        CULBM_CUDA(cudaMemGetInfo(&free_b, &total_b));
+        const double need = static_cast<double>(s->npop) * 27.0 * n * s->esize + 9.0 * n;
+        if (need > static_cast<double>(free_b))
+            return fail(CULBM_ERR_OUT_OF_MEMORY, "domain needs " + std::to_string(need / 1e9) + " GB, " +
+                                                     std::to_string(free_b / 1e9) + " GB free on the device");
+
+        CULBM_TRY(dev_alloc(s, reinterpret_cast<void**>(&s->d_flag), n * sizeof(uint32_t), "flags"));
+        CULBM_TRY(dev_alloc(s, reinterpret_cast<void**>(&s->d_ops), n, "op bytes"));
+        for (int k = 0; k < 4; ++k)
+            CULBM_TRY(dev_alloc(s, reinterpret_cast<void**>(&s->d_mac[k]), n * sizeof(float), "macroscopic buffer"));
+        if (!blocked || !s->cfg.use_ring_ddf_buf) {
+            for (int k = 0; k < s->npop; ++k)
+                CULBM_TRY(dev_alloc(s, &s->d_pop[k], 27ull * n * s->esize, "populations"));
+        }
+        if (inplace) {
+            const long long fx = 9ll * s->dom.ny * s->dom.nz, fy = 9ll * s->dom.nx * s->dom.nz,
+                            fz = 9ll * s->dom.nx * s->dom.ny;
+            s->el.off[0] = 0;
+            s->el.off[1] = fx;
+            s->el.off[2] = 2 * fx;
+            s->el.off[3] = 2 * fx + fy;
+            s->el.off[4] = 2 * fx + 2 * fy;
+            s->el.off[5] = 2 * fx + 2 * fy + fz;
+            s->edge_elems = 2 * (fx + fy + fz);
+            CULBM_TRY(dev_alloc(s, &s->d_edge, s->edge_elems * s->esize, "edge buffer"));
+        }
+        s->red_blocks = 592;
+        CULBM_TRY(dev_alloc(s, reinterpret_cast<void**>(&s->d_red), (4ull * s->red_blocks + 4) * sizeof(double),
+                            "reduction scratch"));
+        if (blocked) CULBM_TRY(tiles_create(s));
+        const float* none[4] = {nullptr, nullptr, nullptr, nullptr};
+        CULBM_TRY(upload_state(s, nullptr, none));
+        s->loaded = false;   // defaults in place; a load call is still expected
+        CULBM_CUDA(cudaStreamSynchronize(s->stream));
+        return CULBM_OK;
+    };
+    const culbm_status st = body();
+    if (st != CULBM_OK) {
+        const std::string msg = t_last_error;
+        release(s);
+        cudaGetLastError();
+        set_last_error(msg);
+        return st;
+    }
+    s->loaded = true;
+    *out = s;
+    return CULBM_OK;
+}
+
+culbm_status culbm_destroy(culbm_sim* sim)
+{
+    if (sim == nullptr) return CULBM_OK;
+    release(sim);
+    return CULBM_OK;
+}
+
+culbm_status culbm_load_state(culbm_sim* sim, const uint32_t* flag, const float* rho, const float* vx,
+                              const float* vy, const float* vz)
+{
+    CULBM_TRY(check_sim(sim));
+    const float* mac[4] = {rho, vx, vy, vz};
+    CULBM_TRY(upload_state(sim, flag, mac));
+    CULBM_CUDA(cudaStreamSynchronize(sim->stream));
+    return CULBM_OK;
+}
+
+culbm_status culbm_load_state_folder(culbm_sim* sim, const char* folder, uint32_t* loaded_mask)
+{
+    CULBM_TRY(check_sim(sim));
+    if (loaded_mask) *loaded_mask = 0;
+    if (folder == nullptr || folder[0] == '\0') return culbm_load_state(sim, nullptr, nullptr, nullptr, nullptr, nullptr);
+    const std::string dir(folder);
+    const size_t n = static_cast<size_t>(sim->n);
+    std::vector<uint32_t> flag(n);
+    bool present = false;
+    std::string err;
+    if (!read_exact(dir + "/flag.dat", flag.data(), n * 4, &present, &err)) {
+        if (!present) return fail(CULBM_ERR_IO, "File: " + dir + "/flag.dat doesn't exist!");
+        return fail(CULBM_ERR_IO, err);
+    }
+    uint32_t mask = 1;
+    std::vector<float> mac[4];
+    const char* names[4] = {"rho", "vx", "vy", "vz"};
+    const float* ptr[4] = {nullptr, nullptr, nullptr, nullptr};
+    for (int k = 0; k < 4; ++k) {
+        mac[k].resize(n);
+        if (read_exact(dir + "/" + names[k] + ".dat", mac[k].data(), n * 4, &present, &err)) {
+            ptr[k] = mac[k].data();
+            mask |= 1u << (k + 1);
+        } else if (present) {
+            return fail(CULBM_ERR_IO, err);
+        }
+    }
+    CULBM_TRY(culbm_load_state(sim, flag.data(), ptr[0], ptr[1], ptr[2], ptr[3]));
+    if (loaded_mask) *loaded_mask = mask;
+    return CULBM_OK;
+}
+
+culbm_status culbm_step(culbm_sim* sim, uint32_t nsteps)
+{
+    CULBM_TRY(check_sim(sim, true));
+    if (nsteps == 0) return CULBM_OK;
+    if (is_blocked(sim->cfg)) {
+        CULBM_TRY(tiles_step(sim, nsteps));
+    } else {
+        CULBM_TRY(with_storage(sim, [&](auto tag) { return plain_steps<typename decltype(tag)::type>(sim, nsteps); }));
+    }
+    sim->step += nsteps;
+    sim->launched_steps += nsteps;
+    return CULBM_OK;
+}
+
+culbm_status culbm_step_timed(culbm_sim* sim, uint32_t nsteps, float* elapsed_ms)
+{
+    CULBM_TRY(check_sim(sim, true));
+    CULBM_CUDA(cudaEventRecord(sim->ev0, sim->stream));
+    CULBM_TRY(culbm_step(sim, nsteps));
+    CULBM_CUDA(cudaEventRecord(sim->ev1, sim->stream));
+    CULBM_CUDA(cudaEventSynchronize(sim->ev1));
+    float ms = 0.0f;
+    CULBM_CUDA(cudaEventElapsedTime(&ms, sim->ev0, sim->ev1));
+    if (elapsed_ms) *elapsed_ms = ms;
+    return CULBM_OK;
+}
+
+culbm_status culbm_synchronize(culbm_sim* sim)
+{
+    CULBM_TRY(check_sim(sim));
+    CULBM_CUDA(cudaStreamSynchronize(sim->stream));
+    return CULBM_OK;
+}
+
+culbm_status culbm_moments(culbm_sim* sim)
+{
+    CULBM_TRY(check_sim(sim, true));
+    const int layout = current_layout(sim);
+    return with_storage(sim, [&](auto tag) -> culbm_status {
+        using S = typename decltype(tag)::type;
+        using R = typename ArithOf<S>::type;
+        auto a = make_args<S>(sim, sim->cur, sim->cur);
+        const dim3 g = cell_grid(sim->dom), b = cell_block();
+        float* const* m = sim->d_mac;
+        if (layout == LAYOUT_PULL)
+            k_moments<LAYOUT_PULL, S, R><<<g, b, 0, sim->stream>>>(a, sim->d_flag, m[0], m[1], m[2], m[3]);
+        else if (layout == LAYOUT_AA_A)
+            k_moments<LAYOUT_AA_A, S, R><<<g, b, 0, sim->stream>>>(a, sim->d_flag, m[0], m[1], m[2], m[3]);
+        else
+            k_moments<LAYOUT_AA_B, S, R><<<g, b, 0, sim->stream>>>(a, sim->d_flag, m[0], m[1], m[2], m[3]);
+        CULBM_CUDA(cudaGetLastError());
+        return CULBM_OK;
+    });
+}
+
+culbm_status culbm_get_field(culbm_sim* sim, culbm_field field, float* host_out)
+{
+    CULBM_TRY(check_sim(sim));
+    if (field < 0 || field > 3 || host_out == nullptr) return fail(CULBM_ERR_INVALID_ARGUMENT, "bad field or NULL output");
+    CULBM_CUDA(cudaMemcpyAsync(host_out, sim->d_mac[field], sim->n * sizeof(float), cudaMemcpyDeviceToHost, sim->stream));
+    CULBM_CUDA(cudaStreamSynchronize(sim->stream));
+    return CULBM_OK;
+}
+
+culbm_status culbm_dump(culbm_sim* sim, const char* folder, uint32_t field_mask)
+{
+    CULBM_TRY(check_sim(sim));
+    if (folder == nullptr) return fail(CULBM_ERR_INVALID_ARGUMENT, "folder is NULL");
+    std::error_code ec;
+    std::filesystem::create_directories(folder, ec);
+    if (ec) return fail(CULBM_ERR_IO, std::string("cannot create dump folder ") + folder + ": " + ec.message());
+    if ((field_mask & 0xFu) == 0) return CULBM_OK;
+    std::vector<float> host(static_cast<size_t>(sim->n));
+    const char* names[4] = {"rho", "vx", "vy", "vz"};
+    for (int k = 0; k < 4; ++k) {
+        if (!(field_mask & (1u << k))) continue;
+        const std::string path = std::string(folder) + "/" + names[k] + "_" + std::to_string(sim->step) + ".dat";
+        std::ofstream f(path, std::ios::binary);
+        if (!f) return fail(CULBM_ERR_IO, "Could not open the file: " + path);
+        CULBM_TRY(culbm_get_field(sim, static_cast<culbm_field>(k), host.data()));
+        f.write(reinterpret_cast<const char*>(host.data()), static_cast<std::streamsize>(host.size() * sizeof(float)));
+        if (!f) return fail(CULBM_ERR_IO, "short write to " + path);
+    }
+    return CULBM_OK;
+}
+
+culbm_status culbm_get_step(culbm_sim* sim, uint64_t* step)
+{
+    if (sim == nullptr || step == nullptr) return fail(CULBM_ERR_INVALID_ARGUMENT, "NULL argument");
+    *step = sim->step;
+    return CULBM_OK;
+}
+
+culbm_status culbm_get_pulled_ddf(culbm_sim* sim, void* host_out, int32_t out_type)
+{
+    CULBM_TRY(check_sim(sim, true));
+    if (host_out == nullptr || (out_type != 0 && out_type != 1))
+        return fail(CULBM_ERR_INVALID_ARGUMENT, "bad output buffer or type");
+    const size_t tsize = out_type == 0 ? 4 : 8;
+    const size_t bytes = 27ull * sim->n * tsize;
+    void* d_out = nullptr;
+    CULBM_CUDA(cudaMalloc(&d_out, bytes));
+    const int layout = current_layout(sim);
+    culbm_status st = with_storage(sim, [&](auto tag) -> culbm_status {
+        using S = typename decltype(tag)::type;
+        using R = typename ArithOf<S>::type;
+        auto a = make_args<S>(sim, sim->cur, sim->cur);
+        const dim3 g = cell_grid(sim->dom), b = cell_block();
+        auto launch = [&](auto tt) {
+            using T = typename decltype(tt)::type;
+            T* o = static_cast<T*>(d_out);
+            if (layout == LAYOUT_PULL)
+                k_export_pulled<LAYOUT_PULL, S, R, T><<<g, b, 0, sim->stream>>>(a, o);
+            else if (layout == LAYOUT_AA_A)
+                k_export_pulled<LAYOUT_AA_A, S, R, T><<<g, b, 0, sim->stream>>>(a, o);
+            else
+                k_export_pulled<LAYOUT_AA_B, S, R, T><<<g, b, 0, sim->stream>>>(a, o);
+        };
+        if (out_type == 0) launch(Tag<float>{});
+        else launch(Tag<double>{});
+        CULBM_CUDA(cudaGetLastError());
+        CULBM_CUDA(cudaMemcpyAsync(host_out, d_out, bytes, cudaMemcpyDeviceToHost, sim->stream));
+        CULBM_CUDA(cudaStreamSynchronize(sim->stream));
+        return CULBM_OK;
+    });
+    cudaFree(d_out);
+    return st;
+}
+
+culbm_status culbm_set_ddf(culbm_sim* sim, const void* host_in, int32_t in_type)
+{
+    CULBM_TRY(check_sim(sim, true));
+    if (host_in == nullptr || (in_type != 0 && in_type != 1))
+        return fail(CULBM_ERR_INVALID_ARGUMENT, "bad input buffer or type");
+    const size_t tsize = in_type == 0 ? 4 : 8;
+    const size_t bytes = 27ull * sim->n * tsize;
+    void* d_in = nullptr;
+    CULBM_CUDA(cudaMalloc(&d_in, bytes));
+    const bool aa = current_layout(sim) != LAYOUT_PULL;
+    culbm_status st = with_storage(sim, [&](auto tag) -> culbm_status {
+        using S = typename decltype(tag)::type;
+        using R = typename ArithOf<S>::type;
+        CULBM_CUDA(cudaMemcpyAsync(d_in, host_in, bytes, cudaMemcpyHostToDevice, sim->stream));
+        const int target = aa ? 0 : sim->cur;
+        auto a = make_args<S>(sim, target, target);
+        const dim3 g = cell_grid(sim->dom), b = cell_block();
+        auto launch = [&](auto tt) {
+            using T = typename decltype(tt)::type;
+            const T* in = static_cast<const T*>(d_in);
+            if (aa)
+                k_import<LAYOUT_AA_A, S, R, T><<<g, b, 0, sim->stream>>>(a, in);
+            else
+                k_import<LAYOUT_PULL, S, R, T><<<g, b, 0, sim->stream>>>(a, in);
+        };
+        if (in_type == 0) launch(Tag<float>{});
+        else launch(Tag<double>{});
+        CULBM_CUDA(cudaGetLastError());
+        CULBM_CUDA(cudaStreamSynchronize(sim->stream));
+        if (aa) sim->aa_phase = 0;
+        return CULBM_OK;
+    });
+    cudaFree(d_in);
+    return st;
+}
+
+culbm_status culbm_mass_momentum(culbm_sim* sim, double out[4])
+{
+    CULBM_TRY(check_sim(sim, true));
+    if (out == nullptr) return fail(CULBM_ERR_INVALID_ARGUMENT, "out is NULL");
+    const int layout = current_layout(sim);
+    return with_storage(sim, [&](auto tag) -> culbm_status {
+        using S = typename decltype(tag)::type;
+        using R = typename ArithOf<S>::type;
+        auto a = make_args<S>(sim, sim->cur, sim->cur);
+        double* part = sim->d_red;
+        const int nb = sim->red_blocks;
+        if (layout == LAYOUT_PULL)
+            k_mass_momentum<LAYOUT_PULL, S, R><<<nb, 256, 0, sim->stream>>>(a, part);
+        else if (layout == LAYOUT_AA_A)
+            k_mass_momentum<LAYOUT_AA_A, S, R><<<nb, 256, 0, sim->stream>>>(a, part);
+        else
+            k_mass_momentum<LAYOUT_AA_B, S, R><<<nb, 256, 0, sim->stream>>>(a, part);
+        CULBM_CUDA(cudaGetLastError());
+        k_sum_partials<<<1, 32, 0, sim->stream>>>(part, nb, part + 4 * nb);
+        CULBM_CUDA(cudaGetLastError());
+        CULBM_CUDA(cudaMemcpyAsync(out, part + 4 * nb, 4 * sizeof(double), cudaMemcpyDeviceToHost, sim->stream));
+        CULBM_CUDA(cudaStreamSynchronize(sim->stream));
+        return CULBM_OK;
+    });
+}
+
+const char* culbm_last_error(void) { return t_last_error.c_str(); }
+
+const char* culbm_status_string(culbm_status s)
+{
+    switch (s) {
+        case CULBM_OK: return "CULBM_OK";
+        case CULBM_ERR_INVALID_ARGUMENT: return "CULBM_ERR_INVALID_ARGUMENT";
+        case CULBM_ERR_CUDA: return "CULBM_ERR_CUDA";
+        case CULBM_ERR_OUT_OF_MEMORY: return "CULBM_ERR_OUT_OF_MEMORY";
+        case CULBM_ERR_IO: return "CULBM_ERR_IO";
+        case CULBM_ERR_STATE: return "CULBM_ERR_STATE";
+        case CULBM_ERR_UNSUPPORTED: return "CULBM_ERR_UNSUPPORTED";
+        case CULBM_ERR_DEVICE_TIMEOUT: return "CULBM_ERR_DEVICE_TIMEOUT";
+    }
+    return "CULBM_ERR_UNKNOWN";
+}
+
+int32_t culbm_abi_version(void) { return CULBM_ABI_VERSION; }
+
+void culbm_debug_inject_cuda_error(int32_t skip, int32_t code)
+{
+    g_inject_skip.store(skip < 0 ? 0 : skip);
+    g_inject_code.store(code);
+}
+
+}  // extern "C"
+
+extern "C" culbm_status culbm_get_info(culbm_sim* sim, culbm_info* info)
+{
+    if (sim == nullptr || info == nullptr) return fail(CULBM_ERR_INVALID_ARGUMENT, "NULL argument");
+    std::memset(info, 0, sizeof(*info));
+    info->cells = static_cast<uint64_t>(sim->n);
+    info->device_bytes = sim->device_bytes;
+    for (int k = 0; k < 3; ++k) {
+        info->blocking_num[k] = 1;
+        info->blocking_dim[k] = sim->cfg.domain_dim[k];
+    }
+    info->storage = sim->cfg.storage;
+    info->stream_policy = sim->cfg.stream_policy;
+    info->opt_policy = sim->cfg.opt_policy;
+    info->inner_loop = sim->cfg.inner_loop;
+    info->kernel_launches_per_step_x1000 =
+        sim->launched_steps ? static_cast<uint32_t>(1000ull * sim->launches / sim->launched_steps) : 0;
+    return CULBM_OK;
+}

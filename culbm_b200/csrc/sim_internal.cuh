@@ -1,0 +1,92 @@
+// Internal state of a culbm_sim and the helpers shared by the host runtime
+// translation units (error reporting with fault injection, launch shapes).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+
+#include "culbm.h"
+#include "stream_kernels.cuh"
+
+namespace culbm {
+
+// ---------------------------------------------------------------- errors ---
+void set_last_error(const std::string& msg);
+culbm_status fail(culbm_status s, const std::string& msg);
+// Returns the injected error for this call, or cudaSuccess (no injection).
+cudaError_t injection_gate();
+culbm_status cuda_fail(cudaError_t e, const char* what, const char* file, int line);
+
+}  // namespace culbm
+
+// Runs a CUDA runtime call through the injection gate; on failure records
+// the message and returns CULBM_ERR_CUDA (or OUT_OF_MEMORY) from the caller.
+#define CULBM_CUDA(expr)                                                          \
+    do {                                                                          \
+        cudaError_t culbm_e_ = ::culbm::injection_gate();                         \
+        if (culbm_e_ == cudaSuccess) culbm_e_ = (expr);                           \
+        if (culbm_e_ != cudaSuccess)                                              \
+            return ::culbm::cuda_fail(culbm_e_, #expr, __FILE__, __LINE__);       \
+    } while (0)
+
+#define CULBM_TRY(expr)                                                           \
+    do {                                                                          \
+        culbm_status culbm_s_ = (expr);                                           \
+        if (culbm_s_ != CULBM_OK) return culbm_s_;                                \
+    } while (0)
+
+namespace culbm {
+
+struct TileState;   // blocked policies (tile_runtime.cu)
+
+}  // namespace culbm
+
+struct culbm_sim {
+    culbm_config cfg{};
+    culbm::Domain dom{};
+    long long n = 0;
+    int dev = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+
+    uint32_t* d_flag = nullptr;     // flag.dat words, N
+    uint8_t* d_ops = nullptr;       // compact op bytes, N
+    float* d_mac[4] = {};           // rho, vx, vy, vz, N each (EQU inputs and dump outputs)
+    void* d_pop[2] = {};            // population buffers, 27*N elements each
+    int npop = 0;                   // 1 (in-place) or 2 (double buffer)
+    void* d_edge = nullptr;         // in-place clamp side buffer
+    culbm::EdgeLayout el{};
+    long long edge_elems = 0;
+    size_t esize = 4;               // bytes per stored population
+    double* d_red = nullptr;        // reduction partials
+    int red_blocks = 0;
+
+    int cur = 0;                    // double buffer: index of the buffer holding the newest state
+    int aa_phase = 0;               // in-place: 0 = layout A, 1 = layout B
+    uint64_t step = 0;
+    uint64_t device_bytes = 0;
+    uint64_t launches = 0;          // kernel launches issued by step calls
+    uint64_t launched_steps = 0;
+    bool loaded = false;
+
+    culbm::TileState* tiles = nullptr;
+};
+
+namespace culbm {
+
+inline dim3 cell_block() { return dim3(32, 8, 1); }
+inline dim3 cell_grid(const Domain& D)
+{
+    return dim3((D.nx + 31) / 32, (D.ny + 7) / 8, D.nz);
+}
+
+// Blocked-policy entry points (tile_runtime.cu).
+culbm_status tiles_create(culbm_sim* sim);
+void tiles_destroy(culbm_sim* sim);
+culbm_status tiles_upload_flags(culbm_sim* sim, const uint32_t* host_flag);
+culbm_status tiles_step(culbm_sim* sim, uint32_t nsteps);
+bool is_blocked(const culbm_config& cfg);
+
+}  // namespace culbm

@@ -1,0 +1,319 @@
+// Whole-domain step kernels: pull double-buffer and in-place (AA pattern),
+// plus the moment (dump), state export/import and fill kernels that know how
+// each layout stores the populations.
+//
+// Layout in HBM: structure of arrays, one array per direction d, cell index
+// i = x + nx*(y + ny*z) (x fastest), exactly the reference's order
+// (src/simulator/single_dev_expt/kernel.cu:48-51) so that dumps and init
+// files map 1:1.  Each direction has its own base pointer in the kernel
+// parameters (constant bank), so no per-direction 64-bit offset is kept in
+// registers.
+//
+// Edge semantics: the reference's pull clamps the neighbour offset to 0 at
+// the domain boundary (kernel.cu:2506-2511), so a boundary cell re-reads its
+// own previous post-collision population for directions whose source is
+// outside.  The pull kernel does the same.  The in-place kernels reproduce it
+// bit for bit with a small side buffer ("edge buffer") that holds, for each
+// boundary cell and each such direction, the value the clamp would read.
+#pragma once
+
+#include "d3q27.cuh"
+#include "storage.cuh"
+
+namespace culbm {
+
+struct Domain {
+    int nx, ny, nz;
+    int nxy;   // nx*ny
+    int n;     // nx*ny*nz (< 2^31, checked on the host)
+};
+
+template <typename S>
+struct Pops {
+    S* p[27];
+};
+
+// Edge buffer: six face blocks (x-low, x-high, y-low, y-high, z-low, z-high),
+// each 9 directions x face cells.  A clamped (cell, d) pair is filed under
+// the first axis (x, then y, then z) along which cell - c_d leaves the domain;
+// the nine directions of a face are indexed by the two other components.
+struct EdgeLayout {
+    long long off[6];
+};
+
+template <typename S, typename R>
+struct StepArgs {
+    Domain dom;
+    const uint8_t* ops;
+    const float* rho;
+    const float* vx;
+    const float* vy;
+    const float* vz;
+    R inv_tau;
+    Pops<S> src;   // pull: read buffer.  in-place: the single buffer.
+    Pops<S> dst;   // pull: write buffer.  in-place: same buffer as src.
+    S* edge;       // in-place only
+    EdgeLayout el;
+};
+
+__device__ __forceinline__ int nb_off(const Domain& D, int d)
+{
+    return cx_of(d) + cy_of(d) * D.nx + cz_of(d) * D.nxy;
+}
+
+__device__ __forceinline__ bool inside(const Domain& D, int x, int y, int z)
+{
+    return (unsigned)x < (unsigned)D.nx && (unsigned)y < (unsigned)D.ny && (unsigned)z < (unsigned)D.nz;
+}
+
+// Element index of the edge-buffer slot of (x,y,z,d); only valid when
+// (x,y,z) - c_d is outside the domain.
+__device__ __forceinline__ long long edge_slot(const Domain& D, const EdgeLayout& L, int x, int y, int z, int d)
+{
+    const int cx = cx_of(d), cy = cy_of(d), cz = cz_of(d);
+    const int sx = x - cx, sy = y - cy;
+    if ((unsigned)sx >= (unsigned)D.nx) {
+        const int j = (cy + 1) + 3 * (cz + 1);
+        return L.off[sx < 0 ? 0 : 1] + (long long)j * D.ny * D.nz + y + (long long)D.ny * z;
+    }
+    if ((unsigned)sy >= (unsigned)D.ny) {
+        const int j = (cx + 1) + 3 * (cz + 1);
+        return L.off[sy < 0 ? 2 : 3] + (long long)j * D.nx * D.nz + x + (long long)D.nx * z;
+    }
+    const int sz = z - cz;
+    const int j = (cx + 1) + 3 * (cy + 1);
+    return L.off[sz < 0 ? 4 : 5] + (long long)j * D.nx * D.ny + x + (long long)D.nx * y;
+}
+
+// How the current state stores "the population f_d that cell x pulls next":
+//   LAYOUT_PULL  standard: post-collision f*_d(y) at [d][y]; pull from x - c_d,
+//                clamped to x at the boundary (pull double buffer, tiles).
+//   LAYOUT_AA_A  reversed own: f*_d(y) at [26-d][y]; pull from x - c_d,
+//                clamped values from the edge buffer (in-place, after an even
+//                step and at start).
+//   LAYOUT_AA_B  streamed: the pulled value already sits at [d][x]
+//                (in-place, after an odd step).
+enum Layout : int { LAYOUT_PULL = 0, LAYOUT_AA_A = 1, LAYOUT_AA_B = 2 };
+
+template <int LAYOUT, typename S, typename R>
+__device__ __forceinline__ void load_pulled(const StepArgs<S, R>& a, int x, int y, int z, int i, bool edge, R* f)
+{
+    const Domain& D = a.dom;
+    if (LAYOUT == LAYOUT_PULL) {
+        const int ndx = (x == 0) ? 0 : -1, pdx = (x == D.nx - 1) ? 0 : 1;
+        const int ndy = (y == 0) ? 0 : -D.nx, pdy = (y == D.ny - 1) ? 0 : D.nx;
+        const int ndz = (z == 0) ? 0 : -D.nxy, pdz = (z == D.nz - 1) ? 0 : D.nxy;
+#pragma unroll
+        for (int d = 0; d < 27; ++d) {
+            const int ox = cx_of(d) == 1 ? ndx : cx_of(d) == -1 ? pdx : 0;
+            const int oy = cy_of(d) == 1 ? ndy : cy_of(d) == -1 ? pdy : 0;
+            const int oz = cz_of(d) == 1 ? ndz : cz_of(d) == -1 ? pdz : 0;
+            f[d] = Cvt<S, R>::ld(a.src.p[d] + (i + ox + oy + oz));
+        }
+    } else if (LAYOUT == LAYOUT_AA_A) {
+        if (!edge) {
+#pragma unroll
+            for (int d = 0; d < 27; ++d) f[d] = Cvt<S, R>::ld(a.src.p[26 - d] + (i - nb_off(D, d)));
+        } else {
+#pragma unroll
+            for (int d = 0; d < 27; ++d) {
+                if (inside(D, x - cx_of(d), y - cy_of(d), z - cz_of(d)))
+                    f[d] = Cvt<S, R>::ld(a.src.p[26 - d] + (i - nb_off(D, d)));
+                else
+                    f[d] = Cvt<S, R>::ld(a.edge + edge_slot(D, a.el, x, y, z, d));
+            }
+        }
+    } else {
+#pragma unroll
+        for (int d = 0; d < 27; ++d) f[d] = Cvt<S, R>::ld(a.src.p[d] + i);
+    }
+}
+
+struct CellCoord {
+    int x, y, z, i;
+    bool valid;
+};
+
+__device__ __forceinline__ CellCoord cell_of_thread(const Domain& D)
+{
+    CellCoord c;
+    c.x = blockIdx.x * blockDim.x + threadIdx.x;
+    c.y = blockIdx.y * blockDim.y + threadIdx.y;
+    c.z = blockIdx.z;
+    c.valid = c.x < D.nx && c.y < D.ny;
+    c.i = c.x + D.nx * (c.y + D.ny * c.z);
+    return c;
+}
+
+// One pull step src -> dst over the whole domain.
+// Replaces StaticD3Q27PullKernel, reference kernel.cu:2489-2632.
+template <typename S, typename R>
+__global__ void __launch_bounds__(256) k_pull_step(const __grid_constant__ StepArgs<S, R> a)
+{
+    const CellCoord c = cell_of_thread(a.dom);
+    if (!c.valid) return;
+    const uint8_t op = a.ops[c.i];
+    R f[27];
+    if (op & OP_LOAD) {
+        load_pulled<LAYOUT_PULL>(a, c.x, c.y, c.z, c.i, false, f);
+    } else {
+#pragma unroll
+        for (int d = 0; d < 27; ++d) f[d] = R(0);
+    }
+    cell_update<R>(op, a.inv_tau, a.rho, a.vx, a.vy, a.vz, c.i, f);
+    if (op & OP_STORE) {
+#pragma unroll
+        for (int d = 0; d < 27; ++d) Cvt<S, R>::st(a.dst.p[d] + c.i, f[d]);
+    }
+}
+
+// In-place odd step (layout A -> B): each cell pulls f_d from the reversed
+// slot of x - c_d and pushes its post-collision f_d into slot d of x + c_d.
+// Cell x reads and writes exactly the same set of locations, so no other
+// thread touches them.  Boundary cells take clamped values from the edge
+// buffer and also write f_d into their own slot d when x - c_d is outside
+// (the value the clamped pull of the next step expects).
+template <typename S, typename R>
+__global__ void __launch_bounds__(256) k_aa_odd(const __grid_constant__ StepArgs<S, R> a)
+{
+    const CellCoord c = cell_of_thread(a.dom);
+    if (!c.valid) return;
+    const Domain& D = a.dom;
+    const uint8_t op = a.ops[c.i];
+    const bool edge = (op & OP_EDGE) != 0;
+    R f[27];
+    if (op & OP_LOAD) {
+        load_pulled<LAYOUT_AA_A>(a, c.x, c.y, c.z, c.i, edge, f);
+    } else {
+#pragma unroll
+        for (int d = 0; d < 27; ++d) f[d] = R(0);
+    }
+    cell_update<R>(op, a.inv_tau, a.rho, a.vx, a.vy, a.vz, c.i, f);
+    if (op & OP_STORE) {
+        if (!edge) {
+#pragma unroll
+            for (int d = 0; d < 27; ++d) Cvt<S, R>::st(a.dst.p[d] + (c.i + nb_off(D, d)), f[d]);
+        } else {
+#pragma unroll
+            for (int d = 0; d < 27; ++d) {
+                const int cx = cx_of(d), cy = cy_of(d), cz = cz_of(d);
+                if (inside(D, c.x + cx, c.y + cy, c.z + cz))
+                    Cvt<S, R>::st(a.dst.p[d] + (c.i + nb_off(D, d)), f[d]);
+                if (!inside(D, c.x - cx, c.y - cy, c.z - cz))
+                    Cvt<S, R>::st(a.dst.p[d] + c.i, f[d]);
+            }
+        }
+    }
+}
+
+// In-place even step (layout B -> A): own slots in, reversed own slots out.
+// Boundary cells also file f_d into the edge buffer for every d whose source
+// x - c_d is outside: the next odd step's clamped pull reads it there, because
+// slot 26-d of x is overwritten by x + c_d during that step.
+template <typename S, typename R>
+__global__ void __launch_bounds__(256) k_aa_even(const __grid_constant__ StepArgs<S, R> a)
+{
+    const CellCoord c = cell_of_thread(a.dom);
+    if (!c.valid) return;
+    const Domain& D = a.dom;
+    const uint8_t op = a.ops[c.i];
+    R f[27];
+    if (op & OP_LOAD) {
+        load_pulled<LAYOUT_AA_B>(a, c.x, c.y, c.z, c.i, false, f);
+    } else {
+#pragma unroll
+        for (int d = 0; d < 27; ++d) f[d] = R(0);
+    }
+    cell_update<R>(op, a.inv_tau, a.rho, a.vx, a.vy, a.vz, c.i, f);
+    if (op & OP_STORE) {
+#pragma unroll
+        for (int d = 0; d < 27; ++d) Cvt<S, R>::st(a.dst.p[26 - d] + c.i, f[d]);
+        if (op & OP_EDGE) {
+#pragma unroll
+            for (int d = 0; d < 27; ++d)
+                if (!inside(D, c.x - cx_of(d), c.y - cy_of(d), c.z - cz_of(d)))
+                    Cvt<S, R>::st(a.edge + edge_slot(D, a.el, c.x, c.y, c.z, d), f[d]);
+        }
+    }
+}
+
+// Moments of the pulled populations, written where the DUMP bits are set.
+// Replaces StaticD3Q27PullDumpKernel, reference kernel.cu:2634-2735 (and the
+// per-tile dump kernels, which compute the same values for CORRECT cells).
+template <int LAYOUT, typename S, typename R>
+__global__ void __launch_bounds__(256) k_moments(const __grid_constant__ StepArgs<S, R> a, const uint32_t* flag,
+                                                 float* rho, float* vx, float* vy, float* vz)
+{
+    const CellCoord c = cell_of_thread(a.dom);
+    if (!c.valid) return;
+    const uint32_t fl = flag[c.i];
+    if ((fl & (FLAG_DUMP_RHO | FLAG_DUMP_VX | FLAG_DUMP_VY | FLAG_DUMP_VZ)) == 0) return;
+    const bool edge = (a.ops[c.i] & OP_EDGE) != 0;
+    R f[27], r, ux, uy, uz;
+    load_pulled<LAYOUT>(a, c.x, c.y, c.z, c.i, edge, f);
+    moments<R>(f, r, ux, uy, uz);
+    if (fl & FLAG_DUMP_RHO) rho[c.i] = float(r);
+    if (fl & FLAG_DUMP_VX) vx[c.i] = float(ux);
+    if (fl & FLAG_DUMP_VY) vy[c.i] = float(uy);
+    if (fl & FLAG_DUMP_VZ) vz[c.i] = float(uz);
+}
+
+// Export the pulled populations out[d*n + i] (T = float or double).
+template <int LAYOUT, typename S, typename R, typename T>
+__global__ void __launch_bounds__(256) k_export_pulled(const __grid_constant__ StepArgs<S, R> a, T* out)
+{
+    const CellCoord c = cell_of_thread(a.dom);
+    if (!c.valid) return;
+    const bool edge = (a.ops[c.i] & OP_EDGE) != 0;
+    R f[27];
+    load_pulled<LAYOUT>(a, c.x, c.y, c.z, c.i, edge, f);
+#pragma unroll
+    for (int d = 0; d < 27; ++d) out[(long long)d * a.dom.n + c.i] = T(f[d]);
+}
+
+// Import a state given as post-collision populations in the standard layout
+// in[d*n + i] (T = float or double) into LAYOUT_PULL (dst) or LAYOUT_AA_A.
+template <int LAYOUT, typename S, typename R, typename T>
+__global__ void __launch_bounds__(256) k_import(const __grid_constant__ StepArgs<S, R> a, const T* in)
+{
+    const CellCoord c = cell_of_thread(a.dom);
+    if (!c.valid) return;
+    const Domain& D = a.dom;
+#pragma unroll 1
+    for (int d = 0; d < 27; ++d) {
+        const R v = R(in[(long long)d * D.n + c.i]);
+        if (LAYOUT == LAYOUT_PULL) {
+            Cvt<S, R>::st(a.dst.p[d] + c.i, v);
+        } else {
+            Cvt<S, R>::st(a.dst.p[26 - d] + c.i, v);
+            if (!inside(D, c.x - cx_of(d), c.y - cy_of(d), c.z - cz_of(d)))
+                Cvt<S, R>::st(a.edge + edge_slot(D, a.el, c.x, c.y, c.z, d), v);
+        }
+    }
+}
+
+// Uniform equilibrium fill feq(rho, u) of every cell (and of the edge buffer
+// for LAYOUT_AA_A): the reference starts from calcEqu(1,0,0,0) everywhere
+// (simulator_expt_platform.cu:230-250).
+template <int LAYOUT, typename S, typename R>
+__global__ void __launch_bounds__(256) k_fill_equilibrium(const __grid_constant__ StepArgs<S, R> a, R rho, R ux,
+                                                          R uy, R uz)
+{
+    const CellCoord c = cell_of_thread(a.dom);
+    if (!c.valid) return;
+    const Domain& D = a.dom;
+    R f[27];
+    equilibrium<R>(rho, ux, uy, uz, f);
+#pragma unroll
+    for (int d = 0; d < 27; ++d) {
+        if (LAYOUT == LAYOUT_PULL) {
+            Cvt<S, R>::st(a.dst.p[d] + c.i, f[d]);
+        } else {
+            Cvt<S, R>::st(a.dst.p[26 - d] + c.i, f[d]);
+            if (!inside(D, c.x - cx_of(d), c.y - cy_of(d), c.z - cz_of(d)))
+                Cvt<S, R>::st(a.edge + edge_slot(D, a.el, c.x, c.y, c.z, d), f[d]);
+        }
+    }
+}
+
+}  // namespace culbm

@@ -1,0 +1,236 @@
+/*
+ * culbm.h — C ABI of culbm_b200, a D3Q27 lattice Boltzmann (BGK) solver for
+ * one NVIDIA B200 (sm_100a).
+ *
+ * The reference (cuLBM) has no C ABI: its boundary is the single_dev_expt_main
+ * process (argv, init-state folder, dump files) over the C++ class
+ * culbm::simulator::single_dev_expt::Simulator
+ * (src/simulator/single_dev_expt/simulator_expt_platform.hpp:5-15).  Each entry
+ * point below names the reference code whose job it takes over.  Plain C
+ * types only: host pointers, sizes and status codes; no exceptions cross it.
+ *
+ * Threading: one culbm_sim is used by one host thread at a time.  All device
+ * work of a culbm_sim runs on its own CUDA stream; calls that return host data
+ * synchronise that stream.
+ *
+ * Ownership: the library owns every device buffer; host buffers passed in are
+ * only read (or written) during the call.
+ *
+ * Errors: every call returns a culbm_status; culbm_last_error() returns the
+ * message of the last failure on the calling thread.
+ */
+#ifndef CULBM_H
+#define CULBM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CULBM_ABI_VERSION 1
+
+typedef enum culbm_status {
+    CULBM_OK = 0,
+    CULBM_ERR_INVALID_ARGUMENT = 1, /* bad size/policy/geometry (reference: std::invalid_argument, runtime_error) */
+    CULBM_ERR_CUDA = 2,             /* a CUDA runtime call failed (reference: basic::cu::CudaRuntimeError) */
+    CULBM_ERR_OUT_OF_MEMORY = 3,    /* device allocation failed or would not fit */
+    CULBM_ERR_IO = 4,               /* init-state file missing or short, dump file not writable */
+    CULBM_ERR_STATE = 5,            /* call out of order */
+    CULBM_ERR_UNSUPPORTED = 6,      /* policy/storage combination not built */
+    CULBM_ERR_DEVICE_TIMEOUT = 7    /* a bounded device-side wait gave up */
+} culbm_status;
+
+/* --streamPolicy, simulator_expt_platform.cu:37-41 */
+typedef enum culbm_stream_policy { CULBM_STREAM_PULL = 0, CULBM_STREAM_INPLACE = 1 } culbm_stream_policy;
+
+/* --optPolicy, simulator_expt_platform.cu:43-49 */
+typedef enum culbm_opt_policy {
+    CULBM_OPT_NONE = 0,
+    CULBM_OPT_STATIC_L2 = 1,
+    CULBM_OPT_L1L2 = 2,
+    CULBM_OPT_DYNAMIC_L2 = 3
+} culbm_opt_policy;
+
+/* Population storage in HBM (no reference counterpart; the reference is FP32 only). */
+typedef enum culbm_storage {
+    CULBM_STORAGE_F32 = 0,  /* FP32, the reference's format */
+    CULBM_STORAGE_F16 = 1,  /* FP16 deviations f_i - w_i (scaled by 2^15), FP32 arithmetic */
+    CULBM_STORAGE_BF16 = 2, /* BF16 deviations f_i - w_i, FP32 arithmetic */
+    CULBM_STORAGE_F64 = 3   /* FP64 storage and arithmetic (the GPU oracle) */
+} culbm_storage;
+
+typedef enum culbm_field {
+    CULBM_FIELD_RHO = 0,
+    CULBM_FIELD_VX = 1,
+    CULBM_FIELD_VY = 2,
+    CULBM_FIELD_VZ = 3
+} culbm_field;
+
+/* Flag bits of flag.dat, src/simulator/single_dev_expt/local_config.hpp:12-22. */
+#define CULBM_FLAG_LOAD (1u << 0)
+#define CULBM_FLAG_EQU (1u << 1)
+#define CULBM_FLAG_COLLIDE (1u << 2)
+#define CULBM_FLAG_BOUNCE_BACK (1u << 3)
+#define CULBM_FLAG_STORE (1u << 4)
+#define CULBM_FLAG_DUMP_RHO (1u << 27)
+#define CULBM_FLAG_DUMP_VX (1u << 28)
+#define CULBM_FLAG_DUMP_VY (1u << 29)
+#define CULBM_FLAG_DUMP_VZ (1u << 30)
+
+/*
+ * Solver configuration.  The first block mirrors the single_dev_expt_main
+ * options and their defaults (simulator_expt_platform.cu:312-354); the rest
+ * are additions.
+ */
+typedef struct culbm_config {
+    int32_t dev_id;            /* --devId, default 0 */
+    uint32_t block_dim[3];     /* --blockDim, default [32,16,2] */
+    uint32_t grid_dim[3];      /* --gridDim, default [2,3,19] */
+    uint32_t domain_dim[3];    /* --domainDim, default [256,256,256] */
+    int32_t inner_loop;        /* --innerLoop, default 5 */
+    int32_t stream_policy;     /* --streamPolicy, culbm_stream_policy */
+    int32_t opt_policy;        /* --optPolicy, culbm_opt_policy */
+    int32_t vel_set;           /* --velSet, 0 = D3Q27 (the only one) */
+    float inv_tau;             /* --invTau, default 0.5 */
+    int32_t use_ring_ddf_buf;  /* --useRingDDFBuf */
+    /* additions */
+    int32_t storage;           /* culbm_storage, default F32 */
+    int32_t persist_l2;        /* 1 (default): L2 persisting window over tile buffers
+                                  (reference build switch CULBM_EXPT_ENABLE_PERSISTENT_L2) */
+    int32_t cache_hints;       /* 1 (default): evict-first/evict-last hints on global/tile traffic
+                                  (reference build switch CULBM_EXPT_CACHE_HINT_POLICY) */
+    int32_t use_graphs;        /* 1 (default): tile launch sequences replayed as CUDA graphs */
+    uint32_t reserved[8];
+} culbm_config;
+
+/* Fills cfg with the reference's defaults plus the additions' defaults. */
+culbm_status culbm_config_init(culbm_config* cfg);
+
+typedef struct culbm_sim culbm_sim;
+
+/*
+ * Validates cfg, selects the device, allocates every device buffer and fills
+ * the populations with rest equilibrium; flags default to fluid everywhere
+ * and rho/u to 1/0 until culbm_load_state is called.
+ * Replaces Simulator::Data::Data, simulator_expt_platform.cu:308-445
+ * (minus argv parsing, which single_dev_expt_main does on top of this ABI).
+ */
+culbm_status culbm_create(const culbm_config* cfg, culbm_sim** out);
+
+/* Frees every device resource.  Replaces Simulator::Data::~Data, simulator_expt_platform.cu:447-505. */
+culbm_status culbm_destroy(culbm_sim* sim);
+
+/*
+ * Loads an init state from host arrays of domain_dim[0]*[1]*[2] values,
+ * x fastest.  flag == NULL selects LOAD|COLLIDE|STORE|DUMP_* everywhere;
+ * rho == NULL selects 1, vx/vy/vz == NULL select 0.  Resets the populations
+ * to rest equilibrium and the step counter to 0.
+ * Replaces initFlag / initBlockingFlag / initRhoU / initDoubleDDFBuf /
+ * initRingDDFBuf, simulator_expt_platform.cu:95-277.
+ */
+culbm_status culbm_load_state(culbm_sim* sim, const uint32_t* flag, const float* rho, const float* vx,
+                              const float* vy, const float* vz);
+
+/*
+ * Same from an init-state folder: <folder>/flag.dat is mandatory, rho.dat,
+ * vx.dat, vy.dat, vz.dat are optional (raw little-endian, N values).
+ * loaded_mask (may be NULL) receives bit k set when field k of
+ * {flag, rho, vx, vy, vz} came from a file.  folder == NULL or "" behaves like
+ * culbm_load_state with all NULL.  Error behaviour of initFlag/initRhoU:
+ * a missing flag.dat is CULBM_ERR_IO.
+ */
+culbm_status culbm_load_state_folder(culbm_sim* sim, const char* folder, uint32_t* loaded_mask);
+
+/*
+ * Advances exactly nsteps time steps (stream-ordered, returns after enqueue).
+ * Replaces one run lambda's inner step loop, simulator_expt_platform.cu:608-991.
+ */
+culbm_status culbm_step(culbm_sim* sim, uint32_t nsteps);
+
+/* Same, then waits and reports the device time of those steps (CUDA events). */
+culbm_status culbm_step_timed(culbm_sim* sim, uint32_t nsteps, float* elapsed_ms);
+
+/* Waits for all work of sim. */
+culbm_status culbm_synchronize(culbm_sim* sim);
+
+/*
+ * Dump kernel: writes rho/vx/vy/vz of the pulled populations into the
+ * device macroscopic buffers where the DUMP bits are set.
+ * Replaces StaticD3Q27PullDumpKernel and the per-tile dump kernels,
+ * src/simulator/single_dev_expt/kernel.cu:2634-2735, 1829-1936.
+ */
+culbm_status culbm_moments(culbm_sim* sim);
+
+/* Copies one device macroscopic buffer (N floats) to host_out; synchronises.
+ * Replaces the cudaMemcpy of dumpRes, simulator_expt_platform.cu:572-606. */
+culbm_status culbm_get_field(culbm_sim* sim, culbm_field field, float* host_out);
+
+/*
+ * Writes <folder>/<rho|vx|vy|vz>_<step>.dat for every field whose bit is set
+ * in field_mask (bit k = culbm_field k), creating the folder first even when
+ * the mask is 0.  Replaces dumpRes, simulator_expt_platform.cu:572-606.
+ */
+culbm_status culbm_dump(culbm_sim* sim, const char* folder, uint32_t field_mask);
+
+/* Time steps done since the last load. */
+culbm_status culbm_get_step(culbm_sim* sim, uint64_t* step);
+
+/*
+ * The 27*N populations each cell would pull at the next step, out[d*N + i],
+ * as float (out_type 0) or double (out_type 1).  This is the state every
+ * streaming policy agrees on bit for bit.  Synchronises.
+ */
+culbm_status culbm_get_pulled_ddf(culbm_sim* sim, void* host_out, int32_t out_type);
+
+/*
+ * Replaces the state by post-collision populations in the standard layout
+ * in[d*N + i] (what the reference's src buffer holds between steps), given as
+ * float (in_type 0) or double (in_type 1).  Does not reset the step counter.
+ */
+culbm_status culbm_set_ddf(culbm_sim* sim, const void* host_in, int32_t in_type);
+
+/* Total mass sum(rho) and momentum sum(rho*u) over the cells that have any of
+ * LOAD|EQU, from the pulled populations, accumulated in FP64 on the device:
+ * out[0] = mass, out[1..3] = momentum x,y,z.  No reference counterpart. */
+culbm_status culbm_mass_momentum(culbm_sim* sim, double out[4]);
+
+typedef struct culbm_info {
+    uint64_t cells;                 /* N */
+    uint64_t device_bytes;          /* bytes the library allocated on the device */
+    uint32_t blocking_num[3];       /* tiles per axis (blocked policies), else 1 */
+    uint32_t blocking_dim[3];       /* tile extent = blockDim*gridDim (blocked policies) */
+    int32_t storage;
+    int32_t stream_policy;
+    int32_t opt_policy;
+    int32_t inner_loop;
+    uint64_t persisting_l2_bytes;   /* bytes of the L2 access-policy window (0 if none) */
+    uint32_t kernel_launches_per_step_x1000;  /* average launches per time step, times 1000 */
+    uint32_t reserved[7];
+} culbm_info;
+
+culbm_status culbm_get_info(culbm_sim* sim, culbm_info* info);
+
+/* Message of the last failure on this thread ("" if none). */
+const char* culbm_last_error(void);
+
+/* Constant name of a status code. */
+const char* culbm_status_string(culbm_status s);
+
+/* ABI version of the loaded library (CULBM_ABI_VERSION it was built with). */
+int32_t culbm_abi_version(void);
+
+/*
+ * Fault-injection hook for the host-side error paths (tests): after `skip`
+ * further CUDA runtime calls made by the library succeed, the next one is
+ * reported as failed with CUDA error code `code` (the call itself is not
+ * made).  code == 0 disables injection.  No device fault is involved.
+ */
+void culbm_debug_inject_cuda_error(int32_t skip, int32_t code);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CULBM_H */

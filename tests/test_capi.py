@@ -1,0 +1,100 @@
+"""C ABI checks that need no GPU: the library loads, exports every declared
+symbol, fills the reference's defaults and rejects bad configurations with
+the reference's messages before touching the device.  CUDA failures are
+injected on the host (culbm_debug_inject_cuda_error); no device fault."""
+import ctypes as C
+import os
+import re
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    names = set()
+    inc = os.path.join(ROOT, "include")
+    for fn in os.listdir(inc):
+        if fn.endswith(".h"):
+            text = open(os.path.join(inc, fn)).read()
+            names.update(re.findall(r"\b(culbm_\w+)\s*\(", text))
+    return sorted(names)
+
+
+def test_library_exports_every_declared_symbol(culbm):
+    from culbm_b200 import _capi
+    lib = _capi.lib()
+    syms = declared_symbols()
+    assert len(syms) >= 20
+    for name in syms:
+        assert hasattr(lib, name), name
+    assert lib.culbm_abi_version() == 1
+
+
+def test_config_defaults_are_the_reference_cli_defaults(culbm):
+    from culbm_b200 import _capi
+    cfg = _capi.default_config()
+    assert list(cfg.block_dim) == [32, 16, 2]
+    assert list(cfg.grid_dim) == [2, 3, 19]
+    assert list(cfg.domain_dim) == [256, 256, 256]
+    assert cfg.inner_loop == 5 and cfg.inv_tau == 0.5
+    assert cfg.stream_policy == 0 and cfg.opt_policy == 0 and cfg.vel_set == 0 and cfg.dev_id == 0
+    assert cfg.use_ring_ddf_buf == 0 and cfg.storage == 0
+
+
+def _create(cfg):
+    from culbm_b200 import _capi
+    h = C.c_void_p()
+    st = _capi.lib().culbm_create(C.byref(cfg), C.byref(h))
+    msg = _capi.lib().culbm_last_error().decode()
+    if st == 0:
+        _capi.lib().culbm_destroy(h)
+    return st, msg
+
+
+@pytest.mark.parametrize("mutate,needle", [
+    (lambda c: setattr(c, "use_ring_ddf_buf", 1), "--useRingDDFBuf is unimplemented"),
+    (lambda c: c.domain_dim.__setitem__(0, 100), "Dimension of domain doesn't match computation grid!"),
+    (lambda c: setattr(c, "vel_set", 3), "Unsupport Velocity Set"),
+    (lambda c: setattr(c, "stream_policy", 2), "streamPolicy"),
+    (lambda c: setattr(c, "inv_tau", 2.5), "invTau"),
+    (lambda c: c.domain_dim.__setitem__(2, 0), "domainDim"),
+])
+def test_invalid_configs_rejected_before_device(culbm, mutate, needle):
+    from culbm_b200 import _capi
+    cfg = _capi.default_config()
+    cfg.grid_dim[0], cfg.grid_dim[1], cfg.grid_dim[2] = 8, 16, 128   # 32*8=256, 16*16=256, 2*128=256
+    mutate(cfg)
+    st, msg = _create(cfg)
+    assert st == 1, (st, msg)
+    assert needle in msg
+
+
+def test_injected_cuda_error_is_reported(culbm):
+    from culbm_b200 import _capi
+    cfg = _capi.default_config()
+    cfg.domain_dim[0] = cfg.domain_dim[1] = cfg.domain_dim[2] = 8
+    cfg.block_dim[0] = cfg.block_dim[1] = cfg.block_dim[2] = 8
+    cfg.grid_dim[0] = cfg.grid_dim[1] = cfg.grid_dim[2] = 1
+    _capi.lib().culbm_debug_inject_cuda_error(0, 2)   # cudaErrorMemoryAllocation on the first call
+    try:
+        st, msg = _create(cfg)
+    finally:
+        _capi.lib().culbm_debug_inject_cuda_error(0, 0)
+    assert st == 3, (st, msg)          # CULBM_ERR_OUT_OF_MEMORY
+    assert "cudaErrorMemoryAllocation" in msg
+
+
+def test_status_strings(culbm):
+    from culbm_b200 import _capi
+    lib = _capi.lib()
+    for code, name in _capi.STATUS_NAMES.items():
+        assert lib.culbm_status_string(code).decode() == name
+
+
+def test_null_arguments(culbm):
+    from culbm_b200 import _capi
+    lib = _capi.lib()
+    assert lib.culbm_create(None, None) == 1
+    assert lib.culbm_step(None, 1) == 1
+    assert lib.culbm_destroy(None) == 0

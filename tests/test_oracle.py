@@ -1,0 +1,102 @@
+"""The CPU oracle pinned against the reference (CPU only).
+
+Two pins: the golden fixtures of tests/golden/ (made from the reference's own
+lbm_core routines, see make_golden.py) and, when oracle/_ref was built, the
+reference routines called live on fresh random inputs.
+"""
+import os
+
+import numpy as np
+import pytest
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def bits(a):
+    return np.ascontiguousarray(a).view(np.uint32 if a.dtype == np.float32 else np.uint64)
+
+
+def load(name):
+    return np.load(os.path.join(GOLDEN, name))
+
+
+def test_unit_vectors_bitwise(orc):
+    g = load("unit_vectors.npz")
+    for k in range(g["rho"].size):
+        e = orc.equ(g["rho"][k], *g["u"][k])
+        assert np.array_equal(bits(e), bits(g["equ"][k])), k
+        c = orc.collide(g["inv_tau"][k], g["f"][k])
+        assert np.array_equal(bits(c), bits(g["collide"][k])), k
+        m = np.array(orc.rhou(np.ascontiguousarray(g["f"][k])), np.float32)
+        assert np.array_equal(bits(m), bits(g["moments"][k])), k
+
+
+@pytest.mark.parametrize("name", ["random_13x11x9.npz", "channel_16x12x10.npz", "stream_9x7x5.npz"])
+def test_stepped_fixtures_bitwise(orc, name):
+    g = load(name)
+    sc = orc.Scene(int(g["nx"]), int(g["ny"]), int(g["nz"]), g["flag"], g["rho"], g["vx"], g["vy"], g["vz"])
+    out = orc.run(sc, float(g["inv_tau"]), int(g["nsteps"]), state=g["state0"])
+    assert np.array_equal(bits(out), bits(g["state"]))
+    assert np.array_equal(bits(orc.pulled(sc, out)), bits(g["pulled"]))
+    mom = orc.moments(sc, out)
+    for got, key in zip(mom, ("d_rho", "d_vx", "d_vy", "d_vz")):
+        assert np.array_equal(bits(got), bits(g[key])), key
+
+
+def test_streaming_fixture_is_permutation(orc):
+    """LOAD|STORE only: every pulled value is some population of the start state."""
+    g = load("stream_9x7x5.npz")
+    start = set(bits(g["state0"]).tolist())
+    assert set(bits(g["state"]).tolist()) <= start
+
+
+def test_oracle_matches_reference_live(orc):
+    if not orc.ref_available():
+        pytest.skip("oracle/_ref not built (make -C oracle ref-cpu)")
+    rng = np.random.default_rng(7)
+    nx, ny, nz = 11, 9, 7
+    n = nx * ny * nz
+    combos = np.array([orc.LOAD | orc.COLLIDE | orc.STORE | orc.DUMP_ALL, orc.LOAD | orc.BOUNCE_BACK | orc.STORE,
+                       orc.EQU | orc.STORE, orc.LOAD | orc.COLLIDE, 0], np.uint32)
+    sc = orc.Scene(nx, ny, nz, rng.choice(combos, n), rho=(1 + 0.01 * rng.standard_normal(n)).astype(np.float32),
+                   vx=(0.02 * rng.standard_normal(n)).astype(np.float32))
+    a = orc.run(sc, 1.3, 9)
+    b = orc.ref_run(sc, 1.3, 9)
+    assert np.array_equal(bits(a), bits(b))
+    for x, y in zip(orc.moments(sc, a), orc.ref_moments(sc, b)):
+        assert np.array_equal(bits(x), bits(y))
+
+
+def test_fp64_oracle_close_to_fp32(orc):
+    g = load("channel_16x12x10.npz")
+    sc = orc.Scene(int(g["nx"]), int(g["ny"]), int(g["nz"]), g["flag"], g["rho"], g["vx"], g["vy"], g["vz"])
+    f32 = orc.run(sc, 0.5, 30)
+    f64 = orc.run(sc, 0.5, 30, dtype=np.float64)
+    assert np.max(np.abs(f64 - f32)) < 1e-6
+    assert np.max(np.abs(f64)) > 1e-3   # the flow is not trivial
+
+
+def test_blocking_geometry_matches_reference(orc):
+    L = orc.lib()
+    R = orc.ref() if orc.ref_available() else None
+    for dom in (7, 64, 96, 280, 288, 384, 768):
+        for blk in (4, 16, 64, 76, 96, 128):
+            for it in (1, 2, 3, 5, 9):
+                v = L.orc_valid_blk_axis(dom, blk, it)
+                if R is not None:
+                    assert v == R.ref_valid_blk_axis(dom, blk, it)
+                if not v:
+                    continue
+                if dom > blk and dom > 2 * (blk + 1 - it) and blk + 2 - 2 * it <= 0:
+                    # validBlkAxisConfig lets this through but calcBlkNum then
+                    # divides by blk+2-2*it <= 0 (the reference crashes or wraps);
+                    # culbm_b200 rejects it at create time instead.
+                    continue
+                num = L.orc_blk_num(dom, blk, it)
+                if R is not None:
+                    assert num == R.ref_blk_num(dom, blk, it)
+                prev = [L.orc_valid_prev(k, blk, num, it, dom) for k in range(num + 1)]
+                if R is not None:
+                    assert prev == [R.ref_valid_prev(k, blk, num, it, dom) for k in range(num + 1)]
+                assert prev[0] == 0 and prev[-1] == dom
+                assert all(b >= a for a, b in zip(prev, prev[1:]))
