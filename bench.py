@@ -1,0 +1,397 @@
+"""D3Q27 BGK throughput on one B200 (MLUPS), with its roofline, an end-to-end
+number through the C ABI and the CPU baseline.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload: the 288x272x280 channel with 40 seeded spheres (radii 4-12),
+invTau 0.5, inlet ux 0.05 (synthetic, seeded; the reference ships no dataset).
+A step is one lattice update of every cell.  The headline `value` is FP32
+in-place streaming (streamPolicy 1, optPolicy 0) timed on the device over K
+steps with inputs resident in HBM; the population buffers (2.37 GB) are far
+larger than L2, so no flush is needed between steps.  The line also carries
+FP32 pull, blocked and FP16/BF16-storage speeds, and the FP16/BF16/FP32 error
+against an FP64 run of the scaled 128x128x64 copy of the 512x512x256 workload.
+
+--impl reference times the reference's own lbm_core routines compiled for
+the host (oracle/_ref, OpenMP over all host cores) on the same workload.
+With torchrun (N > 1) every rank runs an independent replica (the hot path
+has no data-path exchange); value = all ranks' updates / max time over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "D3Q27 MLUPS, FP32 vs FP16-store at stated FP64 err; adjoint/forward cost"
+BYTES_PER_LUP = {"fp32": 216, "fp16": 108, "bf16": 108, "fp64": 432}
+WORKLOAD = "288x272x280 channel, 40 seeded spheres r in [4,12], invTau 0.5, ux_in 0.05"
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi SM clock / throttle sampling during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index=0):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                     timeout=10).stdout.strip()
+                if out:
+                    self.samples.append([v.strip() for v in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        self._t.join(timeout=15)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for s in self.samples for k in range(4) if "Active" in s[2 + k]})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    return ws, rank
+
+
+def dist_init(ws):
+    if ws <= 1:
+        return None
+    import datetime
+
+    import torch.distributed as tdist
+    tdist.init_process_group("gloo", timeout=datetime.timedelta(seconds=120))
+    return tdist
+
+
+def max_over_ranks(tdist, v):
+    if tdist is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64)
+    tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(tdist):
+    if tdist is not None:
+        tdist.barrier()
+
+
+def pinned(arr):
+    """A page-locked host copy of arr (torch pinned memory, viewed by numpy)."""
+    import torch
+    t = torch.empty(arr.size, dtype={np.uint32: torch.int32, np.float32: torch.float32}[arr.dtype.type],
+                    pin_memory=True)
+    out = t.numpy().view(arr.dtype)
+    out[:] = arr.reshape(-1)
+    return out, t
+
+
+def traffic_from_profiles(kernel_key):
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        d = json.load(f)
+    return d.get(kernel_key)
+
+
+# ------------------------------------------------------------------- ours ---
+
+def measure(culbm, scene, sp, op, storage, steps, warmup, tile=None, inner=5, ring=False):
+    arrs = scene.arrays()
+    kw = {"dev_id": int(os.environ.get("LOCAL_RANK", "0"))}
+    if op:
+        kw.update(tile=tile, inner_loop=inner, use_ring=ring)
+    with culbm.Simulation(scene.shape, stream_policy=sp, opt_policy=op, storage=storage, inv_tau=0.5, **kw) as sim:
+        sim.load_state(*arrs)
+        sim.step(warmup)
+        ms = sim.step_timed(steps)
+        info = sim.info()
+    return scene.n * steps / (ms * 1e-3) / 1e6, ms / steps, info
+
+
+def fp64_errors(culbm, steps=1000):
+    """Relative rho/u error after `steps` steps against FP64 storage+arithmetic, on the
+    scaled 128x128x64 copy of the 512x512x256 workload."""
+    from culbm_b200 import scenes
+    sc = scenes.spheres_512(scale=0.25)
+    arrs = sc.arrays()
+    fluid = (arrs[0] & scenes.COLLIDE) != 0
+
+    def fields(storage):
+        with culbm.Simulation(sc.shape, stream_policy=1, storage=storage, inv_tau=0.5) as sim:
+            sim.load_state(*arrs)
+            sim.step(steps)
+            sim.moments()
+            return [f.astype(np.float64) for f in sim.fields()]
+
+    ref = fields("fp64")
+    umag = np.sqrt(ref[1] ** 2 + ref[2] ** 2 + ref[3] ** 2)
+    out = {}
+    for st in ("fp32", "fp16", "bf16"):
+        got = fields(st)
+        du = np.sqrt(sum((got[k] - ref[k]) ** 2 for k in (1, 2, 3)))
+        out[st] = {
+            "rel_u_l2": float(np.linalg.norm(du[fluid]) / np.linalg.norm(umag[fluid])),
+            "rel_u_max": float(np.max(du[fluid]) / np.max(umag[fluid])),
+            "rel_rho_max": float(np.max(np.abs(got[0] - ref[0])[fluid] / ref[0][fluid])),
+        }
+    return {"workload": f"{sc.shape[0]}x{sc.shape[1]}x{sc.shape[2]} spheres (512x512x256 generator at 1/4), "
+                        f"{steps} steps, vs FP64 storage+arithmetic", "errors": out}
+
+
+def e2e_run(culbm, scene, steps, sp=1):
+    """Through the public API with host buffers: pinned H2D of the init state,
+    `steps` steps, the dump kernel and the D2H read of rho/vx/vy/vz."""
+    arrs = scene.arrays()
+    host = [pinned(a) for a in arrs]
+    outs = [pinned(np.zeros(scene.n, np.float32)) for _ in range(4)]
+    import ctypes as C
+
+    from culbm_b200 import _capi
+    with culbm.Simulation(scene.shape, stream_policy=sp, inv_tau=0.5) as sim:
+        sim.load_state(*arrs)
+        sim.step(5)
+        sim.synchronize()
+        lib = _capi.lib()
+        t0 = time.perf_counter()
+        _capi.check(lib.culbm_load_state(sim._h, *[h[0].ctypes.data_as(C.c_void_p) for h in host]))
+        sim.step(steps)
+        sim.moments()
+        for k in range(4):
+            _capi.check(lib.culbm_get_field(sim._h, k, outs[k][0].ctypes.data_as(C.c_void_p)))
+        dt = time.perf_counter() - t0
+    h2d = sum(h[0].nbytes for h in host)
+    d2h = sum(o[0].nbytes for o in outs)
+    return scene.n * steps / dt / 1e6, h2d, d2h
+
+
+def cpu_baseline(scene, budget_s=12.0):
+    import oracle
+    if not oracle.ref_available():
+        return None
+    f, r, ux, uy, uz = scene.arrays()
+    nx, ny, nz = scene.shape
+    o = oracle.Scene(nx, ny, nz, f, r, ux, uy, uz)
+    a = oracle.rest_state(o.n)
+    b = a.copy()
+    threads = oracle.ref().ref_max_threads()
+    oracle.ref_step(o, 0.5, a, b)     # warm-up (page faults, thread pool)
+    steps, t0 = 0, time.perf_counter()
+    while True:
+        oracle.ref_step(o, 0.5, a, b)
+        a, b = b, a
+        steps += 1
+        if time.perf_counter() - t0 > budget_s or steps >= 200:
+            break
+    dt = time.perf_counter() - t0
+    return {"value": round(o.n * steps / dt / 1e6, 2), "unit": "MLUPS", "cores": threads, "kind": "reference",
+            "sample": f"{steps} full steps of the same 288x272x280 workload ({dt:.1f} s); the reference's "
+                      f"lbm_core (device_function.hpp) compiled for the host, pull loop of StaticD3Q27PullKernel, "
+                      f"OpenMP over z with {threads} threads"}
+
+
+def run_ours(args):
+    ws, rank = dist()
+    tdist = dist_init(ws)
+    import culbm_b200
+    from culbm_b200 import _capi, scenes
+    _capi.lib()
+    sc = scenes.spheres_288()
+    arrs = sc.arrays()
+    peak, peak_kind = peaks()
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    # headline: FP32 in-place, whole domain
+    with culbm_b200.Simulation(sc.shape, stream_policy=1, opt_policy=0, storage="fp32", inv_tau=0.5,
+                               dev_id=local) as sim:
+        sim.load_state(*arrs)
+        sim.step(args.warmup)
+        sim.synchronize()
+        barrier(tdist)
+        with ClockSampler(local) as clocks:
+            ms = sim.step_timed(args.steps)
+        info = sim.info()
+    barrier(tdist)
+    ms_max = max_over_ranks(tdist, ms)
+    value = ws * sc.n * args.steps / (ms_max * 1e-3) / 1e6
+    ms_per_step = ms_max / args.steps
+    launches = int(round(info["launches_per_step"] * args.steps))
+
+    if rank != 0:
+        if tdist is not None:
+            tdist.destroy_process_group()
+        return
+
+    achieved = BYTES_PER_LUP["fp32"] * sc.n / (ms / args.steps * 1e-3) / 1e9
+    extra = {}
+    k2 = max(20, args.steps // 4)
+    for name, (sp, op, st, tile) in {
+        "pull_fp32": (0, 0, "fp32", None),
+        "inplace_fp16": (1, 0, "fp16", None),
+        "inplace_bf16": (1, 0, "bf16", None),
+        "pull_fp16": (0, 0, "fp16", None),
+        "blocked_inplace_fp32": (1, 3, "fp32", (144, 68, 40)),
+    }.items():
+        try:
+            mlups, mps, inf = measure(culbm_b200, sc, sp, op, st, k2, 3, tile=tile, inner=5)
+            extra[name] = {"mlups": round(mlups, 1), "ms_per_step": round(mps, 4),
+                           "hbm_frac_of_measured": round(mlups * 1e6 * BYTES_PER_LUP[st] / 1e9 / peak, 4),
+                           "policy": f"streamPolicy {sp}, optPolicy {op}" + (f", tile {tile}, innerLoop 5" if op else "")}
+        except Exception as e:   # report, do not hide
+            extra[name] = {"error": str(e)}
+    try:
+        errs = fp64_errors(culbm_b200, steps=args.err_steps)
+    except Exception as e:
+        errs = {"error": str(e)}
+    e2e_mlups, h2d, d2h = e2e_run(culbm_b200, sc, args.steps)
+    cpu = cpu_baseline(sc) if ws == 1 else None
+
+    line = {
+        "metric": METRIC,
+        "value": round(value, 1),
+        "unit": "MLUPS",
+        "n_gpus": ws,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(ms_per_step, 4),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded sphere channel in the reference's flag.dat format)",
+        "config": {"workload": WORKLOAD, "cells": sc.n, "solid_fraction": round(sc.solid_fraction(), 4),
+                   "policy": "streamPolicy 1 (in-place AA), optPolicy 0", "storage": "fp32",
+                   "l2": "no flush: 2.37 GB of populations per step, 19x the 126 MB L2",
+                   "parallelism": f"{ws} independent replica(s), one per GPU"},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "peak_kind": f"{peak_kind} copy bandwidth",
+                     "algorithmic_bytes_per_lup": BYTES_PER_LUP["fp32"],
+                     "traffic": traffic_from_profiles("inplace_fp32_per_step")},
+        "e2e": {"value": round(e2e_mlups, 1), "unit": "MLUPS", "h2d_bytes_per_step": round(h2d / args.steps),
+                "d2h_bytes_per_step": round(d2h / args.steps),
+                "what": f"culbm_load_state from pinned host + {args.steps} steps + culbm_moments + "
+                        f"4x culbm_get_field to pinned host, host wall clock"},
+        "gpu_launches": launches,
+        "clocks": clocks.summary(),
+        "cpu_baseline": cpu,
+        "variants": extra,
+        "fp64_error": errs,
+    }
+    print(json.dumps(line), flush=True)
+
+
+# -------------------------------------------------------------- reference ---
+
+def run_reference(args):
+    ws, rank = dist()
+    if rank != 0:
+        return
+    import oracle
+    if not oracle.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libref_lbm_core.so not built "
+                                                             "(make -C oracle ref-cpu needs the reference tree)"}))
+        return
+    from culbm_b200 import scenes
+    sc = scenes.spheres_288()
+    f, r, ux, uy, uz = sc.arrays()
+    nx, ny, nz = sc.shape
+    o = oracle.Scene(nx, ny, nz, f, r, ux, uy, uz)
+    a = oracle.rest_state(o.n)
+    b = a.copy()
+    threads = oracle.ref().ref_max_threads()
+    # Each step is one lattice update of a z-slab sample sized so that the
+    # whole run stays within about two minutes of CPU time.
+    t0 = time.perf_counter()
+    oracle.ref_step(o, 0.5, a, b)
+    full_s = time.perf_counter() - t0
+    total = args.steps + args.warmup
+    frac = min(1.0, 100.0 / max(full_s * total, 1e-9))
+    z1 = max(1, int(round(nz * frac)))
+    for _ in range(args.warmup):
+        oracle.ref_step(o, 0.5, a, b, 0, z1)
+        a, b = b, a
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        oracle.ref_step(o, 0.5, a, b, 0, z1)
+        a, b = b, a
+    dt = time.perf_counter() - t0
+    cells = nx * ny * z1
+    mlups = cells * args.steps / dt / 1e6
+    sample = (f"z-planes [0,{z1}) of {nz} ({cells} cells) per step, {args.steps} steps; reference lbm_core "
+              f"(device_function.hpp) compiled for the host, OpenMP over z, {threads} threads")
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": round(mlups, 2), "unit": "MLUPS", "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt / args.steps * 1e3, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded sphere channel)", "config": {"workload": WORKLOAD, "cells": sc.n},
+        "cpu_baseline": {"value": round(mlups, 2), "unit": "MLUPS", "cores": threads, "kind": "reference",
+                         "sample": sample},
+        "e2e": {"value": round(mlups, 2), "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--err-steps", type=int, default=1000)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be at least 3")
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

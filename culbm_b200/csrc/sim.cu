@@ -11,6 +11,7 @@
 #include <filesystem>
 #include <fstream>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "sim_internal.cuh"
@@ -53,11 +54,6 @@ culbm_status cuda_fail(cudaError_t e, const char* what, const char* file, int li
 
 // ------------------------------------------------------------ utilities ---
 
-template <typename S>
-struct Tag {
-    using type = S;
-};
-
 // Calls f(Tag<S>{}) for the storage type of sim.
 template <class F>
 culbm_status with_storage(const culbm_sim* s, F&& f)
@@ -76,6 +72,8 @@ StepArgs<S, typename ArithOf<S>::type> make_args(const culbm_sim* s, int src, in
 {
     using R = typename ArithOf<S>::type;
     StepArgs<S, R> a{};
+    long long stride = s->n;
+    if (is_blocked(s->cfg)) tiles_view(s, &a.ring_nz, &a.ring_off, &stride);
     a.dom = s->dom;
     a.ops = s->d_ops;
     a.rho = s->d_mac[0];
@@ -86,8 +84,8 @@ StepArgs<S, typename ArithOf<S>::type> make_args(const culbm_sim* s, int src, in
     S* b0 = static_cast<S*>(s->d_pop[src]);
     S* b1 = static_cast<S*>(s->d_pop[dst]);
     for (int d = 0; d < 27; ++d) {
-        a.src.p[d] = b0 + static_cast<long long>(d) * s->n;
-        a.dst.p[d] = b1 + static_cast<long long>(d) * s->n;
+        a.src.p[d] = b0 + static_cast<long long>(d) * stride;
+        a.dst.p[d] = b1 + static_cast<long long>(d) * stride;
     }
     a.edge = static_cast<S*>(s->d_edge);
     a.el = s->el;
@@ -99,7 +97,20 @@ int current_layout(const culbm_sim* s)
 {
     if (s->cfg.stream_policy == CULBM_STREAM_INPLACE && !is_blocked(s->cfg))
         return s->aa_phase == 0 ? LAYOUT_AA_A : LAYOUT_AA_B;
+    if (is_blocked(s->cfg) && s->cfg.use_ring_ddf_buf) return LAYOUT_PULL_RING;
     return LAYOUT_PULL;
+}
+
+// Calls f(std::integral_constant<int, layout>{}).
+template <class F>
+void with_layout(int layout, F&& f)
+{
+    switch (layout) {
+        case LAYOUT_AA_A: f(std::integral_constant<int, LAYOUT_AA_A>{}); break;
+        case LAYOUT_AA_B: f(std::integral_constant<int, LAYOUT_AA_B>{}); break;
+        case LAYOUT_PULL_RING: f(std::integral_constant<int, LAYOUT_PULL_RING>{}); break;
+        default: f(std::integral_constant<int, LAYOUT_PULL>{}); break;
+    }
 }
 
 size_t storage_bytes(int storage)
@@ -207,6 +218,7 @@ template <typename S>
 culbm_status fill_rest(culbm_sim* s)
 {
     using R = typename ArithOf<S>::type;
+    if (is_blocked(s->cfg)) return tiles_reset(s);
     const dim3 g = cell_grid(s->dom), b = cell_block();
     for (int k = 0; k < s->npop; ++k) {
         auto a = make_args<S>(s, k, k);
@@ -281,6 +293,7 @@ culbm_status validate_config(const culbm_config& c)
         for (int k = 0; k < 3; ++k)
             if (1ull * c.block_dim[k] * c.grid_dim[k] != c.domain_dim[k])
                 return fail(CULBM_ERR_INVALID_ARGUMENT, "Dimension of domain doesn't match computation grid!");
+    if (is_blocked(c)) return validate_blocking(c);
     return CULBM_OK;
 }
 
@@ -552,12 +565,9 @@ culbm_status culbm_moments(culbm_sim* sim)
         auto a = make_args<S>(sim, sim->cur, sim->cur);
         const dim3 g = cell_grid(sim->dom), b = cell_block();
         float* const* m = sim->d_mac;
-        if (layout == LAYOUT_PULL)
-            k_moments<LAYOUT_PULL, S, R><<<g, b, 0, sim->stream>>>(a, sim->d_flag, m[0], m[1], m[2], m[3]);
-        else if (layout == LAYOUT_AA_A)
-            k_moments<LAYOUT_AA_A, S, R><<<g, b, 0, sim->stream>>>(a, sim->d_flag, m[0], m[1], m[2], m[3]);
-        else
-            k_moments<LAYOUT_AA_B, S, R><<<g, b, 0, sim->stream>>>(a, sim->d_flag, m[0], m[1], m[2], m[3]);
+        with_layout(layout, [&](auto L) {
+            k_moments<decltype(L)::value, S, R><<<g, b, 0, sim->stream>>>(a, sim->d_flag, m[0], m[1], m[2], m[3]);
+        });
         CULBM_CUDA(cudaGetLastError());
         return CULBM_OK;
     });
@@ -619,12 +629,9 @@ culbm_status culbm_get_pulled_ddf(culbm_sim* sim, void* host_out, int32_t out_ty
         auto launch = [&](auto tt) {
             using T = typename decltype(tt)::type;
             T* o = static_cast<T*>(d_out);
-            if (layout == LAYOUT_PULL)
-                k_export_pulled<LAYOUT_PULL, S, R, T><<<g, b, 0, sim->stream>>>(a, o);
-            else if (layout == LAYOUT_AA_A)
-                k_export_pulled<LAYOUT_AA_A, S, R, T><<<g, b, 0, sim->stream>>>(a, o);
-            else
-                k_export_pulled<LAYOUT_AA_B, S, R, T><<<g, b, 0, sim->stream>>>(a, o);
+            with_layout(layout, [&](auto L) {
+                k_export_pulled<decltype(L)::value, S, R, T><<<g, b, 0, sim->stream>>>(a, o);
+            });
         };
         if (out_type == 0) launch(Tag<float>{});
         else launch(Tag<double>{});
@@ -646,7 +653,8 @@ culbm_status culbm_set_ddf(culbm_sim* sim, const void* host_in, int32_t in_type)
     const size_t bytes = 27ull * sim->n * tsize;
     void* d_in = nullptr;
     CULBM_CUDA(cudaMalloc(&d_in, bytes));
-    const bool aa = current_layout(sim) != LAYOUT_PULL;
+    const int layout = current_layout(sim);
+    const bool aa = layout == LAYOUT_AA_A || layout == LAYOUT_AA_B;
     culbm_status st = with_storage(sim, [&](auto tag) -> culbm_status {
         using S = typename decltype(tag)::type;
         using R = typename ArithOf<S>::type;
@@ -659,6 +667,8 @@ culbm_status culbm_set_ddf(culbm_sim* sim, const void* host_in, int32_t in_type)
             const T* in = static_cast<const T*>(d_in);
             if (aa)
                 k_import<LAYOUT_AA_A, S, R, T><<<g, b, 0, sim->stream>>>(a, in);
+            else if (layout == LAYOUT_PULL_RING)
+                k_import<LAYOUT_PULL_RING, S, R, T><<<g, b, 0, sim->stream>>>(a, in);
             else
                 k_import<LAYOUT_PULL, S, R, T><<<g, b, 0, sim->stream>>>(a, in);
         };
@@ -684,12 +694,9 @@ culbm_status culbm_mass_momentum(culbm_sim* sim, double out[4])
         auto a = make_args<S>(sim, sim->cur, sim->cur);
         double* part = sim->d_red;
         const int nb = sim->red_blocks;
-        if (layout == LAYOUT_PULL)
-            k_mass_momentum<LAYOUT_PULL, S, R><<<nb, 256, 0, sim->stream>>>(a, part);
-        else if (layout == LAYOUT_AA_A)
-            k_mass_momentum<LAYOUT_AA_A, S, R><<<nb, 256, 0, sim->stream>>>(a, part);
-        else
-            k_mass_momentum<LAYOUT_AA_B, S, R><<<nb, 256, 0, sim->stream>>>(a, part);
+        with_layout(layout, [&](auto L) {
+            k_mass_momentum<decltype(L)::value, S, R><<<nb, 256, 0, sim->stream>>>(a, part);
+        });
         CULBM_CUDA(cudaGetLastError());
         k_sum_partials<<<1, 32, 0, sim->stream>>>(part, nb, part + 4 * nb);
         CULBM_CUDA(cudaGetLastError());
@@ -742,5 +749,6 @@ extern "C" culbm_status culbm_get_info(culbm_sim* sim, culbm_info* info)
     info->inner_loop = sim->cfg.inner_loop;
     info->kernel_launches_per_step_x1000 =
         sim->launched_steps ? static_cast<uint32_t>(1000ull * sim->launches / sim->launched_steps) : 0;
+    tiles_info(sim, info);
     return CULBM_OK;
 }

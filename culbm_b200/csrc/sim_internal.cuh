@@ -82,11 +82,25 @@ inline dim3 cell_grid(const Domain& D)
     return dim3((D.nx + 31) / 32, (D.ny + 7) / 8, D.nz);
 }
 
+template <typename S>
+struct Tag {
+    using type = S;
+};
+
+// Device allocation counted in sim->device_bytes (sim.cu).
+culbm_status dev_alloc(culbm_sim* s, void** p, size_t bytes, const char* what);
+
 // Blocked-policy entry points (tile_runtime.cu).
+culbm_status validate_blocking(const culbm_config& cfg);
 culbm_status tiles_create(culbm_sim* sim);
 void tiles_destroy(culbm_sim* sim);
 culbm_status tiles_upload_flags(culbm_sim* sim, const uint32_t* host_flag);
+culbm_status tiles_reset(culbm_sim* sim);
 culbm_status tiles_step(culbm_sim* sim, uint32_t nsteps);
+// Where the newest global state lives: ring planes (0 = plain buffers), its
+// z offset in the ring, and the per-direction stride in elements.
+void tiles_view(const culbm_sim* sim, int* ring_nz, int* offz, long long* stride);
+void tiles_info(const culbm_sim* sim, culbm_info* info);
 bool is_blocked(const culbm_config& cfg);
 
 }  // namespace culbm

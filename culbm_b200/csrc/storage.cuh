@@ -21,16 +21,20 @@ constexpr float kHalfInvScale = 1.0f / 32768.0f;
 
 template <typename S, typename R> struct Cvt;
 
+// ld_cs / st_cs: streaming ("evict first") variants for data touched once per
+// pass, so that it does not push L2-resident tile data out.
 template <> struct Cvt<float, float> {
     static __device__ __forceinline__ float ld(const float* p) { return *p; }
     static __device__ __forceinline__ void st(float* p, float v) { *p = v; }
-    static __host__ __device__ __forceinline__ float to(float v) { return v; }
+    static __device__ __forceinline__ float ld_cs(const float* p) { return __ldcs(p); }
+    static __device__ __forceinline__ void st_cs(float* p, float v) { __stcs(p, v); }
 };
 
 template <> struct Cvt<double, double> {
     static __device__ __forceinline__ double ld(const double* p) { return *p; }
     static __device__ __forceinline__ void st(double* p, double v) { *p = v; }
-    static __host__ __device__ __forceinline__ double to(double v) { return v; }
+    static __device__ __forceinline__ double ld_cs(const double* p) { return __ldcs(p); }
+    static __device__ __forceinline__ void st_cs(double* p, double v) { __stcs(p, v); }
 };
 
 template <> struct Cvt<__half, float> {
@@ -42,11 +46,21 @@ template <> struct Cvt<__half, float> {
     {
         *p = __float2half_rn(__fmul_rn(v, kHalfScale));
     }
+    static __device__ __forceinline__ float ld_cs(const __half* p)
+    {
+        return __fmul_rn(__half2float(__ldcs(p)), kHalfInvScale);
+    }
+    static __device__ __forceinline__ void st_cs(__half* p, float v)
+    {
+        __stcs(p, __float2half_rn(__fmul_rn(v, kHalfScale)));
+    }
 };
 
 template <> struct Cvt<__nv_bfloat16, float> {
     static __device__ __forceinline__ float ld(const __nv_bfloat16* p) { return __bfloat162float(*p); }
     static __device__ __forceinline__ void st(__nv_bfloat16* p, float v) { *p = __float2bfloat16_rn(v); }
+    static __device__ __forceinline__ float ld_cs(const __nv_bfloat16* p) { return __bfloat162float(__ldcs(p)); }
+    static __device__ __forceinline__ void st_cs(__nv_bfloat16* p, float v) { __stcs(p, __float2bfloat16_rn(v)); }
 };
 
 // Arithmetic type used with each storage type.

@@ -9,13 +9,17 @@
 // parameters (constant bank), so no per-direction 64-bit offset is kept in
 // registers.
 //
-// Edge semantics: the reference's pull clamps the neighbour offset to 0 at
-// the domain boundary (kernel.cu:2506-2511), so a boundary cell re-reads its
-// own previous post-collision population for directions whose source is
-// outside.  The pull kernel does the same.  The in-place kernels reproduce it
-// bit for bit with a small side buffer ("edge buffer") that holds, for each
-// boundary cell and each such direction, the value the clamp would read.
+// Edge semantics: the reference's pull clamps each neighbour offset component
+// to 0 at the domain boundary (kernel.cu:2506-2511), so a boundary cell pulls
+// a direction whose source is outside from the source with the offending
+// components replaced by its own (itself for face-normal directions, a
+// neighbour along the face otherwise).  The pull kernel does the same.  The
+// in-place kernels reproduce it bit for bit with a small side buffer ("edge
+// buffer") that holds, for each boundary cell and each such direction, the
+// post-collision population of that clamped source.
 #pragma once
+
+#include <type_traits>
 
 #include "d3q27.cuh"
 #include "storage.cuh"
@@ -54,6 +58,8 @@ struct StepArgs {
     Pops<S> dst;   // pull: write buffer.  in-place: same buffer as src.
     S* edge;       // in-place only
     EdgeLayout el;
+    int ring_nz;   // LAYOUT_PULL_RING: planes in the ring buffer
+    int ring_off;  // LAYOUT_PULL_RING: ring plane of domain plane z = 0
 };
 
 __device__ __forceinline__ int nb_off(const Domain& D, int d)
@@ -85,15 +91,62 @@ __device__ __forceinline__ long long edge_slot(const Domain& D, const EdgeLayout
     return L.off[sz < 0 ? 4 : 5] + (long long)j * D.nx * D.ny + x + (long long)D.nx * y;
 }
 
+// The reference clamps a pull per axis: a component of x - c_d that leaves
+// the domain is replaced by x's own component, the others are kept.  So the
+// clamped source of (y, d) is s = clamp(y - c_d), usually a neighbour of y and
+// not y itself.  For a source cell s and direction d this visits every
+// boundary cell y != s + c_d whose clamped pull in direction d reads s: take
+// y = s + c_d and put back s's own component on any non-empty subset of the
+// axes along which s - c_d leaves the domain.
+template <int D_, class F>
+__device__ __forceinline__ void for_each_clamp_reader(const Domain& D, int sx, int sy, int sz, F&& fn)
+{
+    constexpr int cx = cx_of(D_), cy = cy_of(D_), cz = cz_of(D_);
+    const bool kx = cx != 0 && (unsigned)(sx - cx) >= (unsigned)D.nx;
+    const bool ky = cy != 0 && (unsigned)(sy - cy) >= (unsigned)D.ny;
+    const bool kz = cz != 0 && (unsigned)(sz - cz) >= (unsigned)D.nz;
+#pragma unroll
+    for (int m = 1; m < 8; ++m) {
+        if ((m & 1) && !kx) continue;
+        if ((m & 2) && !ky) continue;
+        if ((m & 4) && !kz) continue;
+        const int yx = (m & 1) ? sx : sx + cx;
+        const int yy = (m & 2) ? sy : sy + cy;
+        const int yz = (m & 4) ? sz : sz + cz;
+        if (inside(D, yx, yy, yz)) fn(yx, yy, yz);
+    }
+}
+
+// Compile-time loop over the 27 directions: f(std::integral_constant<int, d>).
+template <int D_ = 0, class F>
+__device__ __forceinline__ void for_dirs(F&& f)
+{
+    if constexpr (D_ < 27) {
+        f(std::integral_constant<int, D_>{});
+        for_dirs<D_ + 1>(f);
+    }
+}
+
 // How the current state stores "the population f_d that cell x pulls next":
 //   LAYOUT_PULL  standard: post-collision f*_d(y) at [d][y]; pull from x - c_d,
-//                clamped to x at the boundary (pull double buffer, tiles).
+//                clamped per axis at the boundary (pull double buffer, tiles).
 //   LAYOUT_AA_A  reversed own: f*_d(y) at [26-d][y]; pull from x - c_d,
 //                clamped values from the edge buffer (in-place, after an even
 //                step and at start).
 //   LAYOUT_AA_B  streamed: the pulled value already sits at [d][x]
 //                (in-place, after an odd step).
-enum Layout : int { LAYOUT_PULL = 0, LAYOUT_AA_A = 1, LAYOUT_AA_B = 2 };
+//   LAYOUT_PULL_RING  standard, in the z-rotating ring buffer of the blocked
+//                in-place policy: domain plane z lives at ring plane
+//                (z + ring_off) mod ring_nz.
+enum Layout : int { LAYOUT_PULL = 0, LAYOUT_AA_A = 1, LAYOUT_AA_B = 2, LAYOUT_PULL_RING = 3 };
+
+template <typename S, typename R>
+__device__ __forceinline__ long long ring_index(const StepArgs<S, R>& a, int x, int y, int z)
+{
+    int pz = z + a.ring_off;
+    if (pz >= a.ring_nz) pz -= a.ring_nz;
+    return (long long)pz * a.dom.nxy + (long long)y * a.dom.nx + x;
+}
 
 template <int LAYOUT, typename S, typename R>
 __device__ __forceinline__ void load_pulled(const StepArgs<S, R>& a, int x, int y, int z, int i, bool edge, R* f)
@@ -109,6 +162,15 @@ __device__ __forceinline__ void load_pulled(const StepArgs<S, R>& a, int x, int 
             const int oy = cy_of(d) == 1 ? ndy : cy_of(d) == -1 ? pdy : 0;
             const int oz = cz_of(d) == 1 ? ndz : cz_of(d) == -1 ? pdz : 0;
             f[d] = Cvt<S, R>::ld(a.src.p[d] + (i + ox + oy + oz));
+        }
+    } else if (LAYOUT == LAYOUT_PULL_RING) {
+#pragma unroll
+        for (int d = 0; d < 27; ++d) {
+            int sx = x - cx_of(d), sy = y - cy_of(d), sz = z - cz_of(d);
+            if ((unsigned)sx >= (unsigned)D.nx) sx = x;
+            if ((unsigned)sy >= (unsigned)D.ny) sy = y;
+            if ((unsigned)sz >= (unsigned)D.nz) sz = z;
+            f[d] = Cvt<S, R>::ld(a.src.p[d] + ring_index(a, sx, sy, sz));
         }
     } else if (LAYOUT == LAYOUT_AA_A) {
         if (!edge) {
@@ -171,8 +233,9 @@ __global__ void __launch_bounds__(256) k_pull_step(const __grid_constant__ StepA
 // slot of x - c_d and pushes its post-collision f_d into slot d of x + c_d.
 // Cell x reads and writes exactly the same set of locations, so no other
 // thread touches them.  Boundary cells take clamped values from the edge
-// buffer and also write f_d into their own slot d when x - c_d is outside
-// (the value the clamped pull of the next step expects).
+// buffer, and a cell that is the clamped source of boundary cells y (see
+// for_each_clamp_reader) also writes f_d into slot d of each such y: nobody
+// else reads or writes that slot during the step, and y reads it next step.
 template <typename S, typename R>
 __global__ void __launch_bounds__(256) k_aa_odd(const __grid_constant__ StepArgs<S, R> a)
 {
@@ -194,22 +257,22 @@ __global__ void __launch_bounds__(256) k_aa_odd(const __grid_constant__ StepArgs
 #pragma unroll
             for (int d = 0; d < 27; ++d) Cvt<S, R>::st(a.dst.p[d] + (c.i + nb_off(D, d)), f[d]);
         } else {
-#pragma unroll
-            for (int d = 0; d < 27; ++d) {
-                const int cx = cx_of(d), cy = cy_of(d), cz = cz_of(d);
-                if (inside(D, c.x + cx, c.y + cy, c.z + cz))
+            for_dirs([&](auto dd) {
+                constexpr int d = decltype(dd)::value;
+                if (inside(D, c.x + cx_of(d), c.y + cy_of(d), c.z + cz_of(d)))
                     Cvt<S, R>::st(a.dst.p[d] + (c.i + nb_off(D, d)), f[d]);
-                if (!inside(D, c.x - cx, c.y - cy, c.z - cz))
-                    Cvt<S, R>::st(a.dst.p[d] + c.i, f[d]);
-            }
+                for_each_clamp_reader<d>(D, c.x, c.y, c.z, [&](int yx, int yy, int yz) {
+                    Cvt<S, R>::st(a.dst.p[d] + (yx + D.nx * (yy + D.ny * yz)), f[d]);
+                });
+            });
         }
     }
 }
 
 // In-place even step (layout B -> A): own slots in, reversed own slots out.
-// Boundary cells also file f_d into the edge buffer for every d whose source
-// x - c_d is outside: the next odd step's clamped pull reads it there, because
-// slot 26-d of x is overwritten by x + c_d during that step.
+// A cell that is the clamped source of boundary cells y also files f_d into
+// the edge-buffer slot of (y, d): the next odd step's clamped pull of y reads
+// it there, because slot 26-d of the source is overwritten during that step.
 template <typename S, typename R>
 __global__ void __launch_bounds__(256) k_aa_even(const __grid_constant__ StepArgs<S, R> a)
 {
@@ -229,10 +292,12 @@ __global__ void __launch_bounds__(256) k_aa_even(const __grid_constant__ StepArg
 #pragma unroll
         for (int d = 0; d < 27; ++d) Cvt<S, R>::st(a.dst.p[26 - d] + c.i, f[d]);
         if (op & OP_EDGE) {
-#pragma unroll
-            for (int d = 0; d < 27; ++d)
-                if (!inside(D, c.x - cx_of(d), c.y - cy_of(d), c.z - cz_of(d)))
-                    Cvt<S, R>::st(a.edge + edge_slot(D, a.el, c.x, c.y, c.z, d), f[d]);
+            for_dirs([&](auto dd) {
+                constexpr int d = decltype(dd)::value;
+                for_each_clamp_reader<d>(D, c.x, c.y, c.z, [&](int yx, int yy, int yz) {
+                    Cvt<S, R>::st(a.edge + edge_slot(D, a.el, yx, yy, yz, d), f[d]);
+                });
+            });
         }
     }
 }
@@ -272,7 +337,8 @@ __global__ void __launch_bounds__(256) k_export_pulled(const __grid_constant__ S
 }
 
 // Import a state given as post-collision populations in the standard layout
-// in[d*n + i] (T = float or double) into LAYOUT_PULL (dst) or LAYOUT_AA_A.
+// in[d*n + i] (T = float or double) into LAYOUT_PULL / LAYOUT_PULL_RING (dst)
+// or LAYOUT_AA_A.
 template <int LAYOUT, typename S, typename R, typename T>
 __global__ void __launch_bounds__(256) k_import(const __grid_constant__ StepArgs<S, R> a, const T* in)
 {
@@ -284,10 +350,18 @@ __global__ void __launch_bounds__(256) k_import(const __grid_constant__ StepArgs
         const R v = R(in[(long long)d * D.n + c.i]);
         if (LAYOUT == LAYOUT_PULL) {
             Cvt<S, R>::st(a.dst.p[d] + c.i, v);
+        } else if (LAYOUT == LAYOUT_PULL_RING) {
+            Cvt<S, R>::st(a.dst.p[d] + ring_index(a, c.x, c.y, c.z), v);
         } else {
             Cvt<S, R>::st(a.dst.p[26 - d] + c.i, v);
-            if (!inside(D, c.x - cx_of(d), c.y - cy_of(d), c.z - cz_of(d)))
-                Cvt<S, R>::st(a.edge + edge_slot(D, a.el, c.x, c.y, c.z, d), v);
+            int sx = c.x - cx_of(d), sy = c.y - cy_of(d), sz = c.z - cz_of(d);
+            if (!inside(D, sx, sy, sz)) {
+                if ((unsigned)sx >= (unsigned)D.nx) sx = c.x;
+                if ((unsigned)sy >= (unsigned)D.ny) sy = c.y;
+                if ((unsigned)sz >= (unsigned)D.nz) sz = c.z;
+                const R w = R(in[(long long)d * D.n + sx + D.nx * (sy + D.ny * sz)]);
+                Cvt<S, R>::st(a.edge + edge_slot(D, a.el, c.x, c.y, c.z, d), w);
+            }
         }
     }
 }

@@ -1,17 +1,432 @@
-// Blocked (L2 temporal blocking) policies.  Placeholder until the tile engine
-// lands: blocked configurations are rejected at create time.
+// Host side of the blocked policies (optPolicy 1, 2, 3): tile geometry, tile
+// buffers kept in L2 by an access-policy window, the per-round launch
+// sequence (replayed as one CUDA graph), and the ring-buffer option.
+//
+// Replaces the reference's haloBlocking*Run lambdas and initBlockingFlag /
+// initRingDDFBuf / mapGlobalMem2PersistL2
+// (src/simulator/single_dev_expt/simulator_expt_platform.cu:120-305, 608-942).
+// optPolicy 1 (static L2) and 2 (L1/L2 mixed) run on the same L2 tile engine
+// as 3 (dynamic L2): all three give the plain step's results bit for bit, so
+// they differ only in speed, and on this GPU the graph-replayed L2 engine is
+// the one kept.
+#include <algorithm>
+#include <cstring>
+#include <string>
+#include <vector>
+
 #include "sim_internal.cuh"
+#include "tile_kernels.cuh"
 
 namespace culbm {
 
+namespace {
+
+// Blocking geometry, restating blocking_core::validBlkAxisConfig,
+// calcBlkNum and calcValidPrev (src/blocking_core/blocking_alogrithm.hpp:7-41)
+// with the unsigned arithmetic the reference instantiates them with.
+bool valid_blk_axis(uint32_t dom, uint32_t blk, uint32_t it)
+{
+    if (blk < dom && blk + 1 <= it) return false;
+    if (2 * (blk + 1 - it) < dom && blk + 2 <= it) return false;
+    return true;
+}
+
+uint32_t blk_num(uint32_t dom, uint32_t blk, uint32_t it)
+{
+    if (dom <= blk) return 1;
+    if (dom <= 2 * (blk + 1 - it)) return 2;
+    const uint32_t num = dom - 2 * (blk + 1 - it), den = blk + 2 - 2 * it;
+    return 2 + (num + den - 1) / den;
+}
+
+int32_t valid_prev(int32_t idx, int32_t blk, int32_t num, int32_t it, int32_t dom)
+{
+    if (idx == num) return dom;
+    if (idx == 0) return 0;
+    return (blk + 1 - it) + (idx - 1) * (blk + 2 - 2 * it);
+}
+
+struct TileGeom {
+    int org[3];
+    int vlo[3], vhi[3];
+};
+
+}  // namespace
+
+struct TileState {
+    int B[3] = {0, 0, 0};
+    int nt[3] = {1, 1, 1};
+    int I = 1;
+    long long tile_n = 0;
+    std::vector<TileGeom> tiles;
+    void* d_tile = nullptr;      // one block: tile buffer 0 (and 1 for pull)
+    RoundState* d_rs = nullptr;
+    RoundState h_rs{};
+    int ring_nz = 0, ring_step = 0;
+    long long gstride = 0;
+    cudaGraphExec_t graph = nullptr;
+    int graph_I = 0;
+    bool window = false;
+    cudaAccessPolicyWindow apw{};
+    size_t persist_bytes = 0;
+};
+
 bool is_blocked(const culbm_config& cfg) { return cfg.opt_policy != CULBM_OPT_NONE; }
 
-culbm_status tiles_create(culbm_sim*)
+namespace {
+
+template <typename S>
+struct TileLauncher {
+    using R = typename ArithOf<S>::type;
+    culbm_sim* s;
+    TileState* ts;
+
+    TileArgs<S, R> base_args() const
+    {
+        TileArgs<S, R> a{};
+        a.dom = s->dom;
+        a.bx = ts->B[0];
+        a.by = ts->B[1];
+        a.bz = ts->B[2];
+        a.bxy = ts->B[0] * ts->B[1];
+        a.ops = s->d_ops;
+        a.rho = s->d_mac[0];
+        a.vx = s->d_mac[1];
+        a.vy = s->d_mac[2];
+        a.vz = s->d_mac[3];
+        a.inv_tau = static_cast<R>(s->cfg.inv_tau);
+        a.g.base[0] = static_cast<S*>(s->d_pop[0]);
+        a.g.base[1] = static_cast<S*>(s->d_pop[ts->ring_nz ? 0 : 1]);
+        a.g.stride = ts->gstride;
+        a.g.ring_nz = ts->ring_nz;
+        a.g.ring_step = ts->ring_step;
+        S* t = static_cast<S*>(ts->d_tile);
+        for (int d = 0; d < 27; ++d) {
+            a.t0.p[d] = t + d * ts->tile_n;
+            a.t1.p[d] = t + (27 + d) * ts->tile_n;
+        }
+        a.edge = static_cast<S*>(s->d_edge);
+        a.el = s->el;
+        a.rs = ts->d_rs;
+        return a;
+    }
+
+    template <typename K>
+    culbm_status launch(K kernel, const TileArgs<S, R>& a)
+    {
+        cudaLaunchConfig_t lc{};
+        lc.gridDim = dim3((ts->B[0] + 31) / 32, (ts->B[1] + 7) / 8, ts->B[2]);
+        lc.blockDim = dim3(32, 8, 1);
+        lc.stream = s->stream;
+        cudaLaunchAttribute attr[1];
+        if (ts->window) {
+            attr[0].id = cudaLaunchAttributeAccessPolicyWindow;
+            attr[0].val.accessPolicyWindow = ts->apw;
+            lc.attrs = attr;
+            lc.numAttrs = 1;
+        }
+        CULBM_CUDA(cudaLaunchKernelEx(&lc, kernel, a));
+        s->launches += 1;
+        return CULBM_OK;
+    }
+
+    // All tiles for one round of k <= I steps, then the round-state advance.
+    culbm_status round(int k)
+    {
+        const bool hint = s->cfg.cache_hints != 0;
+        const bool inplace = s->cfg.stream_policy == CULBM_STREAM_INPLACE;
+        TileArgs<S, R> a = base_args();
+        for (const TileGeom& g : ts->tiles) {
+            a.ox = g.org[0];
+            a.oy = g.org[1];
+            a.oz = g.org[2];
+            for (int q = 0; q < 3; ++q) {
+                a.vlo[q] = g.vlo[q];
+                a.vhi[q] = g.vhi[q];
+            }
+            if (inplace) {
+                if (k == 1) {
+                    CULBM_TRY(hint ? launch(k_tile_aa_first<S, R, true, true>, a)
+                                   : launch(k_tile_aa_first<S, R, true, false>, a));
+                    continue;
+                }
+                CULBM_TRY(hint ? launch(k_tile_aa_first<S, R, false, true>, a)
+                               : launch(k_tile_aa_first<S, R, false, false>, a));
+                for (int j = 2; j < k; ++j) {
+                    if (j % 2 == 0) CULBM_TRY(launch(k_tile_aa_odd<S, R>, a));
+                    else CULBM_TRY(launch(k_tile_aa_even<S, R>, a));
+                }
+                if (k % 2 == 0)
+                    CULBM_TRY(hint ? launch(k_tile_aa_last<LAYOUT_AA_A, S, R, true>, a)
+                                   : launch(k_tile_aa_last<LAYOUT_AA_A, S, R, false>, a));
+                else
+                    CULBM_TRY(hint ? launch(k_tile_aa_last<LAYOUT_AA_B, S, R, true>, a)
+                                   : launch(k_tile_aa_last<LAYOUT_AA_B, S, R, false>, a));
+            } else {
+                if (k == 1) {
+                    CULBM_TRY(hint ? launch(k_tile_pull_first<S, R, true, true>, a)
+                                   : launch(k_tile_pull_first<S, R, true, false>, a));
+                    continue;
+                }
+                TileArgs<S, R> b = a;
+                CULBM_TRY(hint ? launch(k_tile_pull_first<S, R, false, true>, b)
+                               : launch(k_tile_pull_first<S, R, false, false>, b));
+                for (int j = 2; j < k; ++j) {
+                    CULBM_TRY(launch(k_tile_pull_mid<S, R>, b));
+                    std::swap(b.t0, b.t1);
+                }
+                CULBM_TRY(hint ? launch(k_tile_pull_last<S, R, true>, b) : launch(k_tile_pull_last<S, R, false>, b));
+            }
+        }
+        k_tile_advance<<<1, 32, 0, s->stream>>>(ts->d_rs, ts->ring_nz, ts->ring_step);
+        CULBM_CUDA(cudaGetLastError());
+        s->launches += 1;
+        return CULBM_OK;
+    }
+};
+
+void host_advance(TileState* ts)
 {
-    return fail(CULBM_ERR_UNSUPPORTED, "L2 temporal blocking is not built yet");
+    if (ts->ring_nz) {
+        ts->h_rs.src_offz = ts->h_rs.dst_offz;
+        int o = ts->h_rs.dst_offz - ts->ring_step;
+        if (o < 0) o += ts->ring_nz;
+        ts->h_rs.dst_offz = o;
+    } else {
+        ts->h_rs.sel = 1 - ts->h_rs.sel;
+    }
 }
-void tiles_destroy(culbm_sim*) {}
+
+template <typename S>
+culbm_status tiles_step_typed(culbm_sim* s, uint32_t nsteps)
+{
+    TileState* ts = s->tiles;
+    TileLauncher<S> L{s, ts};
+    const uint32_t I = static_cast<uint32_t>(ts->I);
+    uint32_t full = nsteps / I;
+    const uint32_t rem = nsteps % I;
+    if (full > 0 && s->cfg.use_graphs) {
+        if (ts->graph == nullptr || ts->graph_I != ts->I) {
+            if (ts->graph) cudaGraphExecDestroy(ts->graph);
+            ts->graph = nullptr;
+            cudaGraph_t g = nullptr;
+            const uint64_t launches0 = s->launches;
+            CULBM_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+            const culbm_status st = L.round(ts->I);
+            const cudaError_t ce = cudaStreamEndCapture(s->stream, &g);
+            if (st != CULBM_OK) {
+                if (g) cudaGraphDestroy(g);
+                return st;
+            }
+            if (ce != cudaSuccess) return cuda_fail(ce, "cudaStreamEndCapture", __FILE__, __LINE__);
+            const cudaError_t ie = cudaGraphInstantiate(&ts->graph, g, 0);
+            cudaGraphDestroy(g);
+            if (ie != cudaSuccess) return cuda_fail(ie, "cudaGraphInstantiate", __FILE__, __LINE__);
+            ts->graph_I = ts->I;
+            s->launches = launches0;
+        }
+        const uint64_t per_round = ts->tiles.size() * static_cast<uint64_t>(ts->I) + 1;
+        for (uint32_t r = 0; r < full; ++r) {
+            CULBM_CUDA(cudaGraphLaunch(ts->graph, s->stream));
+            s->launches += per_round;
+            host_advance(ts);
+        }
+        full = 0;
+    }
+    for (uint32_t r = 0; r < full; ++r) {
+        CULBM_TRY(L.round(ts->I));
+        host_advance(ts);
+    }
+    if (rem) {
+        CULBM_TRY(L.round(static_cast<int>(rem)));
+        host_advance(ts);
+    }
+    s->cur = ts->h_rs.sel;
+    return CULBM_OK;
+}
+
+template <typename S>
+__global__ void k_fill_dirs(S* base, long long stride, typename ArithOf<S>::type rho)
+{
+    using R = typename ArithOf<S>::type;
+    R f[27];
+    equilibrium<R>(rho, R(0), R(0), R(0), f);
+    for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < stride;
+         j += (long long)gridDim.x * blockDim.x)
+#pragma unroll
+        for (int d = 0; d < 27; ++d) Cvt<S, R>::st(base + d * stride + j, f[d]);
+}
+
+}  // namespace
+
+culbm_status validate_blocking(const culbm_config& c)
+{
+    if (c.inner_loop < 1) return fail(CULBM_ERR_INVALID_ARGUMENT, "innerLoop must be at least 1");
+    const uint32_t I = static_cast<uint32_t>(c.inner_loop);
+    for (int k = 0; k < 3; ++k) {
+        const unsigned long long b = 1ull * c.block_dim[k] * c.grid_dim[k];
+        if (b > 65535) return fail(CULBM_ERR_INVALID_ARGUMENT, "tile extent blockDim*gridDim above 65535");
+        const uint32_t dom = c.domain_dim[k], B = static_cast<uint32_t>(b);
+        if (!valid_blk_axis(dom, B, I))
+            return fail(CULBM_ERR_INVALID_ARGUMENT, "<Domain Dimension, Blocking Dimension and InnerLoop> don't match!");
+        // The reference's check lets B + 2 - 2I <= 0 through when more than
+        // two tiles are needed, and calcBlkNum then divides by it.
+        if (dom > B && dom > 2 * (B + 1 - I) && static_cast<long long>(B) + 2 - 2ll * I <= 0)
+            return fail(CULBM_ERR_INVALID_ARGUMENT,
+                        "<Domain Dimension, Blocking Dimension and InnerLoop> don't match! (tile too small for innerLoop)");
+    }
+    if (c.use_ring_ddf_buf && 1ull * c.block_dim[2] * c.grid_dim[2] < I)
+        return fail(CULBM_ERR_INVALID_ARGUMENT, "ring buffer needs blockDim.z*gridDim.z >= innerLoop");
+    return CULBM_OK;
+}
+
+culbm_status tiles_create(culbm_sim* s)
+{
+    const culbm_config& c = s->cfg;
+    CULBM_TRY(validate_blocking(c));
+    TileState* ts = new TileState();
+    s->tiles = ts;
+    ts->I = c.inner_loop;
+    for (int k = 0; k < 3; ++k) ts->B[k] = static_cast<int>(c.block_dim[k] * c.grid_dim[k]);
+    const uint32_t I = static_cast<uint32_t>(ts->I);
+    for (int k = 0; k < 3; ++k) ts->nt[k] = static_cast<int>(blk_num(c.domain_dim[k], static_cast<uint32_t>(ts->B[k]), I));
+    for (int kz = 0; kz < ts->nt[2]; ++kz)
+        for (int ky = 0; ky < ts->nt[1]; ++ky)
+            for (int kx = 0; kx < ts->nt[0]; ++kx) {
+                TileGeom g{};
+                const int kk[3] = {kx, ky, kz};
+                for (int q = 0; q < 3; ++q) {
+                    const int dom = static_cast<int>(c.domain_dim[q]);
+                    g.vlo[q] = valid_prev(kk[q], ts->B[q], ts->nt[q], ts->I, dom);
+                    g.vhi[q] = valid_prev(kk[q] + 1, ts->B[q], ts->nt[q], ts->I, dom);
+                    g.org[q] = std::max(g.vlo[q] - (ts->I - 1), 0);
+                }
+                ts->tiles.push_back(g);
+            }
+    ts->tile_n = 1ll * ts->B[0] * ts->B[1] * ts->B[2];
+    const bool inplace = c.stream_policy == CULBM_STREAM_INPLACE;
+    const size_t tile_bytes = (inplace ? 1 : 2) * 27ull * ts->tile_n * s->esize;
+    void* p = nullptr;
+    CULBM_TRY(dev_alloc(s, &p, tile_bytes, "tile buffers"));
+    ts->d_tile = p;
+    CULBM_TRY(dev_alloc(s, &p, sizeof(RoundState), "round state"));
+    ts->d_rs = static_cast<RoundState*>(p);
+
+    if (c.use_ring_ddf_buf) {
+        // One global buffer of nz + (Bz - (I-1) + 1) planes; each round writes
+        // its result that many planes below its source, modulo the ring
+        // (simulator_expt_platform.cu:252-277, 749-846).
+        ts->ring_step = ts->B[2] - (ts->I - 1) + 1;
+        ts->ring_nz = s->dom.nz + ts->ring_step;
+        ts->gstride = 1ll * s->dom.nxy * ts->ring_nz;
+        CULBM_TRY(dev_alloc(s, &s->d_pop[0], 27ull * ts->gstride * s->esize, "ring population buffer"));
+        s->npop = 1;
+    } else {
+        ts->gstride = s->n;
+    }
+    if (inplace) {
+        const long long fx = 9ll * s->dom.ny * s->dom.nz, fy = 9ll * s->dom.nx * s->dom.nz, fz = 9ll * s->dom.nx * s->dom.ny;
+        s->el.off[0] = 0;
+        s->el.off[1] = fx;
+        s->el.off[2] = 2 * fx;
+        s->el.off[3] = 2 * fx + fy;
+        s->el.off[4] = 2 * fx + 2 * fy;
+        s->el.off[5] = 2 * fx + 2 * fy + fz;
+        s->edge_elems = 2 * (fx + fy + fz);
+        CULBM_TRY(dev_alloc(s, &s->d_edge, s->edge_elems * s->esize, "edge buffer"));
+    }
+
+    // Keep the tile buffers resident: persisting set-aside + access-policy
+    // window (the reference's mapGlobalMem2PersistL2, which queries device 0;
+    // here the selected device).
+    if (c.persist_l2) {
+        cudaDeviceProp prop{};
+        CULBM_CUDA(cudaGetDeviceProperties(&prop, s->dev));
+        if (prop.persistingL2CacheMaxSize > 0 && prop.accessPolicyMaxWindowSize > 0) {
+            const size_t setaside = std::min<size_t>(tile_bytes, static_cast<size_t>(prop.persistingL2CacheMaxSize));
+            const size_t win = std::min<size_t>(tile_bytes, static_cast<size_t>(prop.accessPolicyMaxWindowSize));
+            CULBM_CUDA(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, setaside));
+            ts->apw.base_ptr = ts->d_tile;
+            ts->apw.num_bytes = win;
+            ts->apw.hitRatio = static_cast<float>(std::min(1.0, static_cast<double>(setaside) / static_cast<double>(win)));
+            ts->apw.hitProp = cudaAccessPropertyPersisting;
+            ts->apw.missProp = cudaAccessPropertyStreaming;
+            ts->window = true;
+            ts->persist_bytes = setaside;
+        }
+    }
+    return CULBM_OK;
+}
+
+void tiles_destroy(culbm_sim* s)
+{
+    TileState* ts = s->tiles;
+    if (ts == nullptr) return;
+    if (ts->graph) cudaGraphExecDestroy(ts->graph);
+    cudaFree(ts->d_tile);
+    cudaFree(ts->d_rs);
+    if (ts->window) {
+        cudaCtxResetPersistingL2Cache();
+        cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, 0);
+    }
+    delete ts;
+    s->tiles = nullptr;
+}
+
 culbm_status tiles_upload_flags(culbm_sim*, const uint32_t*) { return CULBM_OK; }
-culbm_status tiles_step(culbm_sim*, uint32_t) { return fail(CULBM_ERR_UNSUPPORTED, "no tile engine"); }
+
+// Resets the round state and fills the global state with rest equilibrium.
+culbm_status tiles_reset(culbm_sim* s)
+{
+    TileState* ts = s->tiles;
+    ts->h_rs = RoundState{0, 0, ts->ring_nz ? s->dom.nz : 0, 0};
+    CULBM_CUDA(cudaMemcpyAsync(ts->d_rs, &ts->h_rs, sizeof(RoundState), cudaMemcpyHostToDevice, s->stream));
+    auto fill = [&](auto tag) -> culbm_status {
+        using S = typename decltype(tag)::type;
+        using R = typename ArithOf<S>::type;
+        for (int k = 0; k < s->npop; ++k) {
+            k_fill_dirs<S><<<1184, 256, 0, s->stream>>>(static_cast<S*>(s->d_pop[k]), ts->gstride, R(1));
+            CULBM_CUDA(cudaGetLastError());
+        }
+        return CULBM_OK;
+    };
+    switch (s->cfg.storage) {
+        case CULBM_STORAGE_F32: CULBM_TRY(fill(Tag<float>{})); break;
+        case CULBM_STORAGE_F16: CULBM_TRY(fill(Tag<__half>{})); break;
+        case CULBM_STORAGE_BF16: CULBM_TRY(fill(Tag<__nv_bfloat16>{})); break;
+        default: CULBM_TRY(fill(Tag<double>{})); break;
+    }
+    s->cur = 0;
+    return CULBM_OK;
+}
+
+culbm_status tiles_step(culbm_sim* s, uint32_t nsteps)
+{
+    switch (s->cfg.storage) {
+        case CULBM_STORAGE_F32: return tiles_step_typed<float>(s, nsteps);
+        case CULBM_STORAGE_F16: return tiles_step_typed<__half>(s, nsteps);
+        case CULBM_STORAGE_BF16: return tiles_step_typed<__nv_bfloat16>(s, nsteps);
+        default: return tiles_step_typed<double>(s, nsteps);
+    }
+}
+
+void tiles_view(const culbm_sim* s, int* ring_nz, int* offz, long long* stride)
+{
+    const TileState* ts = s->tiles;
+    *ring_nz = ts ? ts->ring_nz : 0;
+    *offz = ts ? ts->h_rs.src_offz : 0;
+    *stride = ts ? ts->gstride : s->n;
+}
+
+void tiles_info(const culbm_sim* s, culbm_info* info)
+{
+    const TileState* ts = s->tiles;
+    if (ts == nullptr) return;
+    for (int k = 0; k < 3; ++k) {
+        info->blocking_num[k] = static_cast<uint32_t>(ts->nt[k]);
+        info->blocking_dim[k] = static_cast<uint32_t>(ts->B[k]);
+    }
+    info->persisting_l2_bytes = ts->persist_bytes;
+}
 
 }  // namespace culbm

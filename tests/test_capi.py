@@ -98,3 +98,21 @@ def test_null_arguments(culbm):
     assert lib.culbm_create(None, None) == 1
     assert lib.culbm_step(None, 1) == 1
     assert lib.culbm_destroy(None) == 0
+
+
+@pytest.mark.parametrize("dims,tile,inner,needle", [
+    ((64, 64, 64), (4, 64, 64), 3, "don't match"),      # B + 2 - 2I <= 0 with more than two tiles
+    ((64, 64, 64), (8, 8, 8), 9, "don't match"),        # B + 1 <= I with B < dom (reference check)
+    ((64, 64, 64), (16, 16, 16), 0, "innerLoop"),
+])
+def test_invalid_blocking_rejected_before_device(culbm, dims, tile, inner, needle):
+    from culbm_b200 import _capi
+    cfg = _capi.default_config()
+    for k in range(3):
+        cfg.domain_dim[k] = dims[k]
+        cfg.block_dim[k] = tile[k]
+        cfg.grid_dim[k] = 1
+    cfg.stream_policy, cfg.opt_policy, cfg.inner_loop = 1, 3, inner
+    st, msg = _create(cfg)
+    assert st == 1, (st, msg)
+    assert needle in msg

@@ -1,0 +1,98 @@
+"""L2 temporal blocking (optPolicy 1, 2, 3): every blocked configuration must
+give the plain pull step's state bit for bit (GPU).
+
+The reference pins its (1,3)+ring path the same way: analysis/correctness/
+compare.sh requires bitwise-equal dumps against the plain pull.  Here the
+comparison is against the oracle's pull step, on full populations.
+"""
+import numpy as np
+import pytest
+
+from culbm_b200 import scenes as S
+
+pytestmark = pytest.mark.gpu
+
+
+def bits(a):
+    a = np.ascontiguousarray(a)
+    return a.view(np.uint32 if a.dtype == np.float32 else np.uint64)
+
+
+def oracle_pulled(orc, scene, inv_tau, nsteps, state0=None, dtype=np.float32):
+    f, r, ux, uy, uz = scene.arrays()
+    nx, ny, nz = scene.shape
+    o = orc.Scene(nx, ny, nz, f, r, ux, uy, uz)
+    return orc.pulled(o, orc.run(o, inv_tau, nsteps, dtype=dtype, state=state0))
+
+
+def run_blocked(culbm, scene, sp, op, tile, inner, nsteps, inv_tau=0.6, ring=False, state0=None, storage="fp32",
+                graphs=True, splits=None):
+    with culbm.Simulation(scene.shape, stream_policy=sp, opt_policy=op, inv_tau=inv_tau, inner_loop=inner,
+                          tile=tile, use_ring=ring, storage=storage, use_graphs=graphs) as sim:
+        sim.load_state(*scene.arrays())
+        if state0 is not None:
+            sim.set_ddf(state0)
+        for k in (splits or [nsteps]):
+            sim.step(k)
+        info = sim.info()
+        return sim.pulled_ddf(np.float64 if storage == "fp64" else np.float32), info
+
+
+CASES = [
+    # (stream, opt, ring, tile, innerLoop)
+    (1, 3, False, (16, 12, 10), 3),
+    (1, 3, True, (16, 12, 10), 3),
+    (1, 3, True, (37, 29, 9), 4),
+    (0, 3, False, (16, 12, 10), 3),
+    (0, 1, False, (16, 12, 10), 2),
+    (1, 1, False, (20, 16, 12), 5),
+    (0, 2, False, (37, 8, 23), 2),
+    (1, 3, False, (16, 12, 10), 1),
+    (0, 3, False, (16, 12, 10), 1),
+]
+
+
+@pytest.mark.parametrize("sp,op,ring,tile,inner", CASES)
+def test_blocked_equals_pull_default_flags(culbm, orc, sp, op, ring, tile, inner):
+    """Fluid everywhere: domain faces inside tiles exercise the per-axis clamp."""
+    sc = S.default_scene(37, 29, 23)
+    rng = np.random.default_rng(inner)
+    state0 = (0.01 * rng.standard_normal(27 * sc.n)).astype(np.float32)
+    nsteps = 2 * inner + 1 if inner > 1 else 3     # a remainder round when inner > 1
+    got, info = run_blocked(culbm, sc, sp, op, tile, inner, nsteps, state0=state0, ring=ring)
+    assert np.array_equal(bits(got), bits(oracle_pulled(orc, sc, 0.6, nsteps, state0)))
+    L = orc.lib()
+    assert info["blocking_num"] == tuple(int(L.orc_blk_num(d, b, inner)) for d, b in zip((37, 29, 23), tile))
+
+
+@pytest.mark.parametrize("sp,ring", [(1, False), (1, True), (0, False)])
+def test_blocked_channel_with_obstacle(culbm, orc, sp, ring):
+    """The reference's channel + cube scene, 3 rounds of innerLoop 5."""
+    sc = S.reference_channel_cube(48, 40, 36, 0.05)
+    got, _ = run_blocked(culbm, sc, sp, 3, (24, 20, 18), 5, 15, inv_tau=0.5, ring=ring)
+    assert np.array_equal(bits(got), bits(oracle_pulled(orc, sc, 0.5, 15)))
+
+
+def test_blocked_graphs_off_and_split_steps(culbm, orc):
+    sc = S.reference_channel(30, 20, 16, 0.05)
+    want = oracle_pulled(orc, sc, 0.5, 13)
+    for graphs, splits in ((False, [13]), (True, [4, 9]), (True, [1, 1, 11])):
+        got, _ = run_blocked(culbm, sc, 1, 3, (16, 12, 10), 3, 13, inv_tau=0.5, graphs=graphs, splits=splits)
+        assert np.array_equal(bits(got), bits(want)), (graphs, splits)
+
+
+def test_blocked_fp64_and_moments(culbm, orc):
+    sc = S.reference_channel(26, 18, 14, 0.05)
+    got, _ = run_blocked(culbm, sc, 1, 3, (14, 10, 8), 3, 9, inv_tau=0.5, storage="fp64")
+    assert np.array_equal(bits(got), bits(oracle_pulled(orc, sc, 0.5, 9, dtype=np.float64)))
+    f, r, ux, uy, uz = sc.arrays()
+    o = orc.Scene(26, 18, 14, f, r, ux, uy, uz)
+    want = orc.moments(o, orc.run(o, 0.5, 9))
+    for ring in (False, True):
+        with culbm.Simulation(sc.shape, stream_policy=1, opt_policy=3, inner_loop=3, tile=(14, 10, 8),
+                              use_ring=ring, inv_tau=0.5) as sim:
+            sim.load_state(f, r, ux, uy, uz)
+            sim.step(9)
+            sim.moments()
+            for k, w in zip(("rho", "vx", "vy", "vz"), want):
+                assert np.array_equal(bits(sim.field(k)), bits(w)), (ring, k)
