@@ -48,33 +48,60 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi SM clock / throttle sampling during the timed region."""
+    """SM clock and throttle-reason sampling (NVML, every 10 ms) during the
+    timed region; falls back to nvidia-smi when NVML is unavailable."""
 
-    FIELDS = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
-              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-              "clocks_event_reasons.sw_power_cap")
+    # NVML clocks-event-reason bits (nvml.h)
+    REASONS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown",
+               0x40: "hw_thermal_slowdown", 0x80: "hw_power_brake_slowdown"}
 
     def __init__(self, index=0):
         self.index = index
         self.samples = []
+        self.max_mhz = None
         self._stop = threading.Event()
         self._t = None
 
-    def _run(self):
+    def _run_nvml(self, nv):
+        h = nv.nvmlDeviceGetHandleByIndex(self.index)
+        self.max_mhz = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        while not self._stop.is_set():
+            sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+            try:
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+            except AttributeError:
+                r = nv.nvmlDeviceGetCurrentClocksThrottleReasons(h)
+            self.samples.append((float(sm), int(r)))
+            self._stop.wait(0.01)
+
+    def _run_smi(self):
+        q = "clocks.sm,clocks.max.sm,clocks_event_reasons.active"
         while not self._stop.is_set():
             try:
-                out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
                                       "--format=csv,noheader,nounits"], capture_output=True, text=True,
-                                     timeout=10).stdout.strip()
-                if out:
-                    self.samples.append([v.strip() for v in out.split(",")])
+                                     timeout=10).stdout.strip().split(",")
+                self.max_mhz = float(out[1])
+                self.samples.append((float(out[0]), int(out[2].strip(), 16)))
             except Exception:
                 pass
-            self._stop.wait(0.2)
+            self._stop.wait(0.05)
+
+    def _run(self):
+        try:
+            import pynvml as nv
+            nv.nvmlInit()
+            try:
+                self._run_nvml(nv)
+            finally:
+                nv.nvmlShutdown()
+        except Exception:
+            self._run_smi()
 
     def __enter__(self):
         self._t = threading.Thread(target=self._run, daemon=True)
         self._t.start()
+        time.sleep(0.05)
         return self
 
     def __exit__(self, *exc):
@@ -83,13 +110,11 @@ class ClockSampler:
 
     def summary(self):
         if not self.samples:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
-        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
-        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for s in self.samples for k in range(4) if "Active" in s[2 + k]})
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.samples)}
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["no samples"], "samples": 0}
+        sm = [s[0] for s in self.samples]
+        reasons = sorted({name for _, r in self.samples for bit, name in self.REASONS.items() if r & bit})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": self.max_mhz, "reasons": reasons,
+                "samples": len(self.samples)}
 
 
 def dist():
@@ -380,8 +405,8 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
-    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=50)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--err-steps", type=int, default=1000)
     args = ap.parse_args()

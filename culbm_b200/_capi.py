@@ -53,7 +53,8 @@ class Config(C.Structure):
         ("persist_l2", C.c_int32),
         ("cache_hints", C.c_int32),
         ("use_graphs", C.c_int32),
-        ("reserved", C.c_uint32 * 8),
+        ("kernel_variant", C.c_int32),
+        ("reserved", C.c_uint32 * 7),
     ]
 
 

@@ -233,6 +233,22 @@ culbm_status fill_rest(culbm_sim* s)
     return CULBM_OK;
 }
 
+// Row-staged odd kernels may need more than the default 48 KB of dynamic
+// shared memory (18 directions x a padded x-row).
+template <typename S>
+culbm_status enable_row_kernels(culbm_sim* s)
+{
+    using R = typename ArithOf<S>::type;
+    const int nxp = (s->dom.nx + 31) / 32 * 32;
+    if (nxp > 1024) return CULBM_OK;
+    const int smem = static_cast<int>(18ull * nxp * sizeof(R) + nxp);
+    if (nxp <= 512)
+        CULBM_CUDA(cudaFuncSetAttribute(k_aa_odd_rows<S, R, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    else
+        CULBM_CUDA(cudaFuncSetAttribute(k_aa_odd_rows<S, R, 1024>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    return CULBM_OK;
+}
+
 template <typename S>
 culbm_status plain_steps(culbm_sim* s, uint32_t nsteps)
 {
@@ -246,10 +262,20 @@ culbm_status plain_steps(culbm_sim* s, uint32_t nsteps)
             s->cur ^= 1;
         } else {
             auto a = make_args<S>(s, 0, 0);
-            if (s->aa_phase == 0)
-                k_aa_odd<S, R><<<g, b, 0, s->stream>>>(a);
-            else
+            if (s->aa_phase == 0) {
+                const int nxp = (s->dom.nx + 31) / 32 * 32;
+                if (s->cfg.kernel_variant == 0 && nxp <= 1024) {
+                    const size_t smem = 18ull * nxp * sizeof(R) + nxp;
+                    if (nxp <= 512)
+                        k_aa_odd_rows<S, R, 512><<<dim3(s->dom.ny, s->dom.nz), nxp, smem, s->stream>>>(a);
+                    else
+                        k_aa_odd_rows<S, R, 1024><<<dim3(s->dom.ny, s->dom.nz), nxp, smem, s->stream>>>(a);
+                } else {
+                    k_aa_odd<S, R><<<g, b, 0, s->stream>>>(a);
+                }
+            } else {
                 k_aa_even<S, R><<<g, b, 0, s->stream>>>(a);
+            }
             CULBM_CUDA(cudaGetLastError());
             s->aa_phase ^= 1;
         }
@@ -452,6 +478,7 @@ culbm_status culbm_create(const culbm_config* cfg, culbm_sim** out)
         s->red_blocks = 592;
         CULBM_TRY(dev_alloc(s, reinterpret_cast<void**>(&s->d_red), (4ull * s->red_blocks + 4) * sizeof(double),
                             "reduction scratch"));
+        if (inplace) CULBM_TRY(with_storage(s, [&](auto tag) { return enable_row_kernels<typename decltype(tag)::type>(s); }));
         if (blocked) CULBM_TRY(tiles_create(s));
         const float* none[4] = {nullptr, nullptr, nullptr, nullptr};
         CULBM_TRY(upload_state(s, nullptr, none));

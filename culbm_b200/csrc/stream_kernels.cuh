@@ -269,6 +269,80 @@ __global__ void __launch_bounds__(256) k_aa_odd(const __grid_constant__ StepArgs
     }
 }
 
+// Rows that receive direction d from row (y, z) in the odd step: the
+// streaming target row (y+cy, z+cz) and, at a y or z face, the rows whose
+// clamped pull reads row (y, z) (for_each_clamp_reader restricted to y, z).
+// Calls fn(Y, Z) for each of them.
+template <class F>
+__device__ __forceinline__ void for_each_row_target(const Domain& D, int y, int z, int cy, int cz, F&& fn)
+{
+    const bool y_norm = (unsigned)(y + cy) < (unsigned)D.ny;
+    const bool y_clamp = cy != 0 && (unsigned)(y - cy) >= (unsigned)D.ny;
+    const bool z_norm = (unsigned)(z + cz) < (unsigned)D.nz;
+    const bool z_clamp = cz != 0 && (unsigned)(z - cz) >= (unsigned)D.nz;
+    if (y_norm && z_norm) fn(y + cy, z + cz);
+    if (y_norm && z_clamp) fn(y + cy, z);
+    if (y_clamp && z_norm) fn(y, z + cz);
+    if (y_clamp && z_clamp) fn(y, z);
+}
+
+// In-place odd step with sector-aligned stores: one CTA per x-row (y, z),
+// one thread per cell.  The post-collision values of the 18 directions with
+// cx != 0 are staged in shared memory; thread p then writes position p of
+// every target row, taking the value of the cell that streams into p
+// (p - cx, or p itself where p - cx leaves the domain, which is the per-axis
+// clamp of the reference).  Every global store of a warp covers 32
+// consecutive cells, so no sector is written partially.  Same results as
+// k_aa_odd bit for bit.
+template <typename S, typename R, int MAXT>
+__global__ void __launch_bounds__(MAXT) k_aa_odd_rows(const __grid_constant__ StepArgs<S, R> a)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const Domain& D = a.dom;
+    const int nxp = blockDim.x;
+    R* sh = reinterpret_cast<R*>(smem_raw);                   // [18][nxp]
+    uint8_t* sst = reinterpret_cast<uint8_t*>(sh + 18 * nxp);  // store bit per cell
+    const int x = threadIdx.x, y = blockIdx.x, z = blockIdx.y;
+    const bool valid = x < D.nx;
+    const int i = x + D.nx * (y + D.ny * z);
+    uint8_t op = 0;
+    R f[27];
+    if (valid) {
+        op = a.ops[i];
+        if (op & OP_LOAD) {
+            load_pulled<LAYOUT_AA_A>(a, x, y, z, i, (op & OP_EDGE) != 0, f);
+        } else {
+#pragma unroll
+            for (int d = 0; d < 27; ++d) f[d] = R(0);
+        }
+        cell_update<R>(op, a.inv_tau, a.rho, a.vx, a.vy, a.vz, i, f);
+#pragma unroll
+        for (int d = 0, k = 0; d < 27; ++d)
+            if (cx_of(d) != 0) sh[(k++) * nxp + x] = f[d];
+        sst[x] = (op & OP_STORE) ? 1 : 0;
+    }
+    __syncthreads();
+    if (!valid) return;
+#pragma unroll
+    for (int d = 0, k = 0; d < 27; ++d) {
+        const int cx = cx_of(d), cy = cy_of(d), cz = cz_of(d);
+        R v;
+        bool st;
+        if (cx == 0) {
+            v = f[d];
+            st = (op & OP_STORE) != 0;
+        } else {
+            const int xs = ((unsigned)(x - cx) < (unsigned)D.nx) ? x - cx : x;
+            v = sh[k * nxp + xs];
+            st = sst[xs] != 0;
+            ++k;
+        }
+        if (!st) continue;
+        for_each_row_target(D, y, z, cy, cz,
+                            [&](int Y, int Z) { Cvt<S, R>::st(a.dst.p[d] + (x + D.nx * (Y + D.ny * Z)), v); });
+    }
+}
+
 // In-place even step (layout B -> A): own slots in, reversed own slots out.
 // A cell that is the clamped source of boundary cells y also files f_d into
 // the edge-buffer slot of (y, d): the next odd step's clamped pull of y reads

@@ -313,10 +313,24 @@ culbm_status tiles_create(culbm_sim* s)
     ts->d_rs = static_cast<RoundState*>(p);
 
     if (c.use_ring_ddf_buf) {
-        // One global buffer of nz + (Bz - (I-1) + 1) planes; each round writes
-        // its result that many planes below its source, modulo the ring
-        // (simulator_expt_platform.cu:252-277, 749-846).
-        ts->ring_step = ts->B[2] - (ts->I - 1) + 1;
+        // One global buffer of nz + step planes; each round writes its result
+        // `step` planes below its source, modulo the ring
+        // (simulator_expt_platform.cu:252-277, 749-846).  A z-slab k of tiles
+        // writes its valid planes [vp(k), vp(k+1)); the tiles still to come
+        // read from plane vp(k) - innerLoop upwards, so the shifted writes stay
+        // clear of them iff step >= extent(k) + innerLoop for k >= 1, and
+        // step >= extent(0) for the first slab.  The reference's fixed
+        // Bz - (I-1) + 1 meets this for middle slabs only; a longer last slab
+        // (or a single slab) would overwrite planes that later tiles read.
+        int step = 0;
+        const int nz = s->dom.nz;
+        for (int kz = 0; kz < ts->nt[2]; ++kz) {
+            const int lo = valid_prev(kz, ts->B[2], ts->nt[2], ts->I, nz);
+            const int hi = valid_prev(kz + 1, ts->B[2], ts->nt[2], ts->I, nz);
+            step = std::max(step, (hi - lo) + (kz > 0 ? ts->I : 0));
+        }
+        step = std::max(step, ts->B[2] - (ts->I - 1) + 1);
+        ts->ring_step = step;
         ts->ring_nz = s->dom.nz + ts->ring_step;
         ts->gstride = 1ll * s->dom.nxy * ts->ring_nz;
         CULBM_TRY(dev_alloc(s, &s->d_pop[0], 27ull * ts->gstride * s->esize, "ring population buffer"));

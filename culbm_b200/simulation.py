@@ -33,7 +33,8 @@ class Simulation:
                  inv_tau: float = 0.5, inner_loop: int = 5, storage: str = "fp32",
                  block_dim: Optional[Sequence[int]] = None, grid_dim: Optional[Sequence[int]] = None,
                  tile: Optional[Sequence[int]] = None, use_ring: bool = False, dev_id: int = 0,
-                 persist_l2: bool = True, cache_hints: bool = True, use_graphs: bool = True):
+                 persist_l2: bool = True, cache_hints: bool = True, use_graphs: bool = True,
+                 kernel_variant: int = 0):
         cfg = _capi.default_config()
         cfg.dev_id = dev_id
         for k in range(3):
@@ -57,6 +58,7 @@ class Simulation:
         cfg.persist_l2 = int(bool(persist_l2))
         cfg.cache_hints = int(bool(cache_hints))
         cfg.use_graphs = int(bool(use_graphs))
+        cfg.kernel_variant = int(kernel_variant)
         self.cfg = cfg
         self.domain = tuple(int(v) for v in domain)
         self.n = self.domain[0] * self.domain[1] * self.domain[2]

@@ -102,7 +102,9 @@ typedef struct culbm_config {
     int32_t cache_hints;       /* 1 (default): evict-first/evict-last hints on global/tile traffic
                                   (reference build switch CULBM_EXPT_CACHE_HINT_POLICY) */
     int32_t use_graphs;        /* 1 (default): tile launch sequences replayed as CUDA graphs */
-    uint32_t reserved[8];
+    int32_t kernel_variant;    /* 0 (default): fastest kernels; 1: one-thread-per-cell kernels only
+                                  (no row staging); same results bit for bit */
+    uint32_t reserved[7];
 } culbm_config;
 
 /* Fills cfg with the reference's defaults plus the additions' defaults. */
