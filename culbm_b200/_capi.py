@@ -25,7 +25,7 @@ STATUS_NAMES = {
 
 STREAM_PULL, STREAM_INPLACE = 0, 1
 OPT_NONE, OPT_STATIC_L2, OPT_L1L2, OPT_DYNAMIC_L2 = 0, 1, 2, 3
-STORAGE = {"fp32": 0, "fp16": 1, "bf16": 2, "fp64": 3}
+STORAGE = {"fp32": 0, "fp16": 1, "bf16": 2, "fp64": 3, "fp16sr": 4, "bf16sr": 5}
 FIELD = {"rho": 0, "vx": 1, "vy": 2, "vz": 3}
 
 # Every symbol include/culbm.h declares.

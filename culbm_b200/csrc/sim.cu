@@ -54,19 +54,6 @@ culbm_status cuda_fail(cudaError_t e, const char* what, const char* file, int li
 
 // ------------------------------------------------------------ utilities ---
 
-// Calls f(Tag<S>{}) for the storage type of sim.
-template <class F>
-culbm_status with_storage(const culbm_sim* s, F&& f)
-{
-    switch (s->cfg.storage) {
-        case CULBM_STORAGE_F32: return f(Tag<float>{});
-        case CULBM_STORAGE_F16: return f(Tag<__half>{});
-        case CULBM_STORAGE_BF16: return f(Tag<__nv_bfloat16>{});
-        case CULBM_STORAGE_F64: return f(Tag<double>{});
-        default: return fail(CULBM_ERR_INVALID_ARGUMENT, "unknown storage format");
-    }
-}
-
 template <typename S>
 StepArgs<S, typename ArithOf<S>::type> make_args(const culbm_sim* s, int src, int dst)
 {
@@ -89,6 +76,7 @@ StepArgs<S, typename ArithOf<S>::type> make_args(const culbm_sim* s, int src, in
     }
     a.edge = static_cast<S*>(s->d_edge);
     a.el = s->el;
+    a.seed = step_seed(static_cast<uint32_t>(s->step));
     return a;
 }
 
@@ -117,7 +105,9 @@ size_t storage_bytes(int storage)
 {
     switch (storage) {
         case CULBM_STORAGE_F16:
-        case CULBM_STORAGE_BF16: return 2;
+        case CULBM_STORAGE_BF16:
+        case CULBM_STORAGE_F16_SR:
+        case CULBM_STORAGE_BF16_SR: return 2;
         case CULBM_STORAGE_F64: return 8;
         default: return 4;
     }
@@ -233,19 +223,24 @@ culbm_status fill_rest(culbm_sim* s)
     return CULBM_OK;
 }
 
-// Row-staged odd kernels may need more than the default 48 KB of dynamic
-// shared memory (18 directions x a padded x-row).
-template <typename S>
-culbm_status enable_row_kernels(culbm_sim* s)
+// Indices of the cells on the domain boundary, x fastest (the in-place
+// steps give them their own launch).
+culbm_status build_edge_list(culbm_sim* s)
 {
-    using R = typename ArithOf<S>::type;
-    const int nxp = (s->dom.nx + 31) / 32 * 32;
-    if (nxp > 1024) return CULBM_OK;
-    const int smem = static_cast<int>(18ull * nxp * sizeof(R) + nxp);
-    if (nxp <= 512)
-        CULBM_CUDA(cudaFuncSetAttribute(k_aa_odd_rows<S, R, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    else
-        CULBM_CUDA(cudaFuncSetAttribute(k_aa_odd_rows<S, R, 1024>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    const Domain& D = s->dom;
+    std::vector<int> list;
+    for (int z = 0; z < D.nz; ++z)
+        for (int y = 0; y < D.ny; ++y) {
+            const bool face = z == 0 || z == D.nz - 1 || y == 0 || y == D.ny - 1;
+            for (int x = 0; x < D.nx; ++x)
+                if (face || x == 0 || x == D.nx - 1) list.push_back(x + D.nx * (y + D.ny * z));
+        }
+    s->n_edge = static_cast<int>(list.size());
+    if (list.empty()) return CULBM_OK;
+    void* p = nullptr;
+    CULBM_TRY(dev_alloc(s, &p, list.size() * sizeof(int), "boundary cell list"));
+    s->d_edge_list = static_cast<int*>(p);
+    CULBM_CUDA(cudaMemcpy(s->d_edge_list, list.data(), list.size() * sizeof(int), cudaMemcpyHostToDevice));
     return CULBM_OK;
 }
 
@@ -255,29 +250,28 @@ culbm_status plain_steps(culbm_sim* s, uint32_t nsteps)
     using R = typename ArithOf<S>::type;
     const dim3 g = cell_grid(s->dom), b = cell_block();
     for (uint32_t k = 0; k < nsteps; ++k) {
+        const uint32_t seed = step_seed(static_cast<uint32_t>(s->step + k));
         if (s->cfg.stream_policy == CULBM_STREAM_PULL) {
             auto a = make_args<S>(s, s->cur, 1 - s->cur);
+            a.seed = seed;
             k_pull_step<S, R><<<g, b, 0, s->stream>>>(a);
             CULBM_CUDA(cudaGetLastError());
             s->cur ^= 1;
         } else {
             auto a = make_args<S>(s, 0, 0);
+            a.seed = seed;
+            const int ne = s->n_edge;
+            const dim3 ge((ne + 255) / 256);
             if (s->aa_phase == 0) {
-                const int nxp = (s->dom.nx + 31) / 32 * 32;
-                if (s->cfg.kernel_variant == 0 && nxp <= 1024) {
-                    const size_t smem = 18ull * nxp * sizeof(R) + nxp;
-                    if (nxp <= 512)
-                        k_aa_odd_rows<S, R, 512><<<dim3(s->dom.ny, s->dom.nz), nxp, smem, s->stream>>>(a);
-                    else
-                        k_aa_odd_rows<S, R, 1024><<<dim3(s->dom.ny, s->dom.nz), nxp, smem, s->stream>>>(a);
-                } else {
-                    k_aa_odd<S, R><<<g, b, 0, s->stream>>>(a);
-                }
+                k_aa_odd<S, R, false><<<g, b, 0, s->stream>>>(a, s->d_edge_list, ne);
+                if (ne) k_aa_odd<S, R, true><<<ge, 256, 0, s->stream>>>(a, s->d_edge_list, ne);
             } else {
-                k_aa_even<S, R><<<g, b, 0, s->stream>>>(a);
+                k_aa_even<S, R, false><<<g, b, 0, s->stream>>>(a, s->d_edge_list, ne);
+                if (ne) k_aa_even<S, R, true><<<ge, 256, 0, s->stream>>>(a, s->d_edge_list, ne);
             }
             CULBM_CUDA(cudaGetLastError());
             s->aa_phase ^= 1;
+            s->launches += ne ? 1 : 0;
         }
         s->launches += 1;
     }
@@ -306,7 +300,7 @@ culbm_status validate_config(const culbm_config& c)
     if (c.stream_policy != CULBM_STREAM_PULL && c.stream_policy != CULBM_STREAM_INPLACE)
         return fail(CULBM_ERR_INVALID_ARGUMENT, "streamPolicy must be 0 or 1");
     if (c.opt_policy < 0 || c.opt_policy > 3) return fail(CULBM_ERR_INVALID_ARGUMENT, "optPolicy must be 0..3");
-    if (c.storage < 0 || c.storage > 3) return fail(CULBM_ERR_INVALID_ARGUMENT, "storage must be 0..3");
+    if (c.storage < 0 || c.storage > 5) return fail(CULBM_ERR_INVALID_ARGUMENT, "storage must be 0..5");
     if (!(c.inv_tau > 0.0f && c.inv_tau < 2.0f))
         return fail(CULBM_ERR_INVALID_ARGUMENT, "invTau must lie in (0, 2)");
     // The reference rejects the ring buffer outside in-place dynamic L2
@@ -334,6 +328,7 @@ void release(culbm_sim* s)
     for (auto& p : s->d_mac) cudaFree(p);
     for (auto& p : s->d_pop) cudaFree(p);
     cudaFree(s->d_edge);
+    cudaFree(s->d_edge_list);
     cudaFree(s->d_red);
     if (s->ev0) cudaEventDestroy(s->ev0);
     if (s->ev1) cudaEventDestroy(s->ev1);
@@ -478,7 +473,7 @@ culbm_status culbm_create(const culbm_config* cfg, culbm_sim** out)
         s->red_blocks = 592;
         CULBM_TRY(dev_alloc(s, reinterpret_cast<void**>(&s->d_red), (4ull * s->red_blocks + 4) * sizeof(double),
                             "reduction scratch"));
-        if (inplace) CULBM_TRY(with_storage(s, [&](auto tag) { return enable_row_kernels<typename decltype(tag)::type>(s); }));
+        if (inplace) CULBM_TRY(build_edge_list(s));
         if (blocked) CULBM_TRY(tiles_create(s));
         const float* none[4] = {nullptr, nullptr, nullptr, nullptr};
         CULBM_TRY(upload_state(s, nullptr, none));

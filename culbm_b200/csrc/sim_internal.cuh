@@ -59,6 +59,8 @@ struct culbm_sim {
     void* d_edge = nullptr;         // in-place clamp side buffer
     culbm::EdgeLayout el{};
     long long edge_elems = 0;
+    int* d_edge_list = nullptr;     // in-place: boundary cell indices
+    int n_edge = 0;
     size_t esize = 4;               // bytes per stored population
     double* d_red = nullptr;        // reduction partials
     int red_blocks = 0;
@@ -86,6 +88,23 @@ template <typename S>
 struct Tag {
     using type = S;
 };
+
+culbm_status fail(culbm_status s, const std::string& msg);
+
+// Calls f(Tag<S>{}) for the storage type of sim.
+template <class F>
+culbm_status with_storage(const culbm_sim* s, F&& f)
+{
+    switch (s->cfg.storage) {
+        case CULBM_STORAGE_F32: return f(Tag<float>{});
+        case CULBM_STORAGE_F16: return f(Tag<__half>{});
+        case CULBM_STORAGE_BF16: return f(Tag<__nv_bfloat16>{});
+        case CULBM_STORAGE_F64: return f(Tag<double>{});
+        case CULBM_STORAGE_F16_SR: return f(Tag<Half16SR>{});
+        case CULBM_STORAGE_BF16_SR: return f(Tag<BF16SR>{});
+        default: return fail(CULBM_ERR_INVALID_ARGUMENT, "unknown storage format");
+    }
+}
 
 // Device allocation counted in sim->device_bytes (sim.cu).
 culbm_status dev_alloc(culbm_sim* s, void** p, size_t bytes, const char* what);

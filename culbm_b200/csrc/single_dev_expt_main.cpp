@@ -69,7 +69,7 @@ void usage(std::ostream& os)
           "                            Dump the field every `dstep` time steps.\n"
           "  --useRingDDFBuf           One global DDF ring buffer for in-place dynamic L2 blocking.\n"
           "  --innerLoop INT [5]       # of iterations in halo-blocking.\n"
-          "  --storage TEXT [fp32]     Population storage: fp32, fp16, bf16 or fp64.\n"
+          "  --storage TEXT [fp32]     Population storage: fp32, fp16, bf16, fp64, fp16sr or bf16sr.\n"
           "  --noPersistL2             No persisting-L2 window over tile buffers.\n"
           "  --noCacheHints            No evict-first/evict-last cache hints.\n"
           "  --noGraphs                Launch tile sequences directly instead of CUDA graphs.\n";
@@ -195,6 +195,8 @@ Options parse(int argc, char** argv)
             else if (v == "fp16") o.cfg.storage = CULBM_STORAGE_F16;
             else if (v == "bf16") o.cfg.storage = CULBM_STORAGE_BF16;
             else if (v == "fp64") o.cfg.storage = CULBM_STORAGE_F64;
+            else if (v == "fp16sr") o.cfg.storage = CULBM_STORAGE_F16_SR;
+            else if (v == "bf16sr") o.cfg.storage = CULBM_STORAGE_BF16_SR;
             else throw ParseError{kConversionError, "Could not convert: --storage = " + v};
         } else if (name == "--noPersistL2") {
             flag();

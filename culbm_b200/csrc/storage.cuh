@@ -9,7 +9,11 @@
 //                      so only the half rounding (nearest-even) loses bits.
 //   S = __nv_bfloat16  BF16 storage of f_i - w_i (float exponent range, no
 //                      scale); FP32 arithmetic, nearest-even rounding.
+//   S = Half16SR, BF16SR  the same two 16-bit layouts written with
+//                      stochastic rounding (see below).
 #pragma once
+
+#include <cstdint>
 
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
@@ -62,6 +66,110 @@ template <> struct Cvt<__nv_bfloat16, float> {
     static __device__ __forceinline__ float ld_cs(const __nv_bfloat16* p) { return __bfloat162float(__ldcs(p)); }
     static __device__ __forceinline__ void st_cs(__nv_bfloat16* p, float v) { __stcs(p, __float2bfloat16_rn(v)); }
 };
+
+// 16-bit storage with stochastic rounding: the same bit layouts as __half
+// (scaled by 2^15) and __nv_bfloat16, but every store rounds up or down with
+// probability given by the discarded fraction, driven by a counter-based hash
+// of (cell, direction, time step).  The hash inputs name the value, not the
+// address it is written to, so every copy of a population (streaming target,
+// clamp slots, tile buffers) gets the same bits and all streaming policies
+// stay bitwise equal to each other.  Deterministic for a given run.
+struct Half16SR {
+    unsigned short bits;
+};
+struct BF16SR {
+    unsigned short bits;
+};
+
+template <typename S> struct IsSR { static constexpr bool value = false; };
+template <> struct IsSR<Half16SR> { static constexpr bool value = true; };
+template <> struct IsSR<BF16SR> { static constexpr bool value = true; };
+
+// Per-step seed and per-value random bits (integer mixing in the style of
+// the murmur3 finaliser).
+__host__ __device__ __forceinline__ uint32_t step_seed(uint32_t t)
+{
+    uint32_t h = t * 0x9E3779B1u + 0x7F4A7C15u;
+    h ^= h >> 16;
+    h *= 0x85EBCA6Bu;
+    h ^= h >> 13;
+    h *= 0xC2B2AE35u;
+    h ^= h >> 16;
+    return h;
+}
+
+__device__ __forceinline__ uint32_t sr_bits(uint32_t cell, uint32_t d, uint32_t seed)
+{
+    uint32_t h = cell * 0x27D4EB2Fu ^ seed ^ (d * 0x165667B1u);
+    h ^= h >> 15;
+    h *= 0x2C1B3C6Du;
+    h ^= h >> 12;
+    h *= 0x297A2D39u;
+    h ^= h >> 15;
+    return h;
+}
+
+template <> struct Cvt<Half16SR, float> {
+    static __device__ __forceinline__ float ld(const Half16SR* p)
+    {
+        return __fmul_rn(__half2float(__ushort_as_half(p->bits)), kHalfInvScale);
+    }
+    static __device__ __forceinline__ float ld_cs(const Half16SR* p)
+    {
+        return __fmul_rn(__half2float(__ushort_as_half(__ldcs(&p->bits))), kHalfInvScale);
+    }
+    // nearest-even (used only for exact values such as the rest state)
+    static __device__ __forceinline__ void st(Half16SR* p, float v)
+    {
+        p->bits = __half_as_ushort(__float2half_rn(__fmul_rn(v, kHalfScale)));
+    }
+    // stochastic: add 13 random bits below the half's last mantissa bit, truncate
+    static __device__ __forceinline__ unsigned short enc(float v, uint32_t rnd)
+    {
+        const uint32_t u = __float_as_uint(__fmul_rn(v, kHalfScale)) + (rnd & 0x1FFFu);
+        return __half_as_ushort(__float2half_rz(__uint_as_float(u)));
+    }
+    static __device__ __forceinline__ void st_sr(Half16SR* p, float v, uint32_t rnd) { p->bits = enc(v, rnd); }
+    static __device__ __forceinline__ void st_sr_cs(Half16SR* p, float v, uint32_t rnd) { __stcs(&p->bits, enc(v, rnd)); }
+};
+
+template <> struct Cvt<BF16SR, float> {
+    static __device__ __forceinline__ float ld(const BF16SR* p) { return __uint_as_float(uint32_t(p->bits) << 16); }
+    static __device__ __forceinline__ float ld_cs(const BF16SR* p)
+    {
+        return __uint_as_float(uint32_t(__ldcs(&p->bits)) << 16);
+    }
+    static __device__ __forceinline__ void st(BF16SR* p, float v)
+    {
+        p->bits = __bfloat16_as_ushort(__float2bfloat16_rn(v));
+    }
+    static __device__ __forceinline__ unsigned short enc(float v, uint32_t rnd)
+    {
+        return static_cast<unsigned short>((__float_as_uint(v) + (rnd & 0xFFFFu)) >> 16);
+    }
+    static __device__ __forceinline__ void st_sr(BF16SR* p, float v, uint32_t rnd) { p->bits = enc(v, rnd); }
+    static __device__ __forceinline__ void st_sr_cs(BF16SR* p, float v, uint32_t rnd) { __stcs(&p->bits, enc(v, rnd)); }
+};
+
+// Store of population d of cell `cell` at time step `seed` names: stochastic
+// rounding for the SR formats, the format's plain conversion otherwise.
+template <typename S, typename R>
+__device__ __forceinline__ void put(S* p, R v, uint32_t cell, int d, uint32_t seed)
+{
+    if constexpr (IsSR<S>::value)
+        Cvt<S, R>::st_sr(p, v, sr_bits(cell, d, seed));
+    else
+        Cvt<S, R>::st(p, v);
+}
+
+template <typename S, typename R>
+__device__ __forceinline__ void put_cs(S* p, R v, uint32_t cell, int d, uint32_t seed)
+{
+    if constexpr (IsSR<S>::value)
+        Cvt<S, R>::st_sr_cs(p, v, sr_bits(cell, d, seed));
+    else
+        Cvt<S, R>::st_cs(p, v);
+}
 
 // Arithmetic type used with each storage type.
 template <typename S> struct ArithOf { using type = float; };

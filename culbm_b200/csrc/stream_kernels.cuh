@@ -60,6 +60,7 @@ struct StepArgs {
     EdgeLayout el;
     int ring_nz;   // LAYOUT_PULL_RING: planes in the ring buffer
     int ring_off;  // LAYOUT_PULL_RING: ring plane of domain plane z = 0
+    uint32_t seed; // step_seed of the time step being written (stochastic rounding)
 };
 
 __device__ __forceinline__ int nb_off(const Domain& D, int d)
@@ -225,7 +226,7 @@ __global__ void __launch_bounds__(256) k_pull_step(const __grid_constant__ StepA
     cell_update<R>(op, a.inv_tau, a.rho, a.vx, a.vy, a.vz, c.i, f);
     if (op & OP_STORE) {
 #pragma unroll
-        for (int d = 0; d < 27; ++d) Cvt<S, R>::st(a.dst.p[d] + c.i, f[d]);
+        for (int d = 0; d < 27; ++d) put(a.dst.p[d] + c.i, f[d], c.i, d, a.seed);
     }
 }
 
@@ -236,110 +237,64 @@ __global__ void __launch_bounds__(256) k_pull_step(const __grid_constant__ StepA
 // buffer, and a cell that is the clamped source of boundary cells y (see
 // for_each_clamp_reader) also writes f_d into slot d of each such y: nobody
 // else reads or writes that slot during the step, and y reads it next step.
-template <typename S, typename R>
-__global__ void __launch_bounds__(256) k_aa_odd(const __grid_constant__ StepArgs<S, R> a)
+//
+// Interior and boundary cells touch disjoint locations, so each in-place step
+// runs as two launches: EDGE = false covers the interior with straight-line
+// code (boundary threads return at once), EDGE = true walks the list of
+// boundary cells with the clamp logic.  Keeping the long clamp code out of
+// the interior kernel keeps its instruction footprint small.
+template <typename S, typename R, bool EDGE>
+__device__ __forceinline__ bool aa_cell(const StepArgs<S, R>& a, const int* edge_list, int n_edge, CellCoord& c)
 {
-    const CellCoord c = cell_of_thread(a.dom);
-    if (!c.valid) return;
+    const Domain& D = a.dom;
+    if (!EDGE) {
+        c = cell_of_thread(D);
+        return c.valid && c.x > 0 && c.x < D.nx - 1 && c.y > 0 && c.y < D.ny - 1 && c.z > 0 && c.z < D.nz - 1;
+    }
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n_edge) return false;
+    c.i = edge_list[t];
+    c.x = c.i % D.nx;
+    c.y = (c.i / D.nx) % D.ny;
+    c.z = c.i / D.nxy;
+    c.valid = true;
+    return true;
+}
+
+template <typename S, typename R, bool EDGE>
+__global__ void __launch_bounds__(256) k_aa_odd(const __grid_constant__ StepArgs<S, R> a, const int* edge_list,
+                                                int n_edge)
+{
+    CellCoord c;
+    if (!aa_cell<S, R, EDGE>(a, edge_list, n_edge, c)) return;
     const Domain& D = a.dom;
     const uint8_t op = a.ops[c.i];
-    const bool edge = (op & OP_EDGE) != 0;
     R f[27];
     if (op & OP_LOAD) {
-        load_pulled<LAYOUT_AA_A>(a, c.x, c.y, c.z, c.i, edge, f);
+        if (!EDGE) {
+#pragma unroll
+            for (int d = 0; d < 27; ++d) f[d] = Cvt<S, R>::ld(a.src.p[26 - d] + (c.i - nb_off(D, d)));
+        } else {
+            load_pulled<LAYOUT_AA_A>(a, c.x, c.y, c.z, c.i, true, f);
+        }
     } else {
 #pragma unroll
         for (int d = 0; d < 27; ++d) f[d] = R(0);
     }
     cell_update<R>(op, a.inv_tau, a.rho, a.vx, a.vy, a.vz, c.i, f);
-    if (op & OP_STORE) {
-        if (!edge) {
+    if (!(op & OP_STORE)) return;
+    if (!EDGE) {
 #pragma unroll
-            for (int d = 0; d < 27; ++d) Cvt<S, R>::st(a.dst.p[d] + (c.i + nb_off(D, d)), f[d]);
-        } else {
-            for_dirs([&](auto dd) {
-                constexpr int d = decltype(dd)::value;
-                if (inside(D, c.x + cx_of(d), c.y + cy_of(d), c.z + cz_of(d)))
-                    Cvt<S, R>::st(a.dst.p[d] + (c.i + nb_off(D, d)), f[d]);
-                for_each_clamp_reader<d>(D, c.x, c.y, c.z, [&](int yx, int yy, int yz) {
-                    Cvt<S, R>::st(a.dst.p[d] + (yx + D.nx * (yy + D.ny * yz)), f[d]);
-                });
+        for (int d = 0; d < 27; ++d) put(a.dst.p[d] + (c.i + nb_off(D, d)), f[d], c.i, d, a.seed);
+    } else {
+        for_dirs([&](auto dd) {
+            constexpr int d = decltype(dd)::value;
+            if (inside(D, c.x + cx_of(d), c.y + cy_of(d), c.z + cz_of(d)))
+                put(a.dst.p[d] + (c.i + nb_off(D, d)), f[d], c.i, d, a.seed);
+            for_each_clamp_reader<d>(D, c.x, c.y, c.z, [&](int yx, int yy, int yz) {
+                put(a.dst.p[d] + (yx + D.nx * (yy + D.ny * yz)), f[d], c.i, d, a.seed);
             });
-        }
-    }
-}
-
-// Rows that receive direction d from row (y, z) in the odd step: the
-// streaming target row (y+cy, z+cz) and, at a y or z face, the rows whose
-// clamped pull reads row (y, z) (for_each_clamp_reader restricted to y, z).
-// Calls fn(Y, Z) for each of them.
-template <class F>
-__device__ __forceinline__ void for_each_row_target(const Domain& D, int y, int z, int cy, int cz, F&& fn)
-{
-    const bool y_norm = (unsigned)(y + cy) < (unsigned)D.ny;
-    const bool y_clamp = cy != 0 && (unsigned)(y - cy) >= (unsigned)D.ny;
-    const bool z_norm = (unsigned)(z + cz) < (unsigned)D.nz;
-    const bool z_clamp = cz != 0 && (unsigned)(z - cz) >= (unsigned)D.nz;
-    if (y_norm && z_norm) fn(y + cy, z + cz);
-    if (y_norm && z_clamp) fn(y + cy, z);
-    if (y_clamp && z_norm) fn(y, z + cz);
-    if (y_clamp && z_clamp) fn(y, z);
-}
-
-// In-place odd step with sector-aligned stores: one CTA per x-row (y, z),
-// one thread per cell.  The post-collision values of the 18 directions with
-// cx != 0 are staged in shared memory; thread p then writes position p of
-// every target row, taking the value of the cell that streams into p
-// (p - cx, or p itself where p - cx leaves the domain, which is the per-axis
-// clamp of the reference).  Every global store of a warp covers 32
-// consecutive cells, so no sector is written partially.  Same results as
-// k_aa_odd bit for bit.
-template <typename S, typename R, int MAXT>
-__global__ void __launch_bounds__(MAXT) k_aa_odd_rows(const __grid_constant__ StepArgs<S, R> a)
-{
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    const Domain& D = a.dom;
-    const int nxp = blockDim.x;
-    R* sh = reinterpret_cast<R*>(smem_raw);                   // [18][nxp]
-    uint8_t* sst = reinterpret_cast<uint8_t*>(sh + 18 * nxp);  // store bit per cell
-    const int x = threadIdx.x, y = blockIdx.x, z = blockIdx.y;
-    const bool valid = x < D.nx;
-    const int i = x + D.nx * (y + D.ny * z);
-    uint8_t op = 0;
-    R f[27];
-    if (valid) {
-        op = a.ops[i];
-        if (op & OP_LOAD) {
-            load_pulled<LAYOUT_AA_A>(a, x, y, z, i, (op & OP_EDGE) != 0, f);
-        } else {
-#pragma unroll
-            for (int d = 0; d < 27; ++d) f[d] = R(0);
-        }
-        cell_update<R>(op, a.inv_tau, a.rho, a.vx, a.vy, a.vz, i, f);
-#pragma unroll
-        for (int d = 0, k = 0; d < 27; ++d)
-            if (cx_of(d) != 0) sh[(k++) * nxp + x] = f[d];
-        sst[x] = (op & OP_STORE) ? 1 : 0;
-    }
-    __syncthreads();
-    if (!valid) return;
-#pragma unroll
-    for (int d = 0, k = 0; d < 27; ++d) {
-        const int cx = cx_of(d), cy = cy_of(d), cz = cz_of(d);
-        R v;
-        bool st;
-        if (cx == 0) {
-            v = f[d];
-            st = (op & OP_STORE) != 0;
-        } else {
-            const int xs = ((unsigned)(x - cx) < (unsigned)D.nx) ? x - cx : x;
-            v = sh[k * nxp + xs];
-            st = sst[xs] != 0;
-            ++k;
-        }
-        if (!st) continue;
-        for_each_row_target(D, y, z, cy, cz,
-                            [&](int Y, int Z) { Cvt<S, R>::st(a.dst.p[d] + (x + D.nx * (Y + D.ny * Z)), v); });
+        });
     }
 }
 
@@ -347,12 +302,13 @@ __global__ void __launch_bounds__(MAXT) k_aa_odd_rows(const __grid_constant__ St
 // A cell that is the clamped source of boundary cells y also files f_d into
 // the edge-buffer slot of (y, d): the next odd step's clamped pull of y reads
 // it there, because slot 26-d of the source is overwritten during that step.
-template <typename S, typename R>
-__global__ void __launch_bounds__(256) k_aa_even(const __grid_constant__ StepArgs<S, R> a)
+// Only boundary cells can be clamped sources, so only EDGE = true does that.
+template <typename S, typename R, bool EDGE>
+__global__ void __launch_bounds__(256) k_aa_even(const __grid_constant__ StepArgs<S, R> a, const int* edge_list,
+                                                 int n_edge)
 {
-    const CellCoord c = cell_of_thread(a.dom);
-    if (!c.valid) return;
-    const Domain& D = a.dom;
+    CellCoord c;
+    if (!aa_cell<S, R, EDGE>(a, edge_list, n_edge, c)) return;
     const uint8_t op = a.ops[c.i];
     R f[27];
     if (op & OP_LOAD) {
@@ -362,17 +318,17 @@ __global__ void __launch_bounds__(256) k_aa_even(const __grid_constant__ StepArg
         for (int d = 0; d < 27; ++d) f[d] = R(0);
     }
     cell_update<R>(op, a.inv_tau, a.rho, a.vx, a.vy, a.vz, c.i, f);
-    if (op & OP_STORE) {
+    if (!(op & OP_STORE)) return;
 #pragma unroll
-        for (int d = 0; d < 27; ++d) Cvt<S, R>::st(a.dst.p[26 - d] + c.i, f[d]);
-        if (op & OP_EDGE) {
-            for_dirs([&](auto dd) {
-                constexpr int d = decltype(dd)::value;
-                for_each_clamp_reader<d>(D, c.x, c.y, c.z, [&](int yx, int yy, int yz) {
-                    Cvt<S, R>::st(a.edge + edge_slot(D, a.el, yx, yy, yz, d), f[d]);
-                });
+    for (int d = 0; d < 27; ++d) put(a.dst.p[26 - d] + c.i, f[d], c.i, d, a.seed);
+    if (EDGE) {
+        const Domain& D = a.dom;
+        for_dirs([&](auto dd) {
+            constexpr int d = decltype(dd)::value;
+            for_each_clamp_reader<d>(D, c.x, c.y, c.z, [&](int yx, int yy, int yz) {
+                put(a.edge + edge_slot(D, a.el, yx, yy, yz, d), f[d], c.i, d, a.seed);
             });
-        }
+        });
     }
 }
 
@@ -423,18 +379,19 @@ __global__ void __launch_bounds__(256) k_import(const __grid_constant__ StepArgs
     for (int d = 0; d < 27; ++d) {
         const R v = R(in[(long long)d * D.n + c.i]);
         if (LAYOUT == LAYOUT_PULL) {
-            Cvt<S, R>::st(a.dst.p[d] + c.i, v);
+            put(a.dst.p[d] + c.i, v, c.i, d, a.seed);
         } else if (LAYOUT == LAYOUT_PULL_RING) {
-            Cvt<S, R>::st(a.dst.p[d] + ring_index(a, c.x, c.y, c.z), v);
+            put(a.dst.p[d] + ring_index(a, c.x, c.y, c.z), v, c.i, d, a.seed);
         } else {
-            Cvt<S, R>::st(a.dst.p[26 - d] + c.i, v);
+            put(a.dst.p[26 - d] + c.i, v, c.i, d, a.seed);
             int sx = c.x - cx_of(d), sy = c.y - cy_of(d), sz = c.z - cz_of(d);
             if (!inside(D, sx, sy, sz)) {
                 if ((unsigned)sx >= (unsigned)D.nx) sx = c.x;
                 if ((unsigned)sy >= (unsigned)D.ny) sy = c.y;
                 if ((unsigned)sz >= (unsigned)D.nz) sz = c.z;
-                const R w = R(in[(long long)d * D.n + sx + D.nx * (sy + D.ny * sz)]);
-                Cvt<S, R>::st(a.edge + edge_slot(D, a.el, c.x, c.y, c.z, d), w);
+                const int si = sx + D.nx * (sy + D.ny * sz);
+                const R w = R(in[(long long)d * D.n + si]);
+                put(a.edge + edge_slot(D, a.el, c.x, c.y, c.z, d), w, si, d, a.seed);
             }
         }
     }

@@ -31,7 +31,7 @@ struct RoundState {
     int sel;        // double buffer: index of the buffer holding the newest state
     int src_offz;   // ring buffer: z offset of the current state
     int dst_offz;   // ring buffer: z offset the round writes to
-    int pad;
+    uint32_t step;  // time steps done before this round (seeds stochastic rounding)
 };
 
 template <typename S>
@@ -59,6 +59,7 @@ struct TileArgs {
     S* edge;                // domain-clamp side buffer (in-place tiles)
     EdgeLayout el;
     const RoundState* rs;
+    int j;                  // step of the round this launch performs (0 = first)
 };
 
 template <typename S>
@@ -83,13 +84,19 @@ __device__ __forceinline__ R gload(const S* p)
 }
 
 template <typename S, typename R, bool HINT>
-__device__ __forceinline__ void gstore(S* p, R v)
+__device__ __forceinline__ void gstore(S* p, R v, uint32_t cell, int d, uint32_t seed)
 {
     if constexpr (HINT) {
-        Cvt<S, R>::st_cs(p, v);
+        put_cs(p, v, cell, d, seed);
     } else {
-        Cvt<S, R>::st(p, v);
+        put(p, v, cell, d, seed);
     }
+}
+
+template <typename S, typename R>
+__device__ __forceinline__ uint32_t tile_seed(const TileArgs<S, R>& a)
+{
+    return step_seed(a.rs->step + static_cast<uint32_t>(a.j));
 }
 
 struct TileCell {
@@ -145,7 +152,9 @@ __device__ __forceinline__ void tile_store_global(const TileArgs<S, R>& a, const
     S* base = a.g.base[sel];
     const long long off = gaddr(a.g, a.dom, offz, c.gx, c.gy, c.gz);
 #pragma unroll
-    for (int d = 0; d < 27; ++d) gstore<S, R, HINT>(base + d * a.g.stride + off, f[d]);
+    const uint32_t seed = tile_seed(a);
+#pragma unroll
+    for (int d = 0; d < 27; ++d) gstore<S, R, HINT>(base + d * a.g.stride + off, f[d], c.gi, d, seed);
 }
 
 // Selected buffers of the current round.
@@ -191,10 +200,11 @@ __device__ __forceinline__ void tile_load_aa(const TileArgs<S, R>& a, const Tile
 template <typename S, typename R>
 __device__ __forceinline__ void tile_file_clamp_sources(const TileArgs<S, R>& a, const TileCell& c, const R* f)
 {
+    const uint32_t seed = tile_seed(a);
     for_dirs([&](auto dd) {
         constexpr int d = decltype(dd)::value;
         for_each_clamp_reader<d>(a.dom, c.gx, c.gy, c.gz, [&](int yx, int yy, int yz) {
-            Cvt<S, R>::st(a.edge + edge_slot(a.dom, a.el, yx, yy, yz, d), f[d]);
+            put(a.edge + edge_slot(a.dom, a.el, yx, yy, yz, d), f[d], c.gi, d, seed);
         });
     });
 }
@@ -220,7 +230,7 @@ __global__ void __launch_bounds__(256) k_tile_aa_first(const __grid_constant__ T
         if (c.correct) tile_store_global<S, R, HINT>(a, c, round_dst_sel(a.rs, ring), a.rs->dst_offz, f);
     } else {
 #pragma unroll
-        for (int d = 0; d < 27; ++d) Cvt<S, R>::st(a.t0.p[26 - d] + c.t, f[d]);
+        for (int d = 0; d < 27; ++d) put(a.t0.p[26 - d] + c.t, f[d], c.gi, d, tile_seed(a));
         if (op & OP_EDGE) tile_file_clamp_sources(a, c, f);
     }
 }
@@ -247,19 +257,20 @@ __global__ void __launch_bounds__(256) k_tile_aa_odd(const __grid_constant__ Til
     if (!edge && tile_inner) {
 #pragma unroll
         for (int d = 0; d < 27; ++d)
-            Cvt<S, R>::st(a.t0.p[d] + (c.t + cx_of(d) + cy_of(d) * a.bx + cz_of(d) * a.bxy), f[d]);
+            put(a.t0.p[d] + (c.t + cx_of(d) + cy_of(d) * a.bx + cz_of(d) * a.bxy), f[d], c.gi, d, tile_seed(a));
         return;
     }
     for_dirs([&](auto dd) {
         constexpr int d = decltype(dd)::value;
         constexpr int cx = cx_of(d), cy = cy_of(d), cz = cz_of(d);
         if (inside(D, c.gx + cx, c.gy + cy, c.gz + cz) && in_tile(c.px + cx, c.py + cy, c.pz + cz, a.bx, a.by, a.bz))
-            Cvt<S, R>::st(a.t0.p[d] + (c.t + cx + cy * a.bx + cz * a.bxy), f[d]);
+            put(a.t0.p[d] + (c.t + cx + cy * a.bx + cz * a.bxy), f[d], c.gi, d, tile_seed(a));
         if (edge) {
             // slot d of each boundary cell whose clamped pull reads this cell
             for_each_clamp_reader<d>(D, c.gx, c.gy, c.gz, [&](int yx, int yy, int yz) {
                 const int qx = yx - a.ox, qy = yy - a.oy, qz = yz - a.oz;
-                if (in_tile(qx, qy, qz, a.bx, a.by, a.bz)) Cvt<S, R>::st(a.t0.p[d] + (qx + a.bx * (qy + a.by * qz)), f[d]);
+                if (in_tile(qx, qy, qz, a.bx, a.by, a.bz))
+                    put(a.t0.p[d] + (qx + a.bx * (qy + a.by * qz)), f[d], c.gi, d, tile_seed(a));
             });
         }
     });
@@ -282,7 +293,7 @@ __global__ void __launch_bounds__(256) k_tile_aa_even(const __grid_constant__ Ti
     cell_update<R>(op, a.inv_tau, a.rho, a.vx, a.vy, a.vz, c.gi, f);
     if (!(op & OP_STORE)) return;
 #pragma unroll
-    for (int d = 0; d < 27; ++d) Cvt<S, R>::st(a.t0.p[26 - d] + c.t, f[d]);
+    for (int d = 0; d < 27; ++d) put(a.t0.p[26 - d] + c.t, f[d], c.gi, d, tile_seed(a));
     if (op & OP_EDGE) tile_file_clamp_sources(a, c, f);
 }
 
@@ -352,7 +363,7 @@ __global__ void __launch_bounds__(256) k_tile_pull_first(const __grid_constant__
         if (c.correct) tile_store_global<S, R, HINT>(a, c, round_dst_sel(a.rs, ring), a.rs->dst_offz, f);
     } else {
 #pragma unroll
-        for (int d = 0; d < 27; ++d) Cvt<S, R>::st(a.t0.p[d] + c.t, f[d]);
+        for (int d = 0; d < 27; ++d) put(a.t0.p[d] + c.t, f[d], c.gi, d, tile_seed(a));
     }
 }
 
@@ -373,7 +384,7 @@ __global__ void __launch_bounds__(256) k_tile_pull_mid(const __grid_constant__ T
     cell_update<R>(op, a.inv_tau, a.rho, a.vx, a.vy, a.vz, c.gi, f);
     if (!(op & OP_STORE)) return;
 #pragma unroll
-    for (int d = 0; d < 27; ++d) Cvt<S, R>::st(a.t1.p[d] + c.t, f[d]);
+    for (int d = 0; d < 27; ++d) put(a.t1.p[d] + c.t, f[d], c.gi, d, tile_seed(a));
 }
 
 template <typename S, typename R, bool HINT>
@@ -394,9 +405,10 @@ __global__ void __launch_bounds__(256) k_tile_pull_last(const __grid_constant__ 
 }
 
 // Advances the round state after all tiles of a round.
-__global__ void k_tile_advance(RoundState* rs, int ring_nz, int ring_step)
+__global__ void k_tile_advance(RoundState* rs, int ring_nz, int ring_step, int steps)
 {
     if (threadIdx.x == 0 && blockIdx.x == 0) {
+        rs->step += static_cast<uint32_t>(steps);
         if (ring_nz) {
             rs->src_offz = rs->dst_offz;
             int o = rs->dst_offz - ring_step;

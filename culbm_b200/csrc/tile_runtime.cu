@@ -144,6 +144,7 @@ struct TileLauncher {
                 a.vlo[q] = g.vlo[q];
                 a.vhi[q] = g.vhi[q];
             }
+            a.j = 0;
             if (inplace) {
                 if (k == 1) {
                     CULBM_TRY(hint ? launch(k_tile_aa_first<S, R, true, true>, a)
@@ -153,9 +154,11 @@ struct TileLauncher {
                 CULBM_TRY(hint ? launch(k_tile_aa_first<S, R, false, true>, a)
                                : launch(k_tile_aa_first<S, R, false, false>, a));
                 for (int j = 2; j < k; ++j) {
+                    a.j = j - 1;
                     if (j % 2 == 0) CULBM_TRY(launch(k_tile_aa_odd<S, R>, a));
                     else CULBM_TRY(launch(k_tile_aa_even<S, R>, a));
                 }
+                a.j = k - 1;
                 if (k % 2 == 0)
                     CULBM_TRY(hint ? launch(k_tile_aa_last<LAYOUT_AA_A, S, R, true>, a)
                                    : launch(k_tile_aa_last<LAYOUT_AA_A, S, R, false>, a));
@@ -172,21 +175,24 @@ struct TileLauncher {
                 CULBM_TRY(hint ? launch(k_tile_pull_first<S, R, false, true>, b)
                                : launch(k_tile_pull_first<S, R, false, false>, b));
                 for (int j = 2; j < k; ++j) {
+                    b.j = j - 1;
                     CULBM_TRY(launch(k_tile_pull_mid<S, R>, b));
                     std::swap(b.t0, b.t1);
                 }
+                b.j = k - 1;
                 CULBM_TRY(hint ? launch(k_tile_pull_last<S, R, true>, b) : launch(k_tile_pull_last<S, R, false>, b));
             }
         }
-        k_tile_advance<<<1, 32, 0, s->stream>>>(ts->d_rs, ts->ring_nz, ts->ring_step);
+        k_tile_advance<<<1, 32, 0, s->stream>>>(ts->d_rs, ts->ring_nz, ts->ring_step, k);
         CULBM_CUDA(cudaGetLastError());
         s->launches += 1;
         return CULBM_OK;
     }
 };
 
-void host_advance(TileState* ts)
+void host_advance(TileState* ts, int steps)
 {
+    ts->h_rs.step += static_cast<uint32_t>(steps);
     if (ts->ring_nz) {
         ts->h_rs.src_offz = ts->h_rs.dst_offz;
         int o = ts->h_rs.dst_offz - ts->ring_step;
@@ -229,17 +235,17 @@ culbm_status tiles_step_typed(culbm_sim* s, uint32_t nsteps)
         for (uint32_t r = 0; r < full; ++r) {
             CULBM_CUDA(cudaGraphLaunch(ts->graph, s->stream));
             s->launches += per_round;
-            host_advance(ts);
+            host_advance(ts, ts->I);
         }
         full = 0;
     }
     for (uint32_t r = 0; r < full; ++r) {
         CULBM_TRY(L.round(ts->I));
-        host_advance(ts);
+        host_advance(ts, ts->I);
     }
     if (rem) {
         CULBM_TRY(L.round(static_cast<int>(rem)));
-        host_advance(ts);
+        host_advance(ts, static_cast<int>(rem));
     }
     s->cur = ts->h_rs.sel;
     return CULBM_OK;
@@ -393,7 +399,7 @@ culbm_status tiles_upload_flags(culbm_sim*, const uint32_t*) { return CULBM_OK; 
 culbm_status tiles_reset(culbm_sim* s)
 {
     TileState* ts = s->tiles;
-    ts->h_rs = RoundState{0, 0, ts->ring_nz ? s->dom.nz : 0, 0};
+    ts->h_rs = RoundState{0, 0, ts->ring_nz ? s->dom.nz : 0, 0u};
     CULBM_CUDA(cudaMemcpyAsync(ts->d_rs, &ts->h_rs, sizeof(RoundState), cudaMemcpyHostToDevice, s->stream));
     auto fill = [&](auto tag) -> culbm_status {
         using S = typename decltype(tag)::type;
@@ -404,24 +410,14 @@ culbm_status tiles_reset(culbm_sim* s)
         }
         return CULBM_OK;
     };
-    switch (s->cfg.storage) {
-        case CULBM_STORAGE_F32: CULBM_TRY(fill(Tag<float>{})); break;
-        case CULBM_STORAGE_F16: CULBM_TRY(fill(Tag<__half>{})); break;
-        case CULBM_STORAGE_BF16: CULBM_TRY(fill(Tag<__nv_bfloat16>{})); break;
-        default: CULBM_TRY(fill(Tag<double>{})); break;
-    }
+    CULBM_TRY(with_storage(s, fill));
     s->cur = 0;
     return CULBM_OK;
 }
 
 culbm_status tiles_step(culbm_sim* s, uint32_t nsteps)
 {
-    switch (s->cfg.storage) {
-        case CULBM_STORAGE_F32: return tiles_step_typed<float>(s, nsteps);
-        case CULBM_STORAGE_F16: return tiles_step_typed<__half>(s, nsteps);
-        case CULBM_STORAGE_BF16: return tiles_step_typed<__nv_bfloat16>(s, nsteps);
-        default: return tiles_step_typed<double>(s, nsteps);
-    }
+    return with_storage(s, [&](auto tag) { return tiles_step_typed<typename decltype(tag)::type>(s, nsteps); });
 }
 
 void tiles_view(const culbm_sim* s, int* ring_nz, int* offz, long long* stride)

@@ -58,7 +58,9 @@ typedef enum culbm_storage {
     CULBM_STORAGE_F32 = 0,  /* FP32, the reference's format */
     CULBM_STORAGE_F16 = 1,  /* FP16 deviations f_i - w_i (scaled by 2^15), FP32 arithmetic */
     CULBM_STORAGE_BF16 = 2, /* BF16 deviations f_i - w_i, FP32 arithmetic */
-    CULBM_STORAGE_F64 = 3   /* FP64 storage and arithmetic (the GPU oracle) */
+    CULBM_STORAGE_F64 = 3,  /* FP64 storage and arithmetic (the GPU oracle) */
+    CULBM_STORAGE_F16_SR = 4,  /* as F16, stored with deterministic stochastic rounding */
+    CULBM_STORAGE_BF16_SR = 5  /* as BF16, stored with deterministic stochastic rounding */
 } culbm_storage;
 
 typedef enum culbm_field {
@@ -102,8 +104,7 @@ typedef struct culbm_config {
     int32_t cache_hints;       /* 1 (default): evict-first/evict-last hints on global/tile traffic
                                   (reference build switch CULBM_EXPT_CACHE_HINT_POLICY) */
     int32_t use_graphs;        /* 1 (default): tile launch sequences replayed as CUDA graphs */
-    int32_t kernel_variant;    /* 0 (default): fastest kernels; 1: one-thread-per-cell kernels only
-                                  (no row staging); same results bit for bit */
+    int32_t kernel_variant;    /* reserved for alternative kernel schedules; 0 = default */
     uint32_t reserved[7];
 } culbm_config;
 

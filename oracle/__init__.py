@@ -65,6 +65,13 @@ def lib():
             getattr(L, f"orc_run_{sfx}").argtypes = [_i64, _i64, _i64, _u32p, _f32p, _f32p, _f32p, _f32p,
                                                      real, _i64, rp, rp]
             getattr(L, f"orc_run_{sfx}").restype = C.c_int
+        u16p = np.ctypeslib.ndpointer(np.uint16, flags="C_CONTIGUOUS")
+        L.orc_step_s16.argtypes = [C.c_int, _i64, _i64, _i64, _u32p, _f32p, _f32p, _f32p, _f32p, C.c_float,
+                                   u16p, u16p, C.c_uint32]
+        L.orc_decode_s16.argtypes = [C.c_int, _i64, u16p, _f32p]
+        L.orc_encode_s16.argtypes = [C.c_int, _i64, _f32p, u16p, C.c_uint32]
+        L.orc_step_seed.argtypes = [C.c_uint32]
+        L.orc_step_seed.restype = C.c_uint32
         L.orc_valid_blk_axis.argtypes = [C.c_uint32] * 3
         L.orc_valid_blk_axis.restype = C.c_int
         L.orc_blk_num.argtypes = [C.c_uint32] * 3
@@ -196,3 +203,26 @@ def ref_moments(scene: Scene, ddf, nthreads=0):
     out = [scene.rho.copy(), scene.vx.copy(), scene.vy.copy(), scene.vz.copy()]
     ref().ref_moments_f32(scene.nx, scene.ny, scene.nz, scene.flag, np.ascontiguousarray(ddf), *out, nthreads)
     return tuple(out)
+
+
+# 16-bit storage kinds of orc_step_s16 (match culbm_b200's storage names)
+S16_KIND = {"fp16": 0, "bf16": 1, "fp16sr": 2, "bf16sr": 3}
+
+
+def run_s16(scene: Scene, storage: str, inv_tau, nsteps, state=None):
+    """nsteps pull steps with 16-bit storage from rest (or from an FP32 state
+    narrowed with nearest-even / stochastic rounding keyed on step 0); returns
+    the newest state widened to FP32."""
+    kind = S16_KIND[storage]
+    L = lib()
+    f32 = rest_state(scene.n) if state is None else np.ascontiguousarray(state, np.float32)
+    a = np.empty(27 * scene.n, np.uint16)
+    L.orc_encode_s16(kind, scene.n, f32, a, 0)
+    b = a.copy()
+    for t in range(nsteps):
+        L.orc_step_s16(kind, scene.nx, scene.ny, scene.nz, scene.flag, scene.rho, scene.vx, scene.vy, scene.vz,
+                       inv_tau, a, b, t)
+        a, b = b, a
+    out = np.empty(27 * scene.n, np.float32)
+    L.orc_decode_s16(kind, 27 * scene.n, a, out)
+    return out

@@ -71,3 +71,124 @@ int32_t orc_valid_prev(int32_t idx, int32_t blk, int32_t num, int32_t iter, int3
     if (idx == 0) return 0;
     return (blk + 1 - iter) + (idx - 1) * (blk + 2 - 2 * iter);
 }
+
+/* ---------------------------------------------------------------------------
+ * 16-bit population storage (no reference counterpart): the stored value is
+ * the shifted population f_i - w_i as IEEE half scaled by 2^15 (kind 0, 2)
+ * or as bfloat16 (kind 1, 3); arithmetic in FP32.  Kinds 0/1 round to nearest
+ * even, kinds 2/3 round stochastically with random bits from a counter-based
+ * hash of (cell, direction, time step).  A step is: widen src to FP32, one FP32
+ * pull step, narrow every cell back.  Widening and narrowing a stored value
+ * gives it back exactly, so cells without STORE keep their old bits.
+ * ------------------------------------------------------------------------- */
+#include <stdlib.h>
+#include <string.h>
+
+static uint32_t f2u(float f) { uint32_t u; memcpy(&u, &f, 4); return u; }
+static float u2f(uint32_t u) { float f; memcpy(&f, &u, 4); return f; }
+
+uint32_t orc_step_seed(uint32_t t)
+{
+    uint32_t h = t * 0x9E3779B1u + 0x7F4A7C15u;
+    h ^= h >> 16; h *= 0x85EBCA6Bu; h ^= h >> 13; h *= 0xC2B2AE35u; h ^= h >> 16;
+    return h;
+}
+
+uint32_t orc_sr_bits(uint32_t cell, uint32_t d, uint32_t seed)
+{
+    uint32_t h = cell * 0x27D4EB2Fu ^ seed ^ (d * 0x165667B1u);
+    h ^= h >> 15; h *= 0x2C1B3C6Du; h ^= h >> 12; h *= 0x297A2D39u; h ^= h >> 15;
+    return h;
+}
+
+static float h16_decode(uint16_t h)
+{
+    _Float16 v;
+    memcpy(&v, &h, 2);
+    return (float)v * (1.0f / 32768.0f);
+}
+
+static uint16_t h16_encode_rn(float v)
+{
+    _Float16 h = (_Float16)(v * 32768.0f);   /* nearest-even */
+    uint16_t b;
+    memcpy(&b, &h, 2);
+    return b;
+}
+
+/* add 13 random bits below the half's last mantissa bit, then truncate */
+static uint16_t h16_encode_sr(float v, uint32_t rnd)
+{
+    const float t = u2f(f2u(v * 32768.0f) + (rnd & 0x1FFFu));
+    float z;
+    if (fabsf(t) >= 6.103515625e-05f)          /* normal half range: keep 10 mantissa bits */
+        z = u2f(f2u(t) & ~0x1FFFu);
+    else                                        /* subnormal half: multiples of 2^-24 */
+        z = truncf(t * 16777216.0f) / 16777216.0f;
+    _Float16 h = (_Float16)z;                   /* exact */
+    uint16_t b;
+    memcpy(&b, &h, 2);
+    return b;
+}
+
+static float b16_decode(uint16_t b) { return u2f((uint32_t)b << 16); }
+
+static uint16_t b16_encode_rn(float v)
+{
+    const uint32_t u = f2u(v);
+    return (uint16_t)((u + 0x7FFFu + ((u >> 16) & 1u)) >> 16);
+}
+
+static uint16_t b16_encode_sr(float v, uint32_t rnd) { return (uint16_t)((f2u(v) + (rnd & 0xFFFFu)) >> 16); }
+
+static float s16_decode(int kind, uint16_t b) { return (kind & 1) ? b16_decode(b) : h16_decode(b); }
+
+static uint16_t s16_encode(int kind, float v, uint32_t cell, uint32_t d, uint32_t seed)
+{
+    switch (kind) {
+        case 0: return h16_encode_rn(v);
+        case 1: return b16_encode_rn(v);
+        case 2: return h16_encode_sr(v, orc_sr_bits(cell, d, seed));
+        default: return b16_encode_sr(v, orc_sr_bits(cell, d, seed));
+    }
+}
+
+/* One step with 16-bit storage; `t` is the index of the step being taken
+ * (0 for the first step after loading), which seeds stochastic rounding. */
+void orc_step_s16(int kind, int64_t nx, int64_t ny, int64_t nz, const uint32_t *flag,
+                  const float *rho, const float *vx, const float *vy, const float *vz,
+                  float inv_tau, const uint16_t *src, uint16_t *dst, uint32_t t)
+{
+    const int64_t n = nx * ny * nz;
+    float *a = (float *)malloc(sizeof(float) * 27 * n);
+    float *b = (float *)malloc(sizeof(float) * 27 * n);
+    for (int64_t k = 0; k < 27 * n; ++k) {
+        a[k] = s16_decode(kind, src[k]);
+        b[k] = s16_decode(kind, dst[k]);
+    }
+    orc_step_f32(nx, ny, nz, flag, rho, vx, vy, vz, inv_tau, a, b);
+    const uint32_t seed = orc_step_seed(t);
+    for (int64_t d = 0; d < 27; ++d)
+        for (int64_t i = 0; i < n; ++i) {
+            if (flag[i] & ORC_STORE)
+                dst[d * n + i] = s16_encode(kind, b[d * n + i], (uint32_t)i, (uint32_t)d, seed);
+        }
+    free(a);
+    free(b);
+}
+
+/* Widen a 16-bit state to FP32 (for comparisons). */
+void orc_decode_s16(int kind, int64_t count, const uint16_t *src, float *out)
+{
+    for (int64_t k = 0; k < count; ++k) out[k] = s16_decode(kind, src[k]);
+}
+
+/* Narrow an FP32 state (rest state, imports) with nearest-even or the
+ * stochastic rule keyed on (cell, direction, seed of step t). */
+void orc_encode_s16(int kind, int64_t n, const float *src, uint16_t *out, uint32_t t)
+{
+    const uint32_t seed = orc_step_seed(t);
+    for (int64_t d = 0; d < 27; ++d)
+        for (int64_t i = 0; i < n; ++i)
+            out[d * n + i] = s16_encode(kind, src[d * n + i], (uint32_t)i, (uint32_t)d, seed);
+}
