@@ -34,7 +34,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "D3Q27 MLUPS, FP32 vs FP16-store at stated FP64 err; adjoint/forward cost"
-BYTES_PER_LUP = {"fp32": 216, "fp16": 108, "bf16": 108, "fp64": 432}
+BYTES_PER_LUP = {"fp32": 216, "fp16": 108, "bf16": 108, "fp16sr": 108, "bf16sr": 108, "fp64": 432}
 WORKLOAD = "288x272x280 channel, 40 seeded spheres r in [4,12], invTau 0.5, ux_in 0.05"
 
 
@@ -199,7 +199,7 @@ def fp64_errors(culbm, steps=1000):
     ref = fields("fp64")
     umag = np.sqrt(ref[1] ** 2 + ref[2] ** 2 + ref[3] ** 2)
     out = {}
-    for st in ("fp32", "fp16", "bf16"):
+    for st in ("fp32", "fp16", "fp16sr", "bf16", "bf16sr"):
         got = fields(st)
         du = np.sqrt(sum((got[k] - ref[k]) ** 2 for k in (1, 2, 3)))
         out[st] = {
@@ -300,8 +300,10 @@ def run_ours(args):
     for name, (sp, op, st, tile) in {
         "pull_fp32": (0, 0, "fp32", None),
         "inplace_fp16": (1, 0, "fp16", None),
+        "inplace_fp16sr": (1, 0, "fp16sr", None),
         "inplace_bf16": (1, 0, "bf16", None),
         "pull_fp16": (0, 0, "fp16", None),
+        "pull_fp16sr": (0, 0, "fp16sr", None),
         "blocked_inplace_fp32": (1, 3, "fp32", (144, 68, 40)),
     }.items():
         try:

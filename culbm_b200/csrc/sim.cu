@@ -223,27 +223,6 @@ culbm_status fill_rest(culbm_sim* s)
     return CULBM_OK;
 }
 
-// Indices of the cells on the domain boundary, x fastest (the in-place
-// steps give them their own launch).
-culbm_status build_edge_list(culbm_sim* s)
-{
-    const Domain& D = s->dom;
-    std::vector<int> list;
-    for (int z = 0; z < D.nz; ++z)
-        for (int y = 0; y < D.ny; ++y) {
-            const bool face = z == 0 || z == D.nz - 1 || y == 0 || y == D.ny - 1;
-            for (int x = 0; x < D.nx; ++x)
-                if (face || x == 0 || x == D.nx - 1) list.push_back(x + D.nx * (y + D.ny * z));
-        }
-    s->n_edge = static_cast<int>(list.size());
-    if (list.empty()) return CULBM_OK;
-    void* p = nullptr;
-    CULBM_TRY(dev_alloc(s, &p, list.size() * sizeof(int), "boundary cell list"));
-    s->d_edge_list = static_cast<int*>(p);
-    CULBM_CUDA(cudaMemcpy(s->d_edge_list, list.data(), list.size() * sizeof(int), cudaMemcpyHostToDevice));
-    return CULBM_OK;
-}
-
 template <typename S>
 culbm_status plain_steps(culbm_sim* s, uint32_t nsteps)
 {
@@ -260,18 +239,18 @@ culbm_status plain_steps(culbm_sim* s, uint32_t nsteps)
         } else {
             auto a = make_args<S>(s, 0, 0);
             a.seed = seed;
-            const int ne = s->n_edge;
-            const dim3 ge((ne + 255) / 256);
+            const int ri = row_count(s->dom, ROWS_INNER), ro = row_count(s->dom, ROWS_OUTER);
+            const dim3 gi((s->dom.nx + 31) / 32, (ri + 7) / 8), go((s->dom.nx + 31) / 32, (ro + 7) / 8);
             if (s->aa_phase == 0) {
-                k_aa_odd<S, R, false><<<g, b, 0, s->stream>>>(a, s->d_edge_list, ne);
-                if (ne) k_aa_odd<S, R, true><<<ge, 256, 0, s->stream>>>(a, s->d_edge_list, ne);
+                if (ri) k_aa_odd<S, R, ROWS_INNER><<<gi, b, 0, s->stream>>>(a);
+                if (ro) k_aa_odd<S, R, ROWS_OUTER><<<go, b, 0, s->stream>>>(a);
             } else {
-                k_aa_even<S, R, false><<<g, b, 0, s->stream>>>(a, s->d_edge_list, ne);
-                if (ne) k_aa_even<S, R, true><<<ge, 256, 0, s->stream>>>(a, s->d_edge_list, ne);
+                if (ri) k_aa_even<S, R, ROWS_INNER><<<gi, b, 0, s->stream>>>(a);
+                if (ro) k_aa_even<S, R, ROWS_OUTER><<<go, b, 0, s->stream>>>(a);
             }
             CULBM_CUDA(cudaGetLastError());
             s->aa_phase ^= 1;
-            s->launches += ne ? 1 : 0;
+            s->launches += (ri ? 1 : 0) + (ro ? 1 : 0) - 1;
         }
         s->launches += 1;
     }
@@ -328,7 +307,6 @@ void release(culbm_sim* s)
     for (auto& p : s->d_mac) cudaFree(p);
     for (auto& p : s->d_pop) cudaFree(p);
     cudaFree(s->d_edge);
-    cudaFree(s->d_edge_list);
     cudaFree(s->d_red);
     if (s->ev0) cudaEventDestroy(s->ev0);
     if (s->ev1) cudaEventDestroy(s->ev1);
@@ -473,7 +451,6 @@ culbm_status culbm_create(const culbm_config* cfg, culbm_sim** out)
         s->red_blocks = 592;
         CULBM_TRY(dev_alloc(s, reinterpret_cast<void**>(&s->d_red), (4ull * s->red_blocks + 4) * sizeof(double),
                             "reduction scratch"));
-        if (inplace) CULBM_TRY(build_edge_list(s));
         if (blocked) CULBM_TRY(tiles_create(s));
         const float* none[4] = {nullptr, nullptr, nullptr, nullptr};
         CULBM_TRY(upload_state(s, nullptr, none));

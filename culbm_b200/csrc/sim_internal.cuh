@@ -59,8 +59,6 @@ struct culbm_sim {
     void* d_edge = nullptr;         // in-place clamp side buffer
     culbm::EdgeLayout el{};
     long long edge_elems = 0;
-    int* d_edge_list = nullptr;     // in-place: boundary cell indices
-    int n_edge = 0;
     size_t esize = 4;               // bytes per stored population
     double* d_red = nullptr;        // reduction partials
     int red_blocks = 0;

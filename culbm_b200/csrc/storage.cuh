@@ -85,8 +85,9 @@ template <typename S> struct IsSR { static constexpr bool value = false; };
 template <> struct IsSR<Half16SR> { static constexpr bool value = true; };
 template <> struct IsSR<BF16SR> { static constexpr bool value = true; };
 
-// Per-step seed and per-value random bits (integer mixing in the style of
-// the murmur3 finaliser).
+// Per-step seed, per-cell hash (one per cell and step) and per-direction
+// random bits.  Integer mixing in the style of the murmur3 finaliser; the
+// per-direction bits are a multiplicative hash whose high bits are used.
 __host__ __device__ __forceinline__ uint32_t step_seed(uint32_t t)
 {
     uint32_t h = t * 0x9E3779B1u + 0x7F4A7C15u;
@@ -98,15 +99,20 @@ __host__ __device__ __forceinline__ uint32_t step_seed(uint32_t t)
     return h;
 }
 
-__device__ __forceinline__ uint32_t sr_bits(uint32_t cell, uint32_t d, uint32_t seed)
+__device__ __forceinline__ uint32_t cell_hash(uint32_t cell, uint32_t seed)
 {
-    uint32_t h = cell * 0x27D4EB2Fu ^ seed ^ (d * 0x165667B1u);
-    h ^= h >> 15;
-    h *= 0x2C1B3C6Du;
-    h ^= h >> 12;
-    h *= 0x297A2D39u;
-    h ^= h >> 15;
+    uint32_t h = cell * 0x27D4EB2Fu ^ seed;
+    h ^= h >> 16;
+    h *= 0x85EBCA6Bu;
+    h ^= h >> 13;
+    h *= 0xC2B2AE35u;
+    h ^= h >> 16;
     return h;
+}
+
+__device__ __forceinline__ uint32_t dir_bits(uint32_t hcell, uint32_t d)
+{
+    return (hcell ^ (d * 0x9E3779B9u)) * 0x2C1B3C6Du;
 }
 
 template <> struct Cvt<Half16SR, float> {
@@ -123,10 +129,11 @@ template <> struct Cvt<Half16SR, float> {
     {
         p->bits = __half_as_ushort(__float2half_rn(__fmul_rn(v, kHalfScale)));
     }
-    // stochastic: add 13 random bits below the half's last mantissa bit, truncate
+    // stochastic: add 13 random bits (the high bits of rnd) below the half's
+    // last mantissa bit, truncate
     static __device__ __forceinline__ unsigned short enc(float v, uint32_t rnd)
     {
-        const uint32_t u = __float_as_uint(__fmul_rn(v, kHalfScale)) + (rnd & 0x1FFFu);
+        const uint32_t u = __float_as_uint(__fmul_rn(v, kHalfScale)) + (rnd >> 19);
         return __half_as_ushort(__float2half_rz(__uint_as_float(u)));
     }
     static __device__ __forceinline__ void st_sr(Half16SR* p, float v, uint32_t rnd) { p->bits = enc(v, rnd); }
@@ -145,28 +152,29 @@ template <> struct Cvt<BF16SR, float> {
     }
     static __device__ __forceinline__ unsigned short enc(float v, uint32_t rnd)
     {
-        return static_cast<unsigned short>((__float_as_uint(v) + (rnd & 0xFFFFu)) >> 16);
+        return static_cast<unsigned short>((__float_as_uint(v) + (rnd >> 16)) >> 16);
     }
     static __device__ __forceinline__ void st_sr(BF16SR* p, float v, uint32_t rnd) { p->bits = enc(v, rnd); }
     static __device__ __forceinline__ void st_sr_cs(BF16SR* p, float v, uint32_t rnd) { __stcs(&p->bits, enc(v, rnd)); }
 };
 
-// Store of population d of cell `cell` at time step `seed` names: stochastic
-// rounding for the SR formats, the format's plain conversion otherwise.
+// Store of population d of the cell whose cell_hash for this step is hcell:
+// stochastic rounding for the SR formats, the format's plain conversion
+// otherwise (hcell then goes unused and its computation is dropped).
 template <typename S, typename R>
-__device__ __forceinline__ void put(S* p, R v, uint32_t cell, int d, uint32_t seed)
+__device__ __forceinline__ void put(S* p, R v, uint32_t hcell, int d)
 {
     if constexpr (IsSR<S>::value)
-        Cvt<S, R>::st_sr(p, v, sr_bits(cell, d, seed));
+        Cvt<S, R>::st_sr(p, v, dir_bits(hcell, d));
     else
         Cvt<S, R>::st(p, v);
 }
 
 template <typename S, typename R>
-__device__ __forceinline__ void put_cs(S* p, R v, uint32_t cell, int d, uint32_t seed)
+__device__ __forceinline__ void put_cs(S* p, R v, uint32_t hcell, int d)
 {
     if constexpr (IsSR<S>::value)
-        Cvt<S, R>::st_sr_cs(p, v, sr_bits(cell, d, seed));
+        Cvt<S, R>::st_sr_cs(p, v, dir_bits(hcell, d));
     else
         Cvt<S, R>::st_cs(p, v);
 }

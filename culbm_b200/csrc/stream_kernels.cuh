@@ -226,7 +226,7 @@ __global__ void __launch_bounds__(256) k_pull_step(const __grid_constant__ StepA
     cell_update<R>(op, a.inv_tau, a.rho, a.vx, a.vy, a.vz, c.i, f);
     if (op & OP_STORE) {
 #pragma unroll
-        for (int d = 0; d < 27; ++d) put(a.dst.p[d] + c.i, f[d], c.i, d, a.seed);
+        for (int d = 0; d < 27; ++d) put(a.dst.p[d] + c.i, f[d], cell_hash(static_cast<uint32_t>(c.i), a.seed), d);
     }
 }
 
@@ -238,42 +238,84 @@ __global__ void __launch_bounds__(256) k_pull_step(const __grid_constant__ StepA
 // for_each_clamp_reader) also writes f_d into slot d of each such y: nobody
 // else reads or writes that slot during the step, and y reads it next step.
 //
-// Interior and boundary cells touch disjoint locations, so each in-place step
-// runs as two launches: EDGE = false covers the interior with straight-line
-// code (boundary threads return at once), EDGE = true walks the list of
-// boundary cells with the clamp logic.  Keeping the long clamp code out of
-// the interior kernel keeps its instruction footprint small.
-template <typename S, typename R, bool EDGE>
-__device__ __forceinline__ bool aa_cell(const StepArgs<S, R>& a, const int* edge_list, int n_edge, CellCoord& c)
+// Each in-place step runs as two launches over disjoint sets of x-rows (cells
+// of different rows never touch the same locations in a step's pattern, so
+// the order does not matter):
+//   ROWS_INNER: rows with 0 < y < ny-1 and 0 < z < nz-1.  Only the x-faces
+//     of such a row are on the boundary, and there only the x component of a
+//     pull can leave the domain, so the clamp handling reduces to pointer
+//     selects and predicated stores; the code stays straight-line.
+//   ROWS_OUTER: rows on a y or z face, processed with the general per-axis
+//     clamp code (about 2 (ny + nz) of the ny*nz rows).
+// Rows are contiguous in x, so both launches keep warp accesses coalesced.
+enum RowSet : int { ROWS_INNER = 0, ROWS_OUTER = 1 };
+
+// Cell of this thread for a row set; false if the thread has none.
+template <int ROWS>
+__device__ __forceinline__ bool row_cell(const Domain& D, CellCoord& c)
 {
-    const Domain& D = a.dom;
-    if (!EDGE) {
-        c = cell_of_thread(D);
-        return c.valid && c.x > 0 && c.x < D.nx - 1 && c.y > 0 && c.y < D.ny - 1 && c.z > 0 && c.z < D.nz - 1;
+    c.x = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c.x >= D.nx) return false;
+    const int r = blockIdx.y * blockDim.y + threadIdx.y;
+    if (ROWS == ROWS_INNER) {
+        const int iy = D.ny - 2;
+        if (iy <= 0 || D.nz <= 2) return false;
+        c.y = 1 + r % iy;
+        c.z = 1 + r / iy;
+        if (c.z > D.nz - 2) return false;
+    } else {
+        // z = 0 plane, z = nz-1 plane (all y), then y = 0 and y = ny-1 for 0 < z < nz-1
+        const int nzf = (D.nz > 1 ? 2 : 1);
+        if (r < nzf * D.ny) {
+            c.y = r % D.ny;
+            c.z = (r / D.ny) ? D.nz - 1 : 0;
+        } else {
+            const int q = r - nzf * D.ny;
+            const int nyf = (D.ny > 1 ? 2 : 1);
+            if (D.nz <= 2 || q >= nyf * (D.nz - 2)) return false;
+            c.z = 1 + q / nyf;
+            c.y = (q % nyf) ? D.ny - 1 : 0;
+        }
     }
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n_edge) return false;
-    c.i = edge_list[t];
-    c.x = c.i % D.nx;
-    c.y = (c.i / D.nx) % D.ny;
-    c.z = c.i / D.nxy;
+    c.i = c.x + D.nx * (c.y + D.ny * c.z);
     c.valid = true;
     return true;
 }
 
-template <typename S, typename R, bool EDGE>
-__global__ void __launch_bounds__(256) k_aa_odd(const __grid_constant__ StepArgs<S, R> a, const int* edge_list,
-                                                int n_edge)
+// Number of rows in a row set (host side launch size).
+inline int row_count(const Domain& D, int rows)
+{
+    if (rows == ROWS_INNER) return (D.ny > 2 && D.nz > 2) ? (D.ny - 2) * (D.nz - 2) : 0;
+    const int nzf = D.nz > 1 ? 2 : 1, nyf = D.ny > 1 ? 2 : 1;
+    return nzf * D.ny + (D.nz > 2 ? nyf * (D.nz - 2) : 0);
+}
+
+template <typename S>
+__device__ __forceinline__ const S* xface_edge_ptr(const S* edge, const Domain& D, const EdgeLayout& L, int side,
+                                                   int d, int y, int z)
+{
+    const int j = (cy_of(d) + 1) + 3 * (cz_of(d) + 1);
+    return edge + L.off[side] + (long long)j * D.ny * D.nz + y + (long long)D.ny * z;
+}
+
+template <typename S, typename R, int ROWS>
+__global__ void __launch_bounds__(256) k_aa_odd(const __grid_constant__ StepArgs<S, R> a)
 {
     CellCoord c;
-    if (!aa_cell<S, R, EDGE>(a, edge_list, n_edge, c)) return;
     const Domain& D = a.dom;
+    if (!row_cell<ROWS>(D, c)) return;
     const uint8_t op = a.ops[c.i];
+    const uint32_t hc = cell_hash(static_cast<uint32_t>(c.i), a.seed);
     R f[27];
     if (op & OP_LOAD) {
-        if (!EDGE) {
+        if (ROWS == ROWS_INNER) {
 #pragma unroll
-            for (int d = 0; d < 27; ++d) f[d] = Cvt<S, R>::ld(a.src.p[26 - d] + (c.i - nb_off(D, d)));
+            for (int d = 0; d < 27; ++d) {
+                const S* p = a.src.p[26 - d] + (c.i - nb_off(D, d));
+                if (cx_of(d) == 1 && c.x == 0) p = xface_edge_ptr(a.edge, D, a.el, 0, d, c.y, c.z);
+                if (cx_of(d) == -1 && c.x == D.nx - 1) p = xface_edge_ptr(a.edge, D, a.el, 1, d, c.y, c.z);
+                f[d] = Cvt<S, R>::ld(p);
+            }
         } else {
             load_pulled<LAYOUT_AA_A>(a, c.x, c.y, c.z, c.i, true, f);
         }
@@ -283,16 +325,23 @@ __global__ void __launch_bounds__(256) k_aa_odd(const __grid_constant__ StepArgs
     }
     cell_update<R>(op, a.inv_tau, a.rho, a.vx, a.vy, a.vz, c.i, f);
     if (!(op & OP_STORE)) return;
-    if (!EDGE) {
+    if (ROWS == ROWS_INNER) {
 #pragma unroll
-        for (int d = 0; d < 27; ++d) put(a.dst.p[d] + (c.i + nb_off(D, d)), f[d], c.i, d, a.seed);
+        for (int d = 0; d < 27; ++d) {
+            const int cx = cx_of(d);
+            S* p = a.dst.p[d] + (c.i + nb_off(D, d));
+            // streaming target x + c_d, unless it leaves the domain in x
+            if (cx == 0 || (cx == 1 && c.x < D.nx - 1) || (cx == -1 && c.x > 0)) put(p, f[d], hc, d);
+            // an x-face cell is the clamped source of the cell on its own face
+            if ((cx == 1 && c.x == 0) || (cx == -1 && c.x == D.nx - 1)) put(p - cx, f[d], hc, d);
+        }
     } else {
         for_dirs([&](auto dd) {
             constexpr int d = decltype(dd)::value;
             if (inside(D, c.x + cx_of(d), c.y + cy_of(d), c.z + cz_of(d)))
-                put(a.dst.p[d] + (c.i + nb_off(D, d)), f[d], c.i, d, a.seed);
+                put(a.dst.p[d] + (c.i + nb_off(D, d)), f[d], hc, d);
             for_each_clamp_reader<d>(D, c.x, c.y, c.z, [&](int yx, int yy, int yz) {
-                put(a.dst.p[d] + (yx + D.nx * (yy + D.ny * yz)), f[d], c.i, d, a.seed);
+                put(a.dst.p[d] + (yx + D.nx * (yy + D.ny * yz)), f[d], hc, d);
             });
         });
     }
@@ -302,14 +351,14 @@ __global__ void __launch_bounds__(256) k_aa_odd(const __grid_constant__ StepArgs
 // A cell that is the clamped source of boundary cells y also files f_d into
 // the edge-buffer slot of (y, d): the next odd step's clamped pull of y reads
 // it there, because slot 26-d of the source is overwritten during that step.
-// Only boundary cells can be clamped sources, so only EDGE = true does that.
-template <typename S, typename R, bool EDGE>
-__global__ void __launch_bounds__(256) k_aa_even(const __grid_constant__ StepArgs<S, R> a, const int* edge_list,
-                                                 int n_edge)
+template <typename S, typename R, int ROWS>
+__global__ void __launch_bounds__(256) k_aa_even(const __grid_constant__ StepArgs<S, R> a)
 {
     CellCoord c;
-    if (!aa_cell<S, R, EDGE>(a, edge_list, n_edge, c)) return;
+    const Domain& D = a.dom;
+    if (!row_cell<ROWS>(D, c)) return;
     const uint8_t op = a.ops[c.i];
+    const uint32_t hc = cell_hash(static_cast<uint32_t>(c.i), a.seed);
     R f[27];
     if (op & OP_LOAD) {
         load_pulled<LAYOUT_AA_B>(a, c.x, c.y, c.z, c.i, false, f);
@@ -320,13 +369,21 @@ __global__ void __launch_bounds__(256) k_aa_even(const __grid_constant__ StepArg
     cell_update<R>(op, a.inv_tau, a.rho, a.vx, a.vy, a.vz, c.i, f);
     if (!(op & OP_STORE)) return;
 #pragma unroll
-    for (int d = 0; d < 27; ++d) put(a.dst.p[26 - d] + c.i, f[d], c.i, d, a.seed);
-    if (EDGE) {
-        const Domain& D = a.dom;
+    for (int d = 0; d < 27; ++d) put(a.dst.p[26 - d] + c.i, f[d], hc, d);
+    if (ROWS == ROWS_INNER) {
+#pragma unroll
+        for (int d = 0; d < 27; ++d) {
+            const int cx = cx_of(d);
+            if (cx == 1 && c.x == 0)
+                put(const_cast<S*>(xface_edge_ptr(a.edge, D, a.el, 0, d, c.y + cy_of(d), c.z + cz_of(d))), f[d], hc, d);
+            if (cx == -1 && c.x == D.nx - 1)
+                put(const_cast<S*>(xface_edge_ptr(a.edge, D, a.el, 1, d, c.y + cy_of(d), c.z + cz_of(d))), f[d], hc, d);
+        }
+    } else {
         for_dirs([&](auto dd) {
             constexpr int d = decltype(dd)::value;
             for_each_clamp_reader<d>(D, c.x, c.y, c.z, [&](int yx, int yy, int yz) {
-                put(a.edge + edge_slot(D, a.el, yx, yy, yz, d), f[d], c.i, d, a.seed);
+                put(a.edge + edge_slot(D, a.el, yx, yy, yz, d), f[d], hc, d);
             });
         });
     }
@@ -379,11 +436,11 @@ __global__ void __launch_bounds__(256) k_import(const __grid_constant__ StepArgs
     for (int d = 0; d < 27; ++d) {
         const R v = R(in[(long long)d * D.n + c.i]);
         if (LAYOUT == LAYOUT_PULL) {
-            put(a.dst.p[d] + c.i, v, c.i, d, a.seed);
+            put(a.dst.p[d] + c.i, v, cell_hash(static_cast<uint32_t>(c.i), a.seed), d);
         } else if (LAYOUT == LAYOUT_PULL_RING) {
-            put(a.dst.p[d] + ring_index(a, c.x, c.y, c.z), v, c.i, d, a.seed);
+            put(a.dst.p[d] + ring_index(a, c.x, c.y, c.z), v, cell_hash(static_cast<uint32_t>(c.i), a.seed), d);
         } else {
-            put(a.dst.p[26 - d] + c.i, v, c.i, d, a.seed);
+            put(a.dst.p[26 - d] + c.i, v, cell_hash(static_cast<uint32_t>(c.i), a.seed), d);
             int sx = c.x - cx_of(d), sy = c.y - cy_of(d), sz = c.z - cz_of(d);
             if (!inside(D, sx, sy, sz)) {
                 if ((unsigned)sx >= (unsigned)D.nx) sx = c.x;
@@ -391,7 +448,7 @@ __global__ void __launch_bounds__(256) k_import(const __grid_constant__ StepArgs
                 if ((unsigned)sz >= (unsigned)D.nz) sz = c.z;
                 const int si = sx + D.nx * (sy + D.ny * sz);
                 const R w = R(in[(long long)d * D.n + si]);
-                put(a.edge + edge_slot(D, a.el, c.x, c.y, c.z, d), w, si, d, a.seed);
+                put(a.edge + edge_slot(D, a.el, c.x, c.y, c.z, d), w, cell_hash(static_cast<uint32_t>(si), a.seed), d);
             }
         }
     }

@@ -84,19 +84,20 @@ __device__ __forceinline__ R gload(const S* p)
 }
 
 template <typename S, typename R, bool HINT>
-__device__ __forceinline__ void gstore(S* p, R v, uint32_t cell, int d, uint32_t seed)
+__device__ __forceinline__ void gstore(S* p, R v, uint32_t hcell, int d)
 {
     if constexpr (HINT) {
-        put_cs(p, v, cell, d, seed);
+        put_cs(p, v, hcell, d);
     } else {
-        put(p, v, cell, d, seed);
+        put(p, v, hcell, d);
     }
 }
 
+// Per-cell stochastic-rounding hash of the step this launch performs.
 template <typename S, typename R>
-__device__ __forceinline__ uint32_t tile_seed(const TileArgs<S, R>& a)
+__device__ __forceinline__ uint32_t tile_hash(const TileArgs<S, R>& a, int gi)
 {
-    return step_seed(a.rs->step + static_cast<uint32_t>(a.j));
+    return cell_hash(static_cast<uint32_t>(gi), step_seed(a.rs->step + static_cast<uint32_t>(a.j)));
 }
 
 struct TileCell {
@@ -152,9 +153,9 @@ __device__ __forceinline__ void tile_store_global(const TileArgs<S, R>& a, const
     S* base = a.g.base[sel];
     const long long off = gaddr(a.g, a.dom, offz, c.gx, c.gy, c.gz);
 #pragma unroll
-    const uint32_t seed = tile_seed(a);
+    const uint32_t hc = tile_hash(a, c.gi);
 #pragma unroll
-    for (int d = 0; d < 27; ++d) gstore<S, R, HINT>(base + d * a.g.stride + off, f[d], c.gi, d, seed);
+    for (int d = 0; d < 27; ++d) gstore<S, R, HINT>(base + d * a.g.stride + off, f[d], hc, d);
 }
 
 // Selected buffers of the current round.
@@ -200,11 +201,11 @@ __device__ __forceinline__ void tile_load_aa(const TileArgs<S, R>& a, const Tile
 template <typename S, typename R>
 __device__ __forceinline__ void tile_file_clamp_sources(const TileArgs<S, R>& a, const TileCell& c, const R* f)
 {
-    const uint32_t seed = tile_seed(a);
+    const uint32_t hc = tile_hash(a, c.gi);
     for_dirs([&](auto dd) {
         constexpr int d = decltype(dd)::value;
         for_each_clamp_reader<d>(a.dom, c.gx, c.gy, c.gz, [&](int yx, int yy, int yz) {
-            put(a.edge + edge_slot(a.dom, a.el, yx, yy, yz, d), f[d], c.gi, d, seed);
+            put(a.edge + edge_slot(a.dom, a.el, yx, yy, yz, d), f[d], hc, d);
         });
     });
 }
@@ -230,7 +231,7 @@ __global__ void __launch_bounds__(256) k_tile_aa_first(const __grid_constant__ T
         if (c.correct) tile_store_global<S, R, HINT>(a, c, round_dst_sel(a.rs, ring), a.rs->dst_offz, f);
     } else {
 #pragma unroll
-        for (int d = 0; d < 27; ++d) put(a.t0.p[26 - d] + c.t, f[d], c.gi, d, tile_seed(a));
+        for (int d = 0; d < 27; ++d) put(a.t0.p[26 - d] + c.t, f[d], tile_hash(a, c.gi), d);
         if (op & OP_EDGE) tile_file_clamp_sources(a, c, f);
     }
 }
@@ -257,20 +258,20 @@ __global__ void __launch_bounds__(256) k_tile_aa_odd(const __grid_constant__ Til
     if (!edge && tile_inner) {
 #pragma unroll
         for (int d = 0; d < 27; ++d)
-            put(a.t0.p[d] + (c.t + cx_of(d) + cy_of(d) * a.bx + cz_of(d) * a.bxy), f[d], c.gi, d, tile_seed(a));
+            put(a.t0.p[d] + (c.t + cx_of(d) + cy_of(d) * a.bx + cz_of(d) * a.bxy), f[d], tile_hash(a, c.gi), d);
         return;
     }
     for_dirs([&](auto dd) {
         constexpr int d = decltype(dd)::value;
         constexpr int cx = cx_of(d), cy = cy_of(d), cz = cz_of(d);
         if (inside(D, c.gx + cx, c.gy + cy, c.gz + cz) && in_tile(c.px + cx, c.py + cy, c.pz + cz, a.bx, a.by, a.bz))
-            put(a.t0.p[d] + (c.t + cx + cy * a.bx + cz * a.bxy), f[d], c.gi, d, tile_seed(a));
+            put(a.t0.p[d] + (c.t + cx + cy * a.bx + cz * a.bxy), f[d], tile_hash(a, c.gi), d);
         if (edge) {
             // slot d of each boundary cell whose clamped pull reads this cell
             for_each_clamp_reader<d>(D, c.gx, c.gy, c.gz, [&](int yx, int yy, int yz) {
                 const int qx = yx - a.ox, qy = yy - a.oy, qz = yz - a.oz;
                 if (in_tile(qx, qy, qz, a.bx, a.by, a.bz))
-                    put(a.t0.p[d] + (qx + a.bx * (qy + a.by * qz)), f[d], c.gi, d, tile_seed(a));
+                    put(a.t0.p[d] + (qx + a.bx * (qy + a.by * qz)), f[d], tile_hash(a, c.gi), d);
             });
         }
     });
@@ -293,7 +294,7 @@ __global__ void __launch_bounds__(256) k_tile_aa_even(const __grid_constant__ Ti
     cell_update<R>(op, a.inv_tau, a.rho, a.vx, a.vy, a.vz, c.gi, f);
     if (!(op & OP_STORE)) return;
 #pragma unroll
-    for (int d = 0; d < 27; ++d) put(a.t0.p[26 - d] + c.t, f[d], c.gi, d, tile_seed(a));
+    for (int d = 0; d < 27; ++d) put(a.t0.p[26 - d] + c.t, f[d], tile_hash(a, c.gi), d);
     if (op & OP_EDGE) tile_file_clamp_sources(a, c, f);
 }
 
@@ -363,7 +364,7 @@ __global__ void __launch_bounds__(256) k_tile_pull_first(const __grid_constant__
         if (c.correct) tile_store_global<S, R, HINT>(a, c, round_dst_sel(a.rs, ring), a.rs->dst_offz, f);
     } else {
 #pragma unroll
-        for (int d = 0; d < 27; ++d) put(a.t0.p[d] + c.t, f[d], c.gi, d, tile_seed(a));
+        for (int d = 0; d < 27; ++d) put(a.t0.p[d] + c.t, f[d], tile_hash(a, c.gi), d);
     }
 }
 
@@ -384,7 +385,7 @@ __global__ void __launch_bounds__(256) k_tile_pull_mid(const __grid_constant__ T
     cell_update<R>(op, a.inv_tau, a.rho, a.vx, a.vy, a.vz, c.gi, f);
     if (!(op & OP_STORE)) return;
 #pragma unroll
-    for (int d = 0; d < 27; ++d) put(a.t1.p[d] + c.t, f[d], c.gi, d, tile_seed(a));
+    for (int d = 0; d < 27; ++d) put(a.t1.p[d] + c.t, f[d], tile_hash(a, c.gi), d);
 }
 
 template <typename S, typename R, bool HINT>

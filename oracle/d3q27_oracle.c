@@ -94,11 +94,14 @@ uint32_t orc_step_seed(uint32_t t)
     return h;
 }
 
+/* random bits of population d of `cell` at the step seeded by `seed`: a
+ * per-cell finaliser hash, then a per-direction multiplicative hash whose
+ * high bits are used */
 uint32_t orc_sr_bits(uint32_t cell, uint32_t d, uint32_t seed)
 {
-    uint32_t h = cell * 0x27D4EB2Fu ^ seed ^ (d * 0x165667B1u);
-    h ^= h >> 15; h *= 0x2C1B3C6Du; h ^= h >> 12; h *= 0x297A2D39u; h ^= h >> 15;
-    return h;
+    uint32_t h = cell * 0x27D4EB2Fu ^ seed;
+    h ^= h >> 16; h *= 0x85EBCA6Bu; h ^= h >> 13; h *= 0xC2B2AE35u; h ^= h >> 16;
+    return (h ^ (d * 0x9E3779B9u)) * 0x2C1B3C6Du;
 }
 
 static float h16_decode(uint16_t h)
@@ -116,10 +119,11 @@ static uint16_t h16_encode_rn(float v)
     return b;
 }
 
-/* add 13 random bits below the half's last mantissa bit, then truncate */
+/* add 13 random bits (the high bits of rnd) below the half's last mantissa
+ * bit, then truncate */
 static uint16_t h16_encode_sr(float v, uint32_t rnd)
 {
-    const float t = u2f(f2u(v * 32768.0f) + (rnd & 0x1FFFu));
+    const float t = u2f(f2u(v * 32768.0f) + (rnd >> 19));
     float z;
     if (fabsf(t) >= 6.103515625e-05f)          /* normal half range: keep 10 mantissa bits */
         z = u2f(f2u(t) & ~0x1FFFu);
@@ -139,7 +143,7 @@ static uint16_t b16_encode_rn(float v)
     return (uint16_t)((u + 0x7FFFu + ((u >> 16) & 1u)) >> 16);
 }
 
-static uint16_t b16_encode_sr(float v, uint32_t rnd) { return (uint16_t)((f2u(v) + (rnd & 0xFFFFu)) >> 16); }
+static uint16_t b16_encode_sr(float v, uint32_t rnd) { return (uint16_t)((f2u(v) + (rnd >> 16)) >> 16); }
 
 static float s16_decode(int kind, uint16_t b) { return (kind & 1) ? b16_decode(b) : h16_decode(b); }
 

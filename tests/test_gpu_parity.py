@@ -170,3 +170,22 @@ def test_dump_files_layout(culbm, orc, tmp_path):
             assert not p.exists()
             continue
         assert_bitwise(np.fromfile(p, dtype="<f4"), w, k)
+
+
+@pytest.mark.parametrize("dims", [(1, 5, 4), (5, 1, 4), (5, 4, 1), (2, 2, 2), (3, 2, 5), (7, 3, 2), (33, 3, 3),
+                                  (40, 6, 5)])
+def test_degenerate_domains_bitwise(culbm, orc, dims):
+    """Thin domains: every row set, x-face and clamp combination of the
+    in-place kernels, against the oracle's pull with the per-axis clamp."""
+    sc = S.default_scene(*dims)
+    rng = np.random.default_rng(sum(dims))
+    state0 = (0.01 * rng.standard_normal(27 * sc.n)).astype(np.float32)
+    o = oracle_scene(orc, sc)
+    for nsteps in (1, 2, 5):
+        want = orc.pulled(o, orc.run(o, 0.8, nsteps, state=state0))
+        for policy in PLAIN:
+            with make_sim(culbm, dims, policy, inv_tau=0.8) as sim:
+                sim.load_state(*sc.arrays())
+                sim.set_ddf(state0)
+                sim.step(nsteps)
+                assert_bitwise(sim.pulled_ddf(), want, f"{dims} {policy} {nsteps}")
