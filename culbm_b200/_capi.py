@@ -34,6 +34,8 @@ EXPORTED = (
     "culbm_step", "culbm_step_timed", "culbm_synchronize", "culbm_moments", "culbm_get_field", "culbm_dump",
     "culbm_get_step", "culbm_get_pulled_ddf", "culbm_set_ddf", "culbm_mass_momentum", "culbm_get_info",
     "culbm_last_error", "culbm_status_string", "culbm_abi_version", "culbm_debug_inject_cuda_error",
+    "culbm_adj_config_init", "culbm_adj_create", "culbm_adj_destroy", "culbm_adj_set_state",
+    "culbm_adj_set_inv_tau", "culbm_adj_forward", "culbm_adj_gradient", "culbm_adj_get_info",
 )
 
 
@@ -71,6 +73,34 @@ class Info(C.Structure):
         ("persisting_l2_bytes", C.c_uint64),
         ("kernel_launches_per_step_x1000", C.c_uint32),
         ("reserved", C.c_uint32 * 7),
+    ]
+
+
+class AdjConfig(C.Structure):
+    _fields_ = [
+        ("dev_id", C.c_int32),
+        ("domain_dim", C.c_uint32 * 3),
+        ("inv_tau", C.c_float),
+        ("window", C.c_int32 * 2),
+        ("plane_x", C.c_int32 * 2),
+        ("checkpoint_every", C.c_int32),
+        ("precision", C.c_int32),
+        ("storage", C.c_int32),
+        ("hbm_budget_bytes", C.c_uint64),
+        ("reserved", C.c_uint32 * 8),
+    ]
+
+
+class AdjInfo(C.Structure):
+    _fields_ = [
+        ("checkpoint_every", C.c_int32),
+        ("checkpoints", C.c_int32),
+        ("device_bytes", C.c_uint64),
+        ("forward_ms", C.c_float),
+        ("recompute_ms", C.c_float),
+        ("adjoint_ms", C.c_float),
+        ("steps", C.c_uint64),
+        ("reserved", C.c_uint32 * 8),
     ]
 
 
@@ -115,6 +145,14 @@ def lib():
     L.culbm_abi_version.restype = C.c_int32
     L.culbm_debug_inject_cuda_error.argtypes = [C.c_int32, C.c_int32]
     L.culbm_debug_inject_cuda_error.restype = None
+    L.culbm_adj_config_init.argtypes = [C.POINTER(AdjConfig)]
+    L.culbm_adj_create.argtypes = [C.POINTER(AdjConfig), C.POINTER(vp)]
+    L.culbm_adj_destroy.argtypes = [vp]
+    L.culbm_adj_set_state.argtypes = [vp, vp, vp, vp, vp, vp, vp]
+    L.culbm_adj_set_inv_tau.argtypes = [vp, C.c_double]
+    L.culbm_adj_forward.argtypes = [vp, C.POINTER(C.c_double)]
+    L.culbm_adj_gradient.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_double), vp, vp]
+    L.culbm_adj_get_info.argtypes = [vp, C.POINTER(AdjInfo)]
     _lib = L
     return L
 

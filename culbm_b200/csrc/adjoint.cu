@@ -1,0 +1,795 @@
+// Discrete adjoint of the D3Q27 BGK step with a soft-obstacle field, for the
+// pressure-drop objective declared in include/culbm.h (culbm_adj_*).  No
+// reference counterpart: cuLBM has no gradient code.
+//
+// Forward step (one thread per cell, pull with the reference's per-axis clamp):
+//     f1 = EQU ? feq(rho_in, u_in) : f          (f pulled from the state)
+//     f2 = BOUNCE_BACK ? B(f1) : f1              (B(g)_d = g_{26-d})
+//     f3 = COLLIDE ? C(f2) + s (B(f2) - C(f2)) : f2,   C = BGK with rate w = invTau
+// stored back for every STORE cell.  With s = 0 this is the plain step bit
+// for bit (the soft term is skipped, not multiplied by zero).
+//
+// Adjoint step (reverse time, one thread per cell s):
+//   * gather: lambda_d(s) = sum of nu_d(y) over the cells y whose pull of
+//     direction d reads s (y = s + c_d and, at the boundary, the clamp readers)
+//     - the transpose of the pull, written as a gather so no atomics are needed;
+//   * reverse of the cell update with the Jacobian of C written out:
+//     (J_C^T l)_e = (1-w) l_e + w [a_rho + c_e.b - u.b],
+//     a_rho = L0 + 3 Lcu + 9/2 Lcu2 - 3/2 |u|^2 L0,  b = 3 L + 9 Lccu - 3 u L0,
+//     with L0 = sum w_d l_d, L = sum w_d l_d c_d, Lcu = sum w_d l_d (c_d.u),
+//     Lcu2 = sum w_d l_d (c_d.u)^2, Lccu = sum w_d l_d c_d (c_d.u);
+//   * nu(s) = adjoint of the pulled populations, plus dJ/df of the objective;
+//   * per-cell FP64 accumulators: dJ/ds += <l, B(f2) - C(f2)>,
+//     dJ/dw += (1-s) <l, feq - f2>, and at EQU cells dJ/d(rho_in, u_in) from
+//     d feq/d(rho, u).
+// States are recomputed from checkpoints taken every K steps.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "sim_internal.cuh"
+
+namespace culbm {
+namespace adj {
+
+template <typename S, typename R>
+struct Args {
+    Domain dom;
+    const uint8_t* ops;
+    const float* rho;
+    const float* vx;
+    const float* vy;
+    const float* vz;
+    const float* soft;
+    R inv_tau;
+    Pops<S> src;      // state F^t
+    Pops<S> dst;      // forward: F^{t+1}
+    R* nu_in[27];     // adjoint: nu^{t+1}
+    R* nu_out[27];    // adjoint: nu^t
+    double* g_soft;
+    double* g_tau;
+    double* g_mac[4];
+    int plane_in, plane_out;
+    R obj_in, obj_out;   // dJ/df_d of one in/out plane cell at this time (0 outside the window)
+    uint32_t seed;
+};
+
+// Pull of the 27 populations of cell (x, y, z) from the state a.src with the
+// per-axis clamp (the same rule as the plain pull step).
+template <typename S, typename R>
+__device__ __forceinline__ void pull_state(const Args<S, R>& a, int x, int y, int z, int i, R* f)
+{
+    const Domain& D = a.dom;
+    const int ndx = (x == 0) ? 0 : -1, pdx = (x == D.nx - 1) ? 0 : 1;
+    const int ndy = (y == 0) ? 0 : -D.nx, pdy = (y == D.ny - 1) ? 0 : D.nx;
+    const int ndz = (z == 0) ? 0 : -D.nxy, pdz = (z == D.nz - 1) ? 0 : D.nxy;
+#pragma unroll
+    for (int d = 0; d < 27; ++d) {
+        const int ox = cx_of(d) == 1 ? ndx : cx_of(d) == -1 ? pdx : 0;
+        const int oy = cy_of(d) == 1 ? ndy : cy_of(d) == -1 ? pdy : 0;
+        const int oz = cz_of(d) == 1 ? ndz : cz_of(d) == -1 ? pdz : 0;
+        f[d] = Cvt<S, R>::ld(a.src.p[d] + (i + ox + oy + oz));
+    }
+}
+
+// Boundary handling and soft collision of the forward model (in place on f).
+template <typename R>
+__device__ __forceinline__ void soft_update(uint8_t op, R inv_tau, R s, const float* rho, const float* vx,
+                                            const float* vy, const float* vz, int i, R* f)
+{
+    using A = Rn<R>;
+    if (op & OP_EQU) equilibrium<R>(R(rho[i]), R(vx[i]), R(vy[i]), R(vz[i]), f);
+    if (op & OP_BB) {
+#pragma unroll
+        for (int d = 0; d < 13; ++d) {
+            const R t = f[d];
+            f[d] = f[26 - d];
+            f[26 - d] = t;
+        }
+    }
+    if (!(op & OP_COLLIDE)) return;
+    R r, ux, uy, uz;
+    moments(f, r, ux, uy, uz);
+    EquTerms<R> t;
+    equ_terms(r, ux, uy, uz, t);
+    const R om = A::sub(R(1), inv_tau);
+    const bool soft = s != R(0);
+#pragma unroll
+    for (int d = 0; d < 13; ++d) {
+        const int e = 26 - d;
+        const R fd = f[d], fe = f[e];
+        const R cd = bgk_relax(t, inv_tau, om, d, fd);
+        const R ce = bgk_relax(t, inv_tau, om, e, fe);
+        f[d] = soft ? A::add(cd, A::mul(s, A::sub(fe, cd))) : cd;
+        f[e] = soft ? A::add(ce, A::mul(s, A::sub(fd, ce))) : ce;
+    }
+    const R c13 = bgk_relax(t, inv_tau, om, 13, f[13]);
+    f[13] = soft ? A::add(c13, A::mul(s, A::sub(f[13], c13))) : c13;
+}
+
+template <typename S, typename R>
+__global__ void __launch_bounds__(256) k_soft_step(const __grid_constant__ Args<S, R> a)
+{
+    const CellCoord c = cell_of_thread(a.dom);
+    if (!c.valid) return;
+    const uint8_t op = a.ops[c.i];
+    R f[27];
+    if (op & OP_LOAD) {
+        pull_state(a, c.x, c.y, c.z, c.i, f);
+    } else {
+#pragma unroll
+        for (int d = 0; d < 27; ++d) f[d] = R(0);
+    }
+    soft_update<R>(op, a.inv_tau, R(a.soft[c.i]), a.rho, a.vx, a.vy, a.vz, c.i, f);
+    if (op & OP_STORE) {
+        const uint32_t hc = cell_hash(static_cast<uint32_t>(c.i), a.seed);
+#pragma unroll
+        for (int d = 0; d < 27; ++d) put(a.dst.p[d] + c.i, f[d], hc, d);
+    }
+}
+
+// Deterministic sum of rho over the COLLIDE cells of plane x = px: one block.
+template <typename S, typename R>
+__global__ void __launch_bounds__(1024) k_plane_rho(const __grid_constant__ Args<S, R> a, int px, double* out)
+{
+    const Domain& D = a.dom;
+    double acc = 0.0;
+    for (int q = threadIdx.x; q < D.ny * D.nz; q += blockDim.x) {
+        const int y = q % D.ny, z = q / D.ny;
+        const int i = px + D.nx * (y + D.ny * z);
+        if (!(a.ops[i] & OP_COLLIDE)) continue;
+        R f[27], r, ux, uy, uz;
+        pull_state(a, px, y, z, i, f);
+        moments(f, r, ux, uy, uz);
+        acc += static_cast<double>(r);
+    }
+    __shared__ double sh[1024];
+    sh[threadIdx.x] = acc;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *out = sh[0];
+}
+
+// Per-population weights of the objective at time t, for every cell.
+template <typename S, typename R>
+__device__ __forceinline__ R objective_term(const Args<S, R>& a, int x, uint8_t op)
+{
+    if (!(op & OP_COLLIDE)) return R(0);
+    R g = R(0);
+    if (x == a.plane_in) g += a.obj_in;
+    if (x == a.plane_out) g += a.obj_out;
+    return g;
+}
+
+// nu^T: the objective's dJ/df at the last state only.
+template <typename S, typename R>
+__global__ void __launch_bounds__(256) k_adj_init(const __grid_constant__ Args<S, R> a)
+{
+    const CellCoord c = cell_of_thread(a.dom);
+    if (!c.valid) return;
+    const R g = objective_term(a, c.x, a.ops[c.i]);
+#pragma unroll
+    for (int d = 0; d < 27; ++d) a.nu_out[d][c.i] = g;
+}
+
+// (a_rho, b) of sum_d l_d d feq_d / d(rho, u) at velocity u: a_rho and
+// rho * b are the rho and u components (see the file header).
+template <typename R>
+__device__ __forceinline__ void feq_vjp(const R* l, R ux, R uy, R uz, R& a_rho, R& bx, R& by, R& bz)
+{
+    R L0 = 0, Lx = 0, Ly = 0, Lz = 0, Lcu = 0, Lcu2 = 0, Lccx = 0, Lccy = 0, Lccz = 0;
+#pragma unroll
+    for (int d = 0; d < 27; ++d) {
+        const R cx = R(cx_of(d)), cy = R(cy_of(d)), cz = R(cz_of(d));
+        const R wl = weight<R>(d) * l[d];
+        const R cu = cx * ux + cy * uy + cz * uz;
+        L0 += wl;
+        Lx += wl * cx;
+        Ly += wl * cy;
+        Lz += wl * cz;
+        Lcu += wl * cu;
+        Lcu2 += wl * cu * cu;
+        Lccx += wl * cx * cu;
+        Lccy += wl * cy * cu;
+        Lccz += wl * cz * cu;
+    }
+    const R uu = ux * ux + uy * uy + uz * uz;
+    a_rho = L0 + R(3) * Lcu + R(4.5) * Lcu2 - R(1.5) * uu * L0;
+    bx = R(3) * Lx + R(9) * Lccx - R(3) * ux * L0;
+    by = R(3) * Ly + R(9) * Lccy - R(3) * uy * L0;
+    bz = R(3) * Lz + R(9) * Lccz - R(3) * uz * L0;
+}
+
+template <typename S, typename R>
+__global__ void __launch_bounds__(256) k_adj_step(const __grid_constant__ Args<S, R> a)
+{
+    const CellCoord c = cell_of_thread(a.dom);
+    if (!c.valid) return;
+    const Domain& D = a.dom;
+    const uint8_t op = a.ops[c.i];
+    R l[27];
+    // lambda: adjoint of this cell's stored populations, gathered from the
+    // cells that pull them
+    if (op & OP_STORE) {
+        if (!(op & OP_EDGE)) {
+#pragma unroll
+            for (int d = 0; d < 27; ++d) l[d] = a.nu_in[d][c.i + nb_off(D, d)];
+        } else {
+            for_dirs([&](auto dd) {
+                constexpr int d = decltype(dd)::value;
+                R v = inside(D, c.x + cx_of(d), c.y + cy_of(d), c.z + cz_of(d)) ? a.nu_in[d][c.i + nb_off(D, d)] : R(0);
+                for_each_clamp_reader<d>(D, c.x, c.y, c.z,
+                                         [&](int yx, int yy, int yz) { v += a.nu_in[d][yx + D.nx * (yy + D.ny * yz)]; });
+                l[d] = v;
+            });
+        }
+    } else {
+#pragma unroll
+        for (int d = 0; d < 27; ++d) l[d] = R(0);
+    }
+    // forward populations of this cell at step t, then its intermediate f2
+    R f[27];
+    if (op & OP_LOAD) {
+        pull_state(a, c.x, c.y, c.z, c.i, f);
+    } else {
+#pragma unroll
+        for (int d = 0; d < 27; ++d) f[d] = R(0);
+    }
+    if (op & OP_EQU) equilibrium<R>(R(a.rho[c.i]), R(a.vx[c.i]), R(a.vy[c.i]), R(a.vz[c.i]), f);
+    if (op & OP_BB) {
+#pragma unroll
+        for (int d = 0; d < 13; ++d) {
+            const R t = f[d];
+            f[d] = f[26 - d];
+            f[26 - d] = t;
+        }
+    }
+    if (op & OP_COLLIDE) {
+        const R s = R(a.soft[c.i]);
+        const R w = a.inv_tau, om = R(1) - w;
+        R r, ux, uy, uz;
+        moments(f, r, ux, uy, uz);
+        EquTerms<R> t;
+        equ_terms(r, ux, uy, uz, t);
+        // parameter sensitivities at this step
+        R gs = 0, gw = 0;
+#pragma unroll
+        for (int d = 0; d < 27; ++d) {
+            const R feq = equ_any(t, d);
+            const R cd = w * feq + om * f[d];
+            gs += l[d] * (f[26 - d] - cd);
+            gw += l[d] * (feq - f[d]);
+        }
+        a.g_soft[c.i] += static_cast<double>(gs);
+        a.g_tau[c.i] += static_cast<double>((R(1) - s) * gw);
+        // lambda2 = (1-s) J_C^T lambda + s B(lambda)
+        R ar, bx, by, bz;
+        feq_vjp(l, ux, uy, uz, ar, bx, by, bz);
+        const R ub = ux * bx + uy * by + uz * bz;
+#pragma unroll
+        for (int d = 0; d < 13; ++d) {
+            const int e = 26 - d;
+            const R ld = l[d], le = l[e];
+            const R jd = om * ld + w * (ar + R(cx_of(d)) * bx + R(cy_of(d)) * by + R(cz_of(d)) * bz - ub);
+            const R je = om * le + w * (ar + R(cx_of(e)) * bx + R(cy_of(e)) * by + R(cz_of(e)) * bz - ub);
+            l[d] = (R(1) - s) * jd + s * le;
+            l[e] = (R(1) - s) * je + s * ld;
+        }
+        l[13] = (R(1) - s) * (om * l[13] + w * (ar - ub)) + s * l[13];
+    }
+    if (op & OP_BB) {
+#pragma unroll
+        for (int d = 0; d < 13; ++d) {
+            const R t = l[d];
+            l[d] = l[26 - d];
+            l[26 - d] = t;
+        }
+    }
+    if (op & OP_EQU) {
+        const R r_in = R(a.rho[c.i]);
+        R ar, bx, by, bz;
+        feq_vjp(l, R(a.vx[c.i]), R(a.vy[c.i]), R(a.vz[c.i]), ar, bx, by, bz);
+        a.g_mac[0][c.i] += static_cast<double>(ar);
+        a.g_mac[1][c.i] += static_cast<double>(r_in * bx);
+        a.g_mac[2][c.i] += static_cast<double>(r_in * by);
+        a.g_mac[3][c.i] += static_cast<double>(r_in * bz);
+    }
+    const bool pulls = (op & OP_LOAD) && !(op & OP_EQU);
+    const R g = objective_term(a, c.x, op);
+#pragma unroll
+    for (int d = 0; d < 27; ++d) a.nu_out[d][c.i] = (pulls ? l[d] : R(0)) + g;
+}
+
+template <typename S>
+__global__ void k_fill_rest(S* base, long long count)
+{
+    using R = typename ArithOf<S>::type;
+    for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < count;
+         j += (long long)gridDim.x * blockDim.x)
+        Cvt<S, R>::st(base + j, R(0));
+}
+
+}  // namespace adj
+}  // namespace culbm
+
+using namespace culbm;
+
+struct culbm_adj {
+    culbm_adj_config cfg{};
+    Domain dom{};
+    long long n = 0;
+    int dev = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    size_t esize = 4, rsize = 4;
+    uint8_t* d_ops = nullptr;
+    uint32_t* d_flag = nullptr;
+    float* d_mac[4] = {};
+    float* d_soft = nullptr;
+    double inv_tau = 0.5;
+    int K = 0, nckpt = 0, nseg = 0;
+    void* d_ckpt = nullptr;     // nckpt states
+    void* d_seg = nullptr;      // nseg states (at least 2)
+    void* d_nu = nullptr;       // 2 x 27 N of the arithmetic type
+    double* d_gsoft = nullptr;
+    double* d_gtau = nullptr;
+    double* d_gmac = nullptr;   // 4 N
+    double* d_psum = nullptr;   // 2 per time step
+    int n_in = 0, n_out = 0;
+    uint64_t device_bytes = 0;
+    float t_fwd = 0, t_rec = 0, t_adj = 0;
+    std::vector<uint32_t> h_flag;
+};
+
+namespace {
+
+culbm_status adj_alloc(culbm_adj* a, void** p, size_t bytes, const char* what)
+{
+    cudaError_t e = injection_gate();
+    if (e == cudaSuccess) e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        cudaGetLastError();
+        return fail(e == cudaErrorMemoryAllocation ? CULBM_ERR_OUT_OF_MEMORY : CULBM_ERR_CUDA,
+                    std::string("device allocation for ") + what + " failed: " + cudaGetErrorString(e));
+    }
+    a->device_bytes += bytes;
+    return CULBM_OK;
+}
+
+void adj_release(culbm_adj* a)
+{
+    if (!a) return;
+    cudaSetDevice(a->dev);
+    if (a->stream) cudaStreamSynchronize(a->stream);
+    cudaFree(a->d_ops);
+    cudaFree(a->d_flag);
+    for (auto& p : a->d_mac) cudaFree(p);
+    cudaFree(a->d_soft);
+    cudaFree(a->d_ckpt);
+    cudaFree(a->d_seg);
+    cudaFree(a->d_nu);
+    cudaFree(a->d_gsoft);
+    cudaFree(a->d_gtau);
+    cudaFree(a->d_gmac);
+    cudaFree(a->d_psum);
+    for (auto& e : a->ev)
+        if (e) cudaEventDestroy(e);
+    if (a->stream) cudaStreamDestroy(a->stream);
+    delete a;
+}
+
+template <class F>
+culbm_status adj_with_storage(const culbm_adj* a, F&& f)
+{
+    switch (a->cfg.storage) {
+        case CULBM_STORAGE_F32: return f(Tag<float>{});
+        case CULBM_STORAGE_F16: return f(Tag<__half>{});
+        case CULBM_STORAGE_F16_SR: return f(Tag<Half16SR>{});
+        case CULBM_STORAGE_F64: return f(Tag<double>{});
+        default: return fail(CULBM_ERR_UNSUPPORTED, "adjoint storage must be F32, F16, F16_SR or F64");
+    }
+}
+
+template <typename S>
+S* state_ptr(culbm_adj* a, bool ckpt, int slot)
+{
+    S* base = static_cast<S*>(ckpt ? a->d_ckpt : a->d_seg);
+    return base + static_cast<long long>(slot) * 27 * a->n;
+}
+
+template <typename S>
+adj::Args<S, typename ArithOf<S>::type> base_args(culbm_adj* a)
+{
+    using R = typename ArithOf<S>::type;
+    adj::Args<S, R> g{};
+    g.dom = a->dom;
+    g.ops = a->d_ops;
+    g.rho = a->d_mac[0];
+    g.vx = a->d_mac[1];
+    g.vy = a->d_mac[2];
+    g.vz = a->d_mac[3];
+    g.soft = a->d_soft;
+    g.inv_tau = static_cast<R>(a->inv_tau);
+    g.g_soft = a->d_gsoft;
+    g.g_tau = a->d_gtau;
+    for (int k = 0; k < 4; ++k) g.g_mac[k] = a->d_gmac + k * a->n;
+    g.plane_in = a->cfg.plane_x[0];
+    g.plane_out = a->cfg.plane_x[1];
+    return g;
+}
+
+template <typename S, typename R>
+void set_pops(Pops<S>& p, S* base, long long n)
+{
+    for (int d = 0; d < 27; ++d) p.p[d] = base + d * n;
+}
+
+// Forward steps t in [t_begin, t_end) from state `src`; states written to the
+// slots chosen by `slot_of(t+1)`; objective partial sums recorded when asked.
+template <typename S, class SlotOf>
+culbm_status forward_run(culbm_adj* a, int t_begin, int t_end, S* src, SlotOf slot_of, bool record)
+{
+    using R = typename ArithOf<S>::type;
+    auto g = base_args<S>(a);
+    const dim3 grid = cell_grid(a->dom), block = cell_block();
+    const int t0 = a->cfg.window[0], t1 = a->cfg.window[1];
+    auto record_sums = [&](S* state, int t) -> culbm_status {
+        if (!record || t < t0 || t > t1) return CULBM_OK;
+        auto h = g;
+        set_pops<S, R>(h.src, state, a->n);
+        adj::k_plane_rho<S, R><<<1, 1024, 0, a->stream>>>(h, a->cfg.plane_x[0], a->d_psum + 2 * t);
+        adj::k_plane_rho<S, R><<<1, 1024, 0, a->stream>>>(h, a->cfg.plane_x[1], a->d_psum + 2 * t + 1);
+        CULBM_CUDA(cudaGetLastError());
+        return CULBM_OK;
+    };
+    if (t_begin == 0) CULBM_TRY(record_sums(src, 0));
+    S* cur = src;
+    for (int t = t_begin; t < t_end; ++t) {
+        S* dst = slot_of(t + 1);
+        set_pops<S, R>(g.src, cur, a->n);
+        set_pops<S, R>(g.dst, dst, a->n);
+        g.seed = step_seed(static_cast<uint32_t>(t));
+        adj::k_soft_step<S, R><<<grid, block, 0, a->stream>>>(g);
+        CULBM_CUDA(cudaGetLastError());
+        CULBM_TRY(record_sums(dst, t + 1));
+        cur = dst;
+    }
+    return CULBM_OK;
+}
+
+template <typename S>
+culbm_status fill_rest(culbm_adj* a, S* state)
+{
+    adj::k_fill_rest<S><<<1184, 256, 0, a->stream>>>(state, 27ll * a->n);
+    CULBM_CUDA(cudaGetLastError());
+    return CULBM_OK;
+}
+
+culbm_status objective(culbm_adj* a, double* J)
+{
+    const int t0 = a->cfg.window[0], t1 = a->cfg.window[1];
+    std::vector<double> ps(2 * (t1 + 1));
+    CULBM_CUDA(cudaMemcpyAsync(ps.data(), a->d_psum, ps.size() * sizeof(double), cudaMemcpyDeviceToHost, a->stream));
+    CULBM_CUDA(cudaStreamSynchronize(a->stream));
+    double acc = 0.0;
+    for (int t = t0; t <= t1; ++t) acc += ps[2 * t] / (3.0 * a->n_in) - ps[2 * t + 1] / (3.0 * a->n_out);
+    *J = acc / (t1 - t0 + 1);
+    return CULBM_OK;
+}
+
+float elapsed(culbm_adj* a)
+{
+    float ms = 0;
+    cudaEventRecord(a->ev[1], a->stream);
+    cudaEventSynchronize(a->ev[1]);
+    cudaEventElapsedTime(&ms, a->ev[0], a->ev[1]);
+    cudaEventRecord(a->ev[0], a->stream);
+    return ms;
+}
+
+template <typename S>
+culbm_status run_forward(culbm_adj* a, bool checkpoints)
+{
+    const int T = a->cfg.window[1], K = a->K;
+    S* s0 = state_ptr<S>(a, true, 0);
+    CULBM_TRY(fill_rest<S>(a, s0));
+    CULBM_CUDA(cudaMemsetAsync(a->d_psum, 0, 2 * (T + 1) * sizeof(double), a->stream));
+    auto slot_of = [&](int t) -> S* {
+        if (checkpoints && t % K == 0) return state_ptr<S>(a, true, t / K);
+        return state_ptr<S>(a, false, t & 1);
+    };
+    return forward_run<S>(a, 0, T, s0, slot_of, true);
+}
+
+template <typename S>
+culbm_status run_gradient(culbm_adj* a)
+{
+    using R = typename ArithOf<S>::type;
+    const int T = a->cfg.window[1], K = a->K;
+    const int t0 = a->cfg.window[0], t1 = a->cfg.window[1];
+    const double nT = t1 - t0 + 1;
+    const R obj_in = static_cast<R>(1.0 / (3.0 * a->n_in * nT));
+    const R obj_out = static_cast<R>(-1.0 / (3.0 * a->n_out * nT));
+    const dim3 grid = cell_grid(a->dom), block = cell_block();
+
+    CULBM_CUDA(cudaEventRecord(a->ev[0], a->stream));
+    CULBM_TRY(run_forward<S>(a, true));
+    a->t_fwd = elapsed(a);
+
+    CULBM_CUDA(cudaMemsetAsync(a->d_gsoft, 0, a->n * sizeof(double), a->stream));
+    CULBM_CUDA(cudaMemsetAsync(a->d_gtau, 0, a->n * sizeof(double), a->stream));
+    CULBM_CUDA(cudaMemsetAsync(a->d_gmac, 0, 4 * a->n * sizeof(double), a->stream));
+    R* nu[2] = {static_cast<R*>(a->d_nu), static_cast<R*>(a->d_nu) + 27 * a->n};
+    auto g = base_args<S>(a);
+    int cur = 0;
+    {
+        for (int d = 0; d < 27; ++d) g.nu_out[d] = nu[cur] + d * a->n;
+        g.obj_in = (T >= t0 && T <= t1) ? obj_in : R(0);
+        g.obj_out = (T >= t0 && T <= t1) ? obj_out : R(0);
+        adj::k_adj_init<S, R><<<grid, block, 0, a->stream>>>(g);
+        CULBM_CUDA(cudaGetLastError());
+    }
+    float rec = 0, adjms = 0;
+    CULBM_CUDA(cudaEventRecord(a->ev[0], a->stream));
+    for (int k = (T - 1) / K; k >= 0; --k) {
+        const int tb = k * K, te = std::min(T, (k + 1) * K);
+        // recompute F^{tb+1} .. F^{te-1} into segment slots 0..
+        S* ck = state_ptr<S>(a, true, k);
+        auto slot_of = [&](int t) -> S* { return state_ptr<S>(a, false, t - tb - 1); };
+        CULBM_TRY(forward_run<S>(a, tb, te - 1, ck, slot_of, false));
+        rec += elapsed(a);
+        for (int t = te - 1; t >= tb; --t) {
+            S* st = (t == tb) ? ck : state_ptr<S>(a, false, t - tb - 1);
+            set_pops<S, R>(g.src, st, a->n);
+            for (int d = 0; d < 27; ++d) {
+                g.nu_in[d] = nu[cur] + d * a->n;
+                g.nu_out[d] = nu[1 - cur] + d * a->n;
+            }
+            const bool in_win = t >= t0 && t <= t1;
+            g.obj_in = in_win ? obj_in : R(0);
+            g.obj_out = in_win ? obj_out : R(0);
+            adj::k_adj_step<S, R><<<grid, block, 0, a->stream>>>(g);
+            CULBM_CUDA(cudaGetLastError());
+            cur = 1 - cur;
+        }
+        adjms += elapsed(a);
+    }
+    a->t_rec = rec;
+    a->t_adj = adjms;
+    return CULBM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+culbm_status culbm_adj_config_init(culbm_adj_config* cfg)
+{
+    if (!cfg) return fail(CULBM_ERR_INVALID_ARGUMENT, "cfg is NULL");
+    std::memset(cfg, 0, sizeof(*cfg));
+    cfg->domain_dim[0] = 128;
+    cfg->domain_dim[1] = 64;
+    cfg->domain_dim[2] = 64;
+    cfg->inv_tau = 0.5f;
+    cfg->window[0] = 300;
+    cfg->window[1] = 500;
+    cfg->plane_x[0] = 1;
+    cfg->plane_x[1] = -1;   // nx - 2
+    cfg->checkpoint_every = 50;
+    cfg->precision = 0;
+    cfg->storage = CULBM_STORAGE_F32;
+    return CULBM_OK;
+}
+
+culbm_status culbm_adj_create(const culbm_adj_config* cfg, culbm_adj** out)
+{
+    if (!cfg || !out) return fail(CULBM_ERR_INVALID_ARGUMENT, "NULL argument");
+    *out = nullptr;
+    const culbm_adj_config& c = *cfg;
+    for (int k = 0; k < 3; ++k)
+        if (c.domain_dim[k] < 1) return fail(CULBM_ERR_INVALID_ARGUMENT, "domain_dim must be positive");
+    const unsigned long long n = 1ull * c.domain_dim[0] * c.domain_dim[1] * c.domain_dim[2];
+    if (n >= (1ull << 31) || c.domain_dim[2] > 65535) return fail(CULBM_ERR_INVALID_ARGUMENT, "domain too large");
+    if (c.window[0] < 0 || c.window[1] < c.window[0]) return fail(CULBM_ERR_INVALID_ARGUMENT, "bad objective window");
+    if (!(c.inv_tau > 0.0f && c.inv_tau < 2.0f)) return fail(CULBM_ERR_INVALID_ARGUMENT, "invTau must lie in (0, 2)");
+    const bool f64 = c.precision == 1;
+    if (c.precision != 0 && c.precision != 1) return fail(CULBM_ERR_INVALID_ARGUMENT, "precision must be 0 or 1");
+    if (f64 != (c.storage == CULBM_STORAGE_F64))
+        return fail(CULBM_ERR_UNSUPPORTED, "FP64 precision goes with FP64 storage and only with it");
+    culbm_adj* a = new culbm_adj();
+    a->cfg = c;
+    if (a->cfg.plane_x[1] < 0) a->cfg.plane_x[1] = static_cast<int>(c.domain_dim[0]) - 2;
+    for (int k = 0; k < 2; ++k)
+        if (a->cfg.plane_x[k] < 0 || a->cfg.plane_x[k] >= static_cast<int>(c.domain_dim[0])) {
+            delete a;
+            return fail(CULBM_ERR_INVALID_ARGUMENT, "measurement plane outside the domain");
+        }
+    a->dev = c.dev_id;
+    a->dom.nx = c.domain_dim[0];
+    a->dom.ny = c.domain_dim[1];
+    a->dom.nz = c.domain_dim[2];
+    a->dom.nxy = a->dom.nx * a->dom.ny;
+    a->n = static_cast<long long>(n);
+    a->dom.n = static_cast<int>(n);
+    a->inv_tau = c.inv_tau;
+    a->esize = c.storage == CULBM_STORAGE_F64 ? 8 : c.storage == CULBM_STORAGE_F32 ? 4 : 2;
+    a->rsize = f64 ? 8 : 4;
+    const int T = c.window[1];
+    const double state_bytes = 27.0 * n * a->esize;
+    if (c.checkpoint_every > 0) {
+        a->K = c.checkpoint_every;
+    } else {
+        a->K = std::max(1, static_cast<int>(std::lround(std::sqrt(std::max(T, 1)))));
+    }
+    a->nckpt = (T + a->K - 1) / a->K + 1;
+    a->nseg = std::max(a->K - 1, 2);
+    auto body = [&]() -> culbm_status {
+        CULBM_CUDA(cudaSetDevice(a->dev));
+        CULBM_CUDA(cudaStreamCreateWithFlags(&a->stream, cudaStreamNonBlocking));
+        CULBM_CUDA(cudaEventCreate(&a->ev[0]));
+        CULBM_CUDA(cudaEventCreate(&a->ev[1]));
+        const double need = (a->nckpt + a->nseg) * state_bytes + 2.0 * 27 * n * a->rsize + 6.0 * 8 * n;
+        if (c.hbm_budget_bytes && need > static_cast<double>(c.hbm_budget_bytes))
+            return fail(CULBM_ERR_OUT_OF_MEMORY, "adjoint needs " + std::to_string(need / 1e9) +
+                                                     " GB, over the HBM budget of " +
+                                                     std::to_string(c.hbm_budget_bytes / 1e9) + " GB");
+        void* p = nullptr;
+        CULBM_TRY(adj_alloc(a, &p, n, "op bytes"));
+        a->d_ops = static_cast<uint8_t*>(p);
+        for (int k = 0; k < 4; ++k) {
+            CULBM_TRY(adj_alloc(a, &p, n * sizeof(float), "macroscopic inputs"));
+            a->d_mac[k] = static_cast<float*>(p);
+        }
+        CULBM_TRY(adj_alloc(a, &p, n * sizeof(float), "soft field"));
+        a->d_soft = static_cast<float*>(p);
+        CULBM_TRY(adj_alloc(a, &a->d_ckpt, static_cast<size_t>(a->nckpt * state_bytes), "checkpoints"));
+        CULBM_TRY(adj_alloc(a, &a->d_seg, static_cast<size_t>(a->nseg * state_bytes), "recompute segment"));
+        CULBM_TRY(adj_alloc(a, &a->d_nu, 2ull * 27 * n * a->rsize, "adjoint populations"));
+        CULBM_TRY(adj_alloc(a, &p, n * sizeof(double), "soft gradient"));
+        a->d_gsoft = static_cast<double*>(p);
+        CULBM_TRY(adj_alloc(a, &p, n * sizeof(double), "invTau gradient"));
+        a->d_gtau = static_cast<double*>(p);
+        CULBM_TRY(adj_alloc(a, &p, 4 * n * sizeof(double), "EQU input gradients"));
+        a->d_gmac = static_cast<double*>(p);
+        CULBM_TRY(adj_alloc(a, &p, 2ull * (T + 1) * sizeof(double), "objective sums"));
+        a->d_psum = static_cast<double*>(p);
+        return CULBM_OK;
+    };
+    const culbm_status st = body();
+    if (st != CULBM_OK) {
+        const std::string msg = culbm_last_error();
+        adj_release(a);
+        set_last_error(msg);
+        return st;
+    }
+    const culbm_status st2 = culbm_adj_set_state(a, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr);
+    if (st2 != CULBM_OK) {
+        const std::string msg = culbm_last_error();
+        adj_release(a);
+        set_last_error(msg);
+        return st2;
+    }
+    *out = a;
+    return CULBM_OK;
+}
+
+culbm_status culbm_adj_destroy(culbm_adj* adj)
+{
+    adj_release(adj);
+    return CULBM_OK;
+}
+
+culbm_status culbm_adj_set_state(culbm_adj* a, const uint32_t* flag, const float* rho, const float* vx,
+                                 const float* vy, const float* vz, const float* soft)
+{
+    if (!a) return fail(CULBM_ERR_INVALID_ARGUMENT, "adjoint handle is NULL");
+    CULBM_CUDA(cudaSetDevice(a->dev));
+    const Domain& D = a->dom;
+    const size_t n = static_cast<size_t>(a->n);
+    std::vector<uint8_t> ops(n);
+    constexpr uint32_t kFluid = FLAG_LOAD | FLAG_COLLIDE | FLAG_STORE;
+    int n_in = 0, n_out = 0;
+    for (int z = 0; z < D.nz; ++z)
+        for (int y = 0; y < D.ny; ++y)
+            for (int x = 0; x < D.nx; ++x) {
+                const size_t i = x + static_cast<size_t>(D.nx) * (y + static_cast<size_t>(D.ny) * z);
+                const uint32_t fl = flag ? flag[i] : kFluid;
+                if ((fl & 0x1Fu) != 0 && !(fl & FLAG_STORE))
+                    return fail(CULBM_ERR_INVALID_ARGUMENT, "adjoint model: every active cell needs STORE");
+                uint8_t op = static_cast<uint8_t>(fl & 0x1Fu);
+                if (x == 0 || x == D.nx - 1 || y == 0 || y == D.ny - 1 || z == 0 || z == D.nz - 1) op |= OP_EDGE;
+                ops[i] = op;
+                if (op & OP_COLLIDE) {
+                    n_in += x == a->cfg.plane_x[0];
+                    n_out += x == a->cfg.plane_x[1];
+                }
+            }
+    if (n_in == 0 || n_out == 0) return fail(CULBM_ERR_INVALID_ARGUMENT, "a measurement plane has no COLLIDE cell");
+    a->n_in = n_in;
+    a->n_out = n_out;
+    CULBM_CUDA(cudaMemcpyAsync(a->d_ops, ops.data(), n, cudaMemcpyHostToDevice, a->stream));
+    const float* mac[4] = {rho, vx, vy, vz};
+    const float dflt[4] = {1.0f, 0.0f, 0.0f, 0.0f};
+    std::vector<float> tmp;
+    for (int k = 0; k < 4; ++k) {
+        const float* src = mac[k];
+        if (!src) {
+            tmp.assign(n, dflt[k]);
+            src = tmp.data();
+        }
+        CULBM_CUDA(cudaMemcpyAsync(a->d_mac[k], src, n * sizeof(float), cudaMemcpyHostToDevice, a->stream));
+        CULBM_CUDA(cudaStreamSynchronize(a->stream));
+    }
+    if (soft) {
+        for (size_t i = 0; i < n; ++i)
+            if (!(soft[i] >= 0.0f && soft[i] <= 1.0f))
+                return fail(CULBM_ERR_INVALID_ARGUMENT, "soft field values must lie in [0, 1]");
+        CULBM_CUDA(cudaMemcpyAsync(a->d_soft, soft, n * sizeof(float), cudaMemcpyHostToDevice, a->stream));
+    } else {
+        CULBM_CUDA(cudaMemsetAsync(a->d_soft, 0, n * sizeof(float), a->stream));
+    }
+    CULBM_CUDA(cudaStreamSynchronize(a->stream));
+    return CULBM_OK;
+}
+
+culbm_status culbm_adj_set_inv_tau(culbm_adj* a, double inv_tau)
+{
+    if (!a) return fail(CULBM_ERR_INVALID_ARGUMENT, "adjoint handle is NULL");
+    if (!(inv_tau > 0.0 && inv_tau < 2.0)) return fail(CULBM_ERR_INVALID_ARGUMENT, "invTau must lie in (0, 2)");
+    a->inv_tau = inv_tau;
+    return CULBM_OK;
+}
+
+culbm_status culbm_adj_forward(culbm_adj* a, double* J)
+{
+    if (!a || !J) return fail(CULBM_ERR_INVALID_ARGUMENT, "NULL argument");
+    CULBM_CUDA(cudaSetDevice(a->dev));
+    CULBM_CUDA(cudaEventRecord(a->ev[0], a->stream));
+    CULBM_TRY(adj_with_storage(a, [&](auto tag) { return run_forward<typename decltype(tag)::type>(a, false); }));
+    a->t_fwd = elapsed(a);
+    return objective(a, J);
+}
+
+culbm_status culbm_adj_gradient(culbm_adj* a, double* J, double* dJ_dinv_tau, double* dJ_dsoft, double* dJ_dmac)
+{
+    if (!a) return fail(CULBM_ERR_INVALID_ARGUMENT, "adjoint handle is NULL");
+    CULBM_CUDA(cudaSetDevice(a->dev));
+    CULBM_TRY(adj_with_storage(a, [&](auto tag) { return run_gradient<typename decltype(tag)::type>(a); }));
+    double j = 0;
+    CULBM_TRY(objective(a, &j));
+    if (J) *J = j;
+    const size_t n = static_cast<size_t>(a->n);
+    if (dJ_dinv_tau) {
+        std::vector<double> g(n);
+        CULBM_CUDA(cudaMemcpy(g.data(), a->d_gtau, n * sizeof(double), cudaMemcpyDeviceToHost));
+        double s = 0;
+        for (double v : g) s += v;
+        *dJ_dinv_tau = s;
+    }
+    if (dJ_dsoft) CULBM_CUDA(cudaMemcpy(dJ_dsoft, a->d_gsoft, n * sizeof(double), cudaMemcpyDeviceToHost));
+    if (dJ_dmac) CULBM_CUDA(cudaMemcpy(dJ_dmac, a->d_gmac, 4 * n * sizeof(double), cudaMemcpyDeviceToHost));
+    return CULBM_OK;
+}
+
+culbm_status culbm_adj_get_info(culbm_adj* a, culbm_adj_info* info)
+{
+    if (!a || !info) return fail(CULBM_ERR_INVALID_ARGUMENT, "NULL argument");
+    std::memset(info, 0, sizeof(*info));
+    info->checkpoint_every = a->K;
+    info->checkpoints = a->nckpt;
+    info->device_bytes = a->device_bytes;
+    info->forward_ms = a->t_fwd;
+    info->recompute_ms = a->t_rec;
+    info->adjoint_ms = a->t_adj;
+    info->steps = static_cast<uint64_t>(a->cfg.window[1]);
+    return CULBM_OK;
+}
+
+}  // extern "C"

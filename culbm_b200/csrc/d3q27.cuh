@@ -197,9 +197,31 @@ __device__ __forceinline__ void equilibrium(R rho, R ux, R uy, R uz, R* f)
     }
 }
 
+// Shifted equilibrium of direction d (centre included) from the terms.
+template <typename R>
+__device__ __forceinline__ R equ_any(const EquTerms<R>& t, int d)
+{
+    using A = Rn<R>;
+    if (d == 13) return A::mul(R(8) / R(27), A::fma(t.rw[0], A::mul(t.h, t.c3), t.rm[0]));
+    return equ_dir(t, d);
+}
+
+// One relaxed population invTau*feq_d + (1-invTau)*f_d, with the centre term
+// associated as the reference does: (invTau*W0)*fma(rho, c3/2, rho-1).
+template <typename R>
+__device__ __forceinline__ R bgk_relax(const EquTerms<R>& t, R inv_tau, R om, int d, R fd)
+{
+    using A = Rn<R>;
+    R e;
+    if (d == 13)
+        e = A::mul(A::mul(inv_tau, R(8) / R(27)), A::fma(t.rw[0], A::mul(t.h, t.c3), t.rm[0]));
+    else
+        e = A::mul(inv_tau, equ_dir(t, d));
+    return A::add(e, A::mul(om, fd));
+}
+
 // BGK relaxation on shifted populations, bgk::detail::collision2<27>
-// (device_function.hpp:676-754): f <- invTau*feq + (1-invTau)*f, centre term
-// associated as (invTau*W0)*fma(rho, c3/2, rho-1).
+// (device_function.hpp:676-754): f <- invTau*feq + (1-invTau)*f.
 template <typename R>
 __device__ __forceinline__ void collide(R inv_tau, R* f)
 {
@@ -210,14 +232,7 @@ __device__ __forceinline__ void collide(R inv_tau, R* f)
     equ_terms(rho, ux, uy, uz, t);
     const R om = A::sub(R(1), inv_tau);
 #pragma unroll
-    for (int d = 0; d < 27; ++d) {
-        R e;
-        if (d == 13)
-            e = A::mul(A::mul(inv_tau, R(8) / R(27)), A::fma(rho, A::mul(t.h, t.c3), t.rm[0]));
-        else
-            e = A::mul(inv_tau, equ_dir(t, d));
-        f[d] = A::add(e, A::mul(om, f[d]));
-    }
+    for (int d = 0; d < 27; ++d) f[d] = bgk_relax(t, inv_tau, om, d, f[d]);
 }
 
 // Boundary and collision sequence of one cell after its populations were

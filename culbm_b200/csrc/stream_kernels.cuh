@@ -306,9 +306,16 @@ __global__ void __launch_bounds__(256) k_aa_odd(const __grid_constant__ StepArgs
     if (!row_cell<ROWS>(D, c)) return;
     const uint8_t op = a.ops[c.i];
     const uint32_t hc = cell_hash(static_cast<uint32_t>(c.i), a.seed);
+    // Warps without an x-face lane (all but the first and last of a row) take
+    // the straight path; the choice is uniform across the warp.
+    const int xw = c.x - (threadIdx.x & 31);
+    const bool xface = ROWS == ROWS_INNER && (xw == 0 || xw + 31 >= D.nx - 1);
     R f[27];
     if (op & OP_LOAD) {
-        if (ROWS == ROWS_INNER) {
+        if (ROWS == ROWS_INNER && !xface) {
+#pragma unroll
+            for (int d = 0; d < 27; ++d) f[d] = Cvt<S, R>::ld(a.src.p[26 - d] + (c.i - nb_off(D, d)));
+        } else if (ROWS == ROWS_INNER) {
 #pragma unroll
             for (int d = 0; d < 27; ++d) {
                 const S* p = a.src.p[26 - d] + (c.i - nb_off(D, d));
@@ -325,7 +332,10 @@ __global__ void __launch_bounds__(256) k_aa_odd(const __grid_constant__ StepArgs
     }
     cell_update<R>(op, a.inv_tau, a.rho, a.vx, a.vy, a.vz, c.i, f);
     if (!(op & OP_STORE)) return;
-    if (ROWS == ROWS_INNER) {
+    if (ROWS == ROWS_INNER && !xface) {
+#pragma unroll
+        for (int d = 0; d < 27; ++d) put(a.dst.p[d] + (c.i + nb_off(D, d)), f[d], hc, d);
+    } else if (ROWS == ROWS_INNER) {
 #pragma unroll
         for (int d = 0; d < 27; ++d) {
             const int cx = cx_of(d);
@@ -371,6 +381,7 @@ __global__ void __launch_bounds__(256) k_aa_even(const __grid_constant__ StepArg
 #pragma unroll
     for (int d = 0; d < 27; ++d) put(a.dst.p[26 - d] + c.i, f[d], hc, d);
     if (ROWS == ROWS_INNER) {
+        if (c.x != 0 && c.x != D.nx - 1) return;
 #pragma unroll
         for (int d = 0; d < 27; ++d) {
             const int cx = cx_of(d);

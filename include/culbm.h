@@ -215,6 +215,74 @@ typedef struct culbm_info {
 
 culbm_status culbm_get_info(culbm_sim* sim, culbm_info* info);
 
+/* ------------------------------------------------------------------------
+ * Discrete adjoint (no reference counterpart).
+ *
+ * Forward model: the same D3Q27 BGK step (pull with the per-axis clamp, EQU,
+ * full-way bounce-back, BGK) in which every COLLIDE cell x carries a soft
+ * obstacle value s(x) in [0,1] applied as partial bounce-back:
+ *     f' = C(f) + s (B(f) - C(f)),   C = BGK, B(f)_d = f_{26-d},
+ * so s = 0 is the plain step bit for bit.  Objective: the pressure drop
+ *     J = mean_{t in [t0,t1]} ( mean_{inlet plane} rho/3 - mean_{outlet plane} rho/3 )
+ * with rho from the pulled populations of the state after t steps, over the
+ * COLLIDE cells of the planes x = plane_x[0] and x = plane_x[1].  The adjoint
+ * is the exact reverse of that map (pull transposed into a push of adjoint
+ * populations), run over checkpoints taken every `checkpoint_every` steps
+ * with recomputation in between; parameter gradients are accumulated in FP64.
+ * ---------------------------------------------------------------------- */
+typedef struct culbm_adj_config {
+    int32_t dev_id;
+    uint32_t domain_dim[3];
+    float inv_tau;                 /* default 0.5 */
+    int32_t window[2];             /* [t0, t1], states after t steps; the forward runs t1 steps (default 300, 500) */
+    int32_t plane_x[2];            /* inlet / outlet measurement planes (default 1 and nx-2) */
+    int32_t checkpoint_every;      /* K; 0 = choose about sqrt(t1) within hbm_budget_bytes */
+    int32_t precision;             /* 0: FP32 forward and adjoint (default), 1: FP64 */
+    int32_t storage;               /* forward states and checkpoints: CULBM_STORAGE_F32 (default), _F16, _F16_SR;
+                                      CULBM_STORAGE_F64 with precision 1 */
+    uint64_t hbm_budget_bytes;     /* 0 = no limit */
+    uint32_t reserved[8];
+} culbm_adj_config;
+
+typedef struct culbm_adj culbm_adj;
+
+typedef struct culbm_adj_info {
+    int32_t checkpoint_every;
+    int32_t checkpoints;
+    uint64_t device_bytes;
+    float forward_ms;              /* the recorded forward pass (with the objective) */
+    float recompute_ms;            /* forward recomputation between checkpoints */
+    float adjoint_ms;              /* adjoint sweep */
+    uint64_t steps;                /* forward steps per pass (t1) */
+    uint32_t reserved[8];
+} culbm_adj_info;
+
+culbm_status culbm_adj_config_init(culbm_adj_config* cfg);
+culbm_status culbm_adj_create(const culbm_adj_config* cfg, culbm_adj** out);
+culbm_status culbm_adj_destroy(culbm_adj* adj);
+
+/* Flags, EQU macroscopic inputs (NULL: defaults as culbm_load_state) and the
+ * soft field (NULL: 0) as host arrays of N values.  Cells must have STORE or
+ * a zero flag word. */
+culbm_status culbm_adj_set_state(culbm_adj* adj, const uint32_t* flag, const float* rho, const float* vx,
+                                 const float* vy, const float* vz, const float* soft);
+
+/* Overrides the relaxation rate invTau (double; rounded to the arithmetic type). */
+culbm_status culbm_adj_set_inv_tau(culbm_adj* adj, double inv_tau);
+
+/* Forward run from rest equilibrium; returns J. */
+culbm_status culbm_adj_forward(culbm_adj* adj, double* J);
+
+/*
+ * Forward run, then the adjoint sweep.  Outputs (host, any may be NULL):
+ * J; dJ/d invTau; dJ/ds per cell (N doubles, 0 where no COLLIDE); dJ/d of the
+ * EQU inputs rho, vx, vy, vz per cell (4*N doubles, field-major, 0 where no EQU).
+ */
+culbm_status culbm_adj_gradient(culbm_adj* adj, double* J, double* dJ_dinv_tau, double* dJ_dsoft,
+                                double* dJ_dmac);
+
+culbm_status culbm_adj_get_info(culbm_adj* adj, culbm_adj_info* info);
+
 /* Message of the last failure on this thread ("" if none). */
 const char* culbm_last_error(void);
 

@@ -1,0 +1,182 @@
+"""Discrete adjoint (GPU): gradients of the channel pressure drop with respect
+to the soft-obstacle field, invTau and the inlet profile.
+
+Checks: PyTorch autograd of a tensor-op D3Q27 step (FP64, CPU); FP64 central
+finite differences with h = 1e-6 on the 32x16x16 case; checkpoint-stride
+invariance; FP32 against FP64; the torch.autograd.Function shim; s = 0 gives
+the plain step's objective.
+"""
+import numpy as np
+import pytest
+import torch
+
+from culbm_b200 import scenes as S
+from culbm_b200.adjoint import AdjointProblem, PressureDrop
+
+from torch_d3q27 import pressure_drop
+
+pytestmark = pytest.mark.gpu
+
+
+def case(nx, ny, nz, bumps, seed=7):
+    sc, soft = S.adjoint_channel(nx, ny, nz, u_peak=0.04, bumps=bumps, seed=seed)
+    f, r, ux, uy, uz = sc.arrays()
+    return sc, f, r, ux, uy, uz, soft.reshape(-1)
+
+
+def rel(a, b):
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def test_adjoint_matches_torch_autograd():
+    dims = (14, 8, 8)
+    sc, f, r, ux, uy, uz, soft = case(*dims, bumps=3)
+    window, planes, w = (15, 30), (1, dims[0] - 2), 0.6
+    with AdjointProblem(dims, window=window, planes=planes, inv_tau=w, checkpoint_every=7, precision="fp64") as p:
+        p.set_state(f, r, ux, uy, uz, soft)
+        J, g_tau, g_soft, g_mac = p.gradient()
+    ts = torch.tensor(soft.astype(np.float64), requires_grad=True)
+    tw = torch.tensor(w, dtype=torch.float64, requires_grad=True)
+    tvx = torch.tensor(ux.astype(np.float64), requires_grad=True)
+    Jt = pressure_drop(dims, f, torch.tensor(r, dtype=torch.float64), tvx, torch.tensor(uy, dtype=torch.float64),
+                       torch.tensor(uz, dtype=torch.float64), ts, tw, window, planes)
+    Jt.backward()
+    assert abs(J - Jt.item()) <= 1e-12 * abs(Jt.item())
+    assert rel(g_soft, ts.grad.numpy()) < 1e-9
+    assert abs(g_tau - tw.grad.item()) <= 1e-9 * abs(tw.grad.item())
+    equ = (f & S.EQU) != 0
+    assert rel(g_mac[1][equ], tvx.grad.numpy()[equ]) < 1e-9
+    assert np.abs(ts.grad.numpy()).max() > 0
+
+
+@pytest.fixture(scope="module")
+def fd_case():
+    dims = (32, 16, 16)
+    sc, f, r, ux, uy, uz, soft = case(*dims, bumps=16)
+    p = AdjointProblem(dims, window=(300, 500), inv_tau=0.5, checkpoint_every=50, precision="fp64")
+    p.set_state(f, r, ux, uy, uz, soft)
+    J, g_tau, g_soft, g_mac = p.gradient()
+    yield dict(p=p, dims=dims, f=f, r=r, ux=ux, uy=uy, uz=uz, soft=soft, J=J, g_tau=g_tau, g_soft=g_soft,
+               g_mac=g_mac)
+    p.close()
+
+
+def test_fd_invtau(fd_case):
+    c, h = fd_case, 1e-6
+    p = c["p"]
+    p.set_inv_tau(0.5 + h)
+    jp = p.forward()
+    p.set_inv_tau(0.5 - h)
+    jm = p.forward()
+    p.set_inv_tau(0.5)
+    fd = (jp - jm) / (2 * h)
+    assert abs(fd - c["g_tau"]) <= 1e-4 * abs(fd), (fd, c["g_tau"])
+
+
+def _fd_field(c, key, idx, h=1e-6):
+    p = c["p"]
+    base = c[key].copy()
+    out = []
+    for i in idx:
+        plus, minus = base.copy(), base.copy()
+        plus[i] = np.float32(base[i] + h)
+        minus[i] = np.float32(base[i] - h)
+        args = {k: c[k] for k in ("f", "r", "ux", "uy", "uz", "soft")}
+        args[key] = plus
+        p.set_state(args["f"], args["r"], args["ux"], args["uy"], args["uz"], args["soft"])
+        jp = p.forward()
+        args[key] = minus
+        p.set_state(args["f"], args["r"], args["ux"], args["uy"], args["uz"], args["soft"])
+        jm = p.forward()
+        out.append((jp - jm) / (float(plus[i]) - float(minus[i])))
+    p.set_state(c["f"], c["r"], c["ux"], c["uy"], c["uz"], c["soft"])
+    return np.array(out)
+
+
+def test_fd_soft_field(fd_case):
+    c = fd_case
+    g = c["g_soft"]
+    inner = (c["soft"] > 0.02) & (c["soft"] < 0.98)
+    cand = np.flatnonzero(inner)
+    idx = cand[np.argsort(-np.abs(g[cand]))[:6]]
+    fd = _fd_field(c, "soft", idx)
+    for i, a, b in zip(idx, g[idx], fd):
+        assert abs(a - b) <= 1e-4 * abs(b), (i, a, b)
+
+
+def test_fd_inlet_profile(fd_case):
+    c = fd_case
+    g = c["g_mac"][1]
+    inlet = np.flatnonzero(((c["f"] & S.EQU) != 0) & (c["ux"] > 0.01))
+    idx = inlet[np.argsort(-np.abs(g[inlet]))[:4]]
+    fd = _fd_field(c, "ux", idx)
+    for i, a, b in zip(idx, g[idx], fd):
+        assert abs(a - b) <= 1e-4 * abs(b), (i, a, b)
+
+
+def test_checkpoint_stride_does_not_change_gradients():
+    dims = (20, 10, 10)
+    sc, f, r, ux, uy, uz, soft = case(*dims, bumps=4)
+    outs = []
+    for K in (1, 7, 60):
+        with AdjointProblem(dims, window=(30, 60), checkpoint_every=K, precision="fp64") as p:
+            p.set_state(f, r, ux, uy, uz, soft)
+            outs.append(p.gradient())
+    for o in outs[1:]:
+        assert o[0] == outs[0][0] and o[1] == outs[0][1]
+        assert np.array_equal(o[2], outs[0][2]) and np.array_equal(o[3], outs[0][3])
+
+
+def test_fp32_adjoint_close_to_fp64():
+    dims = (32, 16, 16)
+    sc, f, r, ux, uy, uz, soft = case(*dims, bumps=16)
+    res = {}
+    for prec in ("fp32", "fp64"):
+        with AdjointProblem(dims, window=(100, 200), checkpoint_every=20, precision=prec) as p:
+            p.set_state(f, r, ux, uy, uz, soft)
+            res[prec] = p.gradient()
+    assert abs(res["fp32"][0] - res["fp64"][0]) <= 1e-4 * abs(res["fp64"][0])
+    assert rel(res["fp32"][2], res["fp64"][2]) < 1e-3
+    assert abs(res["fp32"][1] - res["fp64"][1]) <= 1e-3 * abs(res["fp64"][1])
+
+
+def test_torch_shim_backward():
+    dims = (16, 8, 8)
+    sc, f, r, ux, uy, uz, soft = case(*dims, bumps=3)
+    with AdjointProblem(dims, window=(10, 20), checkpoint_every=5, precision="fp64") as p:
+        pd = PressureDrop(p, f, r, uy, uz)
+        ts = torch.tensor(soft, dtype=torch.float64, requires_grad=True)
+        tw = torch.tensor(0.5, dtype=torch.float64, requires_grad=True)
+        tvx = torch.tensor(ux, dtype=torch.float64, requires_grad=True)
+        J = pd.apply(ts, tw, tvx)
+        (2.0 * J).backward()
+        p.set_state(f, r, ux, uy, uz, soft)
+        p.set_inv_tau(0.5)
+        J2, g_tau, g_soft, g_mac = p.gradient()
+    assert J.item() == J2
+    assert np.allclose(ts.grad.numpy(), 2 * g_soft, rtol=0, atol=0)
+    assert tw.grad.item() == 2 * g_tau
+    assert np.array_equal(tvx.grad.numpy(), 2 * g_mac[1])
+
+
+def test_zero_soft_field_is_the_plain_step(culbm):
+    dims = (24, 12, 10)
+    sc, f, r, ux, uy, uz, soft = case(*dims, bumps=2)
+    window = (5, 15)
+    with AdjointProblem(dims, window=window, checkpoint_every=5) as p:
+        p.set_state(f, r, ux, uy, uz, None)
+        J = p.forward()
+    coll = (f & S.COLLIDE) != 0
+    x = np.arange(f.size) % dims[0]
+    acc = 0.0
+    with culbm.Simulation(dims, stream_policy=0, inv_tau=0.5) as sim:
+        sim.load_state(f, r, ux, uy, uz)
+        for t in range(window[1] + 1):
+            if t >= window[0]:
+                sim.moments()
+                rho = sim.field("rho").astype(np.float64)
+                acc += rho[coll & (x == 1)].mean() / 3 - rho[coll & (x == dims[0] - 2)].mean() / 3
+            if t < window[1]:
+                sim.step(1)
+    assert abs(J - acc / (window[1] - window[0] + 1)) <= 1e-12 * abs(J)
