@@ -55,6 +55,9 @@ struct Args {
     int plane_in, plane_out;
     R obj_in, obj_out;   // dJ/df_d of one in/out plane cell at this time (0 outside the window)
     uint32_t seed;
+    double* rho_plane;   // forward: rho of the two measurement planes of the pulled state, this step
+                         // (null outside the objective window); [2][ny*nz]
+    double* g_tau_block; // adjoint: one FP64 accumulator per thread block
 };
 
 // Pull of the 27 populations of cell (x, y, z) from the state a.src with the
@@ -123,6 +126,18 @@ __global__ void __launch_bounds__(256) k_soft_step(const __grid_constant__ Args<
 #pragma unroll
         for (int d = 0; d < 27; ++d) f[d] = R(0);
     }
+    if (a.rho_plane && (c.x == a.plane_in || c.x == a.plane_out)) {
+        // objective: rho of the pulled state on the measurement planes
+        double r = 0.0;
+        if (op & OP_COLLIDE) {
+            R rr, ux, uy, uz;
+            moments(f, rr, ux, uy, uz);
+            r = static_cast<double>(rr);
+        }
+        const int q = c.y + a.dom.ny * c.z;
+        if (c.x == a.plane_in) a.rho_plane[q] = r;
+        if (c.x == a.plane_out) a.rho_plane[a.dom.ny * a.dom.nz + q] = r;
+    }
     soft_update<R>(op, a.inv_tau, R(a.soft[c.i]), a.rho, a.vx, a.vy, a.vz, c.i, f);
     if (op & OP_STORE) {
         const uint32_t hc = cell_hash(static_cast<uint32_t>(c.i), a.seed);
@@ -131,21 +146,36 @@ __global__ void __launch_bounds__(256) k_soft_step(const __grid_constant__ Args<
     }
 }
 
-// Deterministic sum of rho over the COLLIDE cells of plane x = px: one block.
+// rho of the pulled state on the two measurement planes (the last state of
+// the window, which no step pulls).
 template <typename S, typename R>
-__global__ void __launch_bounds__(1024) k_plane_rho(const __grid_constant__ Args<S, R> a, int px, double* out)
+__global__ void __launch_bounds__(256) k_plane_rho(const __grid_constant__ Args<S, R> a)
 {
     const Domain& D = a.dom;
-    double acc = 0.0;
-    for (int q = threadIdx.x; q < D.ny * D.nz; q += blockDim.x) {
-        const int y = q % D.ny, z = q / D.ny;
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= D.ny * D.nz) return;
+    const int y = q % D.ny, z = q / D.ny;
+    for (int side = 0; side < 2; ++side) {
+        const int px = side ? a.plane_out : a.plane_in;
         const int i = px + D.nx * (y + D.ny * z);
-        if (!(a.ops[i] & OP_COLLIDE)) continue;
-        R f[27], r, ux, uy, uz;
-        pull_state(a, px, y, z, i, f);
-        moments(f, r, ux, uy, uz);
-        acc += static_cast<double>(r);
+        double r = 0.0;
+        if (a.ops[i] & OP_COLLIDE) {
+            R f[27], rr, ux, uy, uz;
+            pull_state(a, px, y, z, i, f);
+            moments(f, rr, ux, uy, uz);
+            r = static_cast<double>(rr);
+        }
+        a.rho_plane[side * D.ny * D.nz + q] = r;
     }
+}
+
+// Sums each recorded plane in a fixed order: block b sums plane b of
+// planes[b][m], writes out[b].
+__global__ void __launch_bounds__(1024) k_sum_planes(const double* planes, int m, double* out)
+{
+    const double* p = planes + static_cast<long long>(blockIdx.x) * m;
+    double acc = 0.0;
+    for (int q = threadIdx.x; q < m; q += blockDim.x) acc += p[q];
     __shared__ double sh[1024];
     sh[threadIdx.x] = acc;
     __syncthreads();
@@ -153,7 +183,7 @@ __global__ void __launch_bounds__(1024) k_plane_rho(const __grid_constant__ Args
         if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
         __syncthreads();
     }
-    if (threadIdx.x == 0) *out = sh[0];
+    if (threadIdx.x == 0) out[blockIdx.x] = sh[0];
 }
 
 // Per-population weights of the objective at time t, for every cell.
@@ -206,42 +236,56 @@ __device__ __forceinline__ void feq_vjp(const R* l, R ux, R uy, R uz, R& a_rho, 
     bz = R(3) * Lz + R(9) * Lccz - R(3) * uz * L0;
 }
 
-template <typename S, typename R>
-__global__ void __launch_bounds__(256) k_adj_step(const __grid_constant__ Args<S, R> a)
+// FP64 block sum of v into the block's own accumulator (no atomics: each
+// block owns its slot, so the result does not depend on scheduling).
+__device__ __forceinline__ void block_accumulate(double v, double* slot)
 {
-    const CellCoord c = cell_of_thread(a.dom);
-    if (!c.valid) return;
-    const Domain& D = a.dom;
-    const uint8_t op = a.ops[c.i];
-    R l[27];
-    // lambda: adjoint of this cell's stored populations, gathered from the
-    // cells that pull them
-    if (op & OP_STORE) {
-        if (!(op & OP_EDGE)) {
+    __shared__ double sh[8];
 #pragma unroll
-            for (int d = 0; d < 27; ++d) l[d] = a.nu_in[d][c.i + nb_off(D, d)];
-        } else {
-            for_dirs([&](auto dd) {
-                constexpr int d = decltype(dd)::value;
-                R v = inside(D, c.x + cx_of(d), c.y + cy_of(d), c.z + cz_of(d)) ? a.nu_in[d][c.i + nb_off(D, d)] : R(0);
-                for_each_clamp_reader<d>(D, c.x, c.y, c.z,
-                                         [&](int yx, int yy, int yz) { v += a.nu_in[d][yx + D.nx * (yy + D.ny * yz)]; });
-                l[d] = v;
-            });
-        }
-    } else {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xFFFFFFFFu, v, o);
+    const int lane = (threadIdx.x + blockDim.x * threadIdx.y) & 31;
+    const int warp = (threadIdx.x + blockDim.x * threadIdx.y) >> 5;
+    if (lane == 0) sh[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+        double w = lane < 8 ? sh[lane] : 0.0;
 #pragma unroll
-        for (int d = 0; d < 27; ++d) l[d] = R(0);
+        for (int o = 4; o > 0; o >>= 1) w += __shfl_down_sync(0xFFFFFFFFu, w, o);
+        if (lane == 0) *slot += w;
     }
-    // forward populations of this cell at step t, then its intermediate f2
+}
+
+// Adjoint of the stored population d of cell c: the sum of nu_d over the
+// cells whose pull of d reads c (the streaming target and clamp readers).
+template <int d, typename S, typename R>
+__device__ __forceinline__ R gather_lambda(const Args<S, R>& a, const CellCoord& c, bool edge)
+{
+    const Domain& D = a.dom;
+    if (!edge) return a.nu_in[d][c.i + nb_off(D, d)];
+    R v = inside(D, c.x + cx_of(d), c.y + cy_of(d), c.z + cz_of(d)) ? a.nu_in[d][c.i + nb_off(D, d)] : R(0);
+    for_each_clamp_reader<d>(D, c.x, c.y, c.z,
+                             [&](int yx, int yy, int yz) { v += a.nu_in[d][yx + D.nx * (yy + D.ny * yz)]; });
+    return v;
+}
+
+// Reverse of one cell update at step t.  Works on direction pairs (d, 26-d)
+// so that the gathered adjoint fills the registers the forward populations
+// free; the linearisation point uses feq in plain arithmetic (the forward
+// pass itself rounds exactly like the plain step).
+template <typename S, typename R>
+__device__ __forceinline__ void adj_cell(const Args<S, R>& a, const CellCoord c, double& gtau_local)
+{
+    const uint8_t op = a.ops[c.i];
+    const bool store = (op & OP_STORE) != 0, edge = (op & OP_EDGE) != 0;
     R f[27];
-    if (op & OP_LOAD) {
+    if (op & OP_EQU) {
+        equilibrium<R>(R(a.rho[c.i]), R(a.vx[c.i]), R(a.vy[c.i]), R(a.vz[c.i]), f);
+    } else if (op & OP_LOAD) {
         pull_state(a, c.x, c.y, c.z, c.i, f);
     } else {
 #pragma unroll
         for (int d = 0; d < 27; ++d) f[d] = R(0);
     }
-    if (op & OP_EQU) equilibrium<R>(R(a.rho[c.i]), R(a.vx[c.i]), R(a.vy[c.i]), R(a.vz[c.i]), f);
     if (op & OP_BB) {
 #pragma unroll
         for (int d = 0; d < 13; ++d) {
@@ -250,34 +294,73 @@ __global__ void __launch_bounds__(256) k_adj_step(const __grid_constant__ Args<S
             f[26 - d] = t;
         }
     }
-    if (op & OP_COLLIDE) {
+    R l[27];
+    if (!store) {
+#pragma unroll
+        for (int d = 0; d < 27; ++d) l[d] = R(0);
+    } else if (!(op & OP_COLLIDE)) {
+        for_dirs([&](auto dd) {
+            constexpr int d = decltype(dd)::value;
+            l[d] = gather_lambda<d>(a, c, edge);
+        });
+    } else {
         const R s = R(a.soft[c.i]);
         const R w = a.inv_tau, om = R(1) - w;
-        R r, ux, uy, uz;
-        moments(f, r, ux, uy, uz);
-        EquTerms<R> t;
-        equ_terms(r, ux, uy, uz, t);
-        // parameter sensitivities at this step
-        R gs = 0, gw = 0;
-#pragma unroll
-        for (int d = 0; d < 27; ++d) {
-            const R feq = equ_any(t, d);
-            const R cd = w * feq + om * f[d];
-            gs += l[d] * (f[26 - d] - cd);
-            gw += l[d] * (feq - f[d]);
-        }
+        R rho, ux, uy, uz;
+        moments(f, rho, ux, uy, uz);
+        const R uu = ux * ux + uy * uy + uz * uz;
+        R gs = 0, gw = 0, L0 = 0, Lx = 0, Ly = 0, Lz = 0, Lcu = 0, Lcu2 = 0, Lcx = 0, Lcy = 0, Lcz = 0;
+        for_dirs([&](auto dd) {
+            constexpr int d = decltype(dd)::value;
+            if constexpr (d < 13) {
+                constexpr int e = 26 - d;
+                const R ld = gather_lambda<d>(a, c, edge), le = gather_lambda<e>(a, c, edge);
+                const R cx = R(cx_of(d)), cy = R(cy_of(d)), cz = R(cz_of(d)), wd = weight<R>(d);
+                const R cu = cx * ux + cy * uy + cz * uz;
+                const R base = R(1) + R(4.5) * cu * cu - R(1.5) * uu;
+                const R feqd = wd * (rho * (base + R(3) * cu) - R(1));
+                const R feqe = wd * (rho * (base - R(3) * cu) - R(1));
+                const R Cd = w * feqd + om * f[d], Ce = w * feqe + om * f[e];
+                gs += ld * (f[e] - Cd) + le * (f[d] - Ce);
+                gw += ld * (feqd - f[d]) + le * (feqe - f[e]);
+                const R sp = wd * (ld + le), sm = wd * (ld - le);
+                L0 += sp;
+                Lx += cx * sm;
+                Ly += cy * sm;
+                Lz += cz * sm;
+                Lcu += cu * sm;
+                Lcu2 += cu * cu * sp;
+                Lcx += cx * cu * sp;
+                Lcy += cy * cu * sp;
+                Lcz += cz * cu * sp;
+                l[d] = ld;
+                l[e] = le;
+            } else if constexpr (d == 13) {
+                const R l13 = gather_lambda<13>(a, c, edge);
+                const R w0 = weight<R>(13);
+                const R feq = w0 * (rho * (R(1) - R(1.5) * uu) - R(1));
+                const R C13 = w * feq + om * f[13];
+                gs += l13 * (f[13] - C13);
+                gw += l13 * (feq - f[13]);
+                L0 += w0 * l13;
+                l[13] = l13;
+            }
+        });
         a.g_soft[c.i] += static_cast<double>(gs);
-        a.g_tau[c.i] += static_cast<double>((R(1) - s) * gw);
+        gtau_local = static_cast<double>((R(1) - s) * gw);
         // lambda2 = (1-s) J_C^T lambda + s B(lambda)
-        R ar, bx, by, bz;
-        feq_vjp(l, ux, uy, uz, ar, bx, by, bz);
+        const R ar = L0 + R(3) * Lcu + R(4.5) * Lcu2 - R(1.5) * uu * L0;
+        const R bx = R(3) * Lx + R(9) * Lcx - R(3) * ux * L0;
+        const R by = R(3) * Ly + R(9) * Lcy - R(3) * uy * L0;
+        const R bz = R(3) * Lz + R(9) * Lcz - R(3) * uz * L0;
         const R ub = ux * bx + uy * by + uz * bz;
 #pragma unroll
         for (int d = 0; d < 13; ++d) {
             const int e = 26 - d;
             const R ld = l[d], le = l[e];
-            const R jd = om * ld + w * (ar + R(cx_of(d)) * bx + R(cy_of(d)) * by + R(cz_of(d)) * bz - ub);
-            const R je = om * le + w * (ar + R(cx_of(e)) * bx + R(cy_of(e)) * by + R(cz_of(e)) * bz - ub);
+            const R cb = R(cx_of(d)) * bx + R(cy_of(d)) * by + R(cz_of(d)) * bz;
+            const R jd = om * ld + w * (ar + cb - ub);
+            const R je = om * le + w * (ar - cb - ub);
             l[d] = (R(1) - s) * jd + s * le;
             l[e] = (R(1) - s) * je + s * ld;
         }
@@ -304,6 +387,15 @@ __global__ void __launch_bounds__(256) k_adj_step(const __grid_constant__ Args<S
     const R g = objective_term(a, c.x, op);
 #pragma unroll
     for (int d = 0; d < 27; ++d) a.nu_out[d][c.i] = (pulls ? l[d] : R(0)) + g;
+}
+
+template <typename S, typename R>
+__global__ void __launch_bounds__(256) k_adj_step(const __grid_constant__ Args<S, R> a)
+{
+    const CellCoord c = cell_of_thread(a.dom);
+    double gtau_local = 0.0;
+    if (c.valid) adj_cell(a, c, gtau_local);
+    block_accumulate(gtau_local, a.g_tau_block + (blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)));
 }
 
 template <typename S>
@@ -340,7 +432,9 @@ struct culbm_adj {
     double* d_gsoft = nullptr;
     double* d_gtau = nullptr;
     double* d_gmac = nullptr;   // 4 N
-    double* d_psum = nullptr;   // 2 per time step
+    double* d_psum = nullptr;   // 2 per time step of the window
+    double* d_rho_plane = nullptr;  // window x 2 planes x ny*nz
+    long long n_tau_blocks = 0;
     int n_in = 0, n_out = 0;
     uint64_t device_bytes = 0;
     float t_fwd = 0, t_rec = 0, t_adj = 0;
@@ -379,6 +473,7 @@ void adj_release(culbm_adj* a)
     cudaFree(a->d_gtau);
     cudaFree(a->d_gmac);
     cudaFree(a->d_psum);
+    cudaFree(a->d_rho_plane);
     for (auto& e : a->ev)
         if (e) cudaEventDestroy(e);
     if (a->stream) cudaStreamDestroy(a->stream);
@@ -440,26 +535,23 @@ culbm_status forward_run(culbm_adj* a, int t_begin, int t_end, S* src, SlotOf sl
     auto g = base_args<S>(a);
     const dim3 grid = cell_grid(a->dom), block = cell_block();
     const int t0 = a->cfg.window[0], t1 = a->cfg.window[1];
-    auto record_sums = [&](S* state, int t) -> culbm_status {
-        if (!record || t < t0 || t > t1) return CULBM_OK;
-        auto h = g;
-        set_pops<S, R>(h.src, state, a->n);
-        adj::k_plane_rho<S, R><<<1, 1024, 0, a->stream>>>(h, a->cfg.plane_x[0], a->d_psum + 2 * t);
-        adj::k_plane_rho<S, R><<<1, 1024, 0, a->stream>>>(h, a->cfg.plane_x[1], a->d_psum + 2 * t + 1);
-        CULBM_CUDA(cudaGetLastError());
-        return CULBM_OK;
-    };
-    if (t_begin == 0) CULBM_TRY(record_sums(src, 0));
+    const long long plane = 2ll * a->dom.ny * a->dom.nz;
     S* cur = src;
     for (int t = t_begin; t < t_end; ++t) {
         S* dst = slot_of(t + 1);
         set_pops<S, R>(g.src, cur, a->n);
         set_pops<S, R>(g.dst, dst, a->n);
         g.seed = step_seed(static_cast<uint32_t>(t));
+        g.rho_plane = (record && t >= t0 && t <= t1) ? a->d_rho_plane + (t - t0) * plane : nullptr;
         adj::k_soft_step<S, R><<<grid, block, 0, a->stream>>>(g);
         CULBM_CUDA(cudaGetLastError());
-        CULBM_TRY(record_sums(dst, t + 1));
         cur = dst;
+    }
+    if (record && t_end >= t0 && t_end <= t1) {
+        set_pops<S, R>(g.src, cur, a->n);
+        g.rho_plane = a->d_rho_plane + (t_end - t0) * plane;
+        adj::k_plane_rho<S, R><<<(a->dom.ny * a->dom.nz + 255) / 256, 256, 0, a->stream>>>(g);
+        CULBM_CUDA(cudaGetLastError());
     }
     return CULBM_OK;
 }
@@ -475,12 +567,15 @@ culbm_status fill_rest(culbm_adj* a, S* state)
 culbm_status objective(culbm_adj* a, double* J)
 {
     const int t0 = a->cfg.window[0], t1 = a->cfg.window[1];
-    std::vector<double> ps(2 * (t1 + 1));
+    const int nt = t1 - t0 + 1;
+    adj::k_sum_planes<<<2 * nt, 1024, 0, a->stream>>>(a->d_rho_plane, a->dom.ny * a->dom.nz, a->d_psum);
+    CULBM_CUDA(cudaGetLastError());
+    std::vector<double> ps(2 * nt);
     CULBM_CUDA(cudaMemcpyAsync(ps.data(), a->d_psum, ps.size() * sizeof(double), cudaMemcpyDeviceToHost, a->stream));
     CULBM_CUDA(cudaStreamSynchronize(a->stream));
     double acc = 0.0;
-    for (int t = t0; t <= t1; ++t) acc += ps[2 * t] / (3.0 * a->n_in) - ps[2 * t + 1] / (3.0 * a->n_out);
-    *J = acc / (t1 - t0 + 1);
+    for (int k = 0; k < nt; ++k) acc += ps[2 * k] / (3.0 * a->n_in) - ps[2 * k + 1] / (3.0 * a->n_out);
+    *J = acc / nt;
     return CULBM_OK;
 }
 
@@ -500,7 +595,6 @@ culbm_status run_forward(culbm_adj* a, bool checkpoints)
     const int T = a->cfg.window[1], K = a->K;
     S* s0 = state_ptr<S>(a, true, 0);
     CULBM_TRY(fill_rest<S>(a, s0));
-    CULBM_CUDA(cudaMemsetAsync(a->d_psum, 0, 2 * (T + 1) * sizeof(double), a->stream));
     auto slot_of = [&](int t) -> S* {
         if (checkpoints && t % K == 0) return state_ptr<S>(a, true, t / K);
         return state_ptr<S>(a, false, t & 1);
@@ -524,10 +618,11 @@ culbm_status run_gradient(culbm_adj* a)
     a->t_fwd = elapsed(a);
 
     CULBM_CUDA(cudaMemsetAsync(a->d_gsoft, 0, a->n * sizeof(double), a->stream));
-    CULBM_CUDA(cudaMemsetAsync(a->d_gtau, 0, a->n * sizeof(double), a->stream));
+    CULBM_CUDA(cudaMemsetAsync(a->d_gtau, 0, a->n_tau_blocks * sizeof(double), a->stream));
     CULBM_CUDA(cudaMemsetAsync(a->d_gmac, 0, 4 * a->n * sizeof(double), a->stream));
     R* nu[2] = {static_cast<R*>(a->d_nu), static_cast<R*>(a->d_nu) + 27 * a->n};
     auto g = base_args<S>(a);
+    g.g_tau_block = a->d_gtau;
     int cur = 0;
     {
         for (int d = 0; d < 27; ++d) g.nu_out[d] = nu[cur] + d * a->n;
@@ -635,7 +730,8 @@ culbm_status culbm_adj_create(const culbm_adj_config* cfg, culbm_adj** out)
         CULBM_CUDA(cudaStreamCreateWithFlags(&a->stream, cudaStreamNonBlocking));
         CULBM_CUDA(cudaEventCreate(&a->ev[0]));
         CULBM_CUDA(cudaEventCreate(&a->ev[1]));
-        const double need = (a->nckpt + a->nseg) * state_bytes + 2.0 * 27 * n * a->rsize + 6.0 * 8 * n;
+        const double need = (a->nckpt + a->nseg) * state_bytes + 2.0 * 27 * n * a->rsize + 5.0 * 8 * n +
+                            16.0 * (c.window[1] - c.window[0] + 1) * c.domain_dim[1] * c.domain_dim[2];
         if (c.hbm_budget_bytes && need > static_cast<double>(c.hbm_budget_bytes))
             return fail(CULBM_ERR_OUT_OF_MEMORY, "adjoint needs " + std::to_string(need / 1e9) +
                                                      " GB, over the HBM budget of " +
@@ -654,12 +750,19 @@ culbm_status culbm_adj_create(const culbm_adj_config* cfg, culbm_adj** out)
         CULBM_TRY(adj_alloc(a, &a->d_nu, 2ull * 27 * n * a->rsize, "adjoint populations"));
         CULBM_TRY(adj_alloc(a, &p, n * sizeof(double), "soft gradient"));
         a->d_gsoft = static_cast<double*>(p);
-        CULBM_TRY(adj_alloc(a, &p, n * sizeof(double), "invTau gradient"));
+        {
+            const dim3 g = cell_grid(a->dom);
+            a->n_tau_blocks = 1ll * g.x * g.y * g.z;
+        }
+        CULBM_TRY(adj_alloc(a, &p, a->n_tau_blocks * sizeof(double), "invTau gradient"));
         a->d_gtau = static_cast<double*>(p);
         CULBM_TRY(adj_alloc(a, &p, 4 * n * sizeof(double), "EQU input gradients"));
         a->d_gmac = static_cast<double*>(p);
-        CULBM_TRY(adj_alloc(a, &p, 2ull * (T + 1) * sizeof(double), "objective sums"));
+        const long long nt = c.window[1] - c.window[0] + 1;
+        CULBM_TRY(adj_alloc(a, &p, 2ull * nt * sizeof(double), "objective sums"));
         a->d_psum = static_cast<double*>(p);
+        CULBM_TRY(adj_alloc(a, &p, 2ull * nt * a->dom.ny * a->dom.nz * sizeof(double), "objective planes"));
+        a->d_rho_plane = static_cast<double*>(p);
         return CULBM_OK;
     };
     const culbm_status st = body();
@@ -767,8 +870,8 @@ culbm_status culbm_adj_gradient(culbm_adj* a, double* J, double* dJ_dinv_tau, do
     if (J) *J = j;
     const size_t n = static_cast<size_t>(a->n);
     if (dJ_dinv_tau) {
-        std::vector<double> g(n);
-        CULBM_CUDA(cudaMemcpy(g.data(), a->d_gtau, n * sizeof(double), cudaMemcpyDeviceToHost));
+        std::vector<double> g(static_cast<size_t>(a->n_tau_blocks));
+        CULBM_CUDA(cudaMemcpy(g.data(), a->d_gtau, g.size() * sizeof(double), cudaMemcpyDeviceToHost));
         double s = 0;
         for (double v : g) s += v;
         *dJ_dinv_tau = s;
