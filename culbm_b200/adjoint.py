@@ -165,3 +165,34 @@ class _Lazy:
 
 
 _PressureDropFn = _Lazy
+
+
+def main(argv=None):
+    """Run one gradient of the pressure drop on the soft-obstacle channel and
+    print J, the gradient norms and the timings (JSON)."""
+    import argparse
+    import json
+
+    from . import scenes
+    ap = argparse.ArgumentParser(prog="python -m culbm_b200.adjoint", description=main.__doc__)
+    ap.add_argument("--domain", type=int, nargs=3, default=(128, 64, 64))
+    ap.add_argument("--window", type=int, nargs=2, default=(300, 500))
+    ap.add_argument("--checkpoint-every", type=int, default=50)
+    ap.add_argument("--bumps", type=int, default=16)
+    ap.add_argument("--precision", choices=("fp32", "fp64"), default="fp32")
+    ap.add_argument("--storage", default=None)
+    ap.add_argument("--inv-tau", type=float, default=0.5)
+    args = ap.parse_args(argv)
+    sc, soft = scenes.adjoint_channel(*args.domain, u_peak=0.04, bumps=args.bumps)
+    f, r, ux, uy, uz = sc.arrays()
+    with AdjointProblem(args.domain, window=args.window, checkpoint_every=args.checkpoint_every,
+                        precision=args.precision, storage=args.storage, inv_tau=args.inv_tau) as p:
+        p.set_state(f, r, ux, uy, uz, soft.reshape(-1))
+        J, g_tau, g_soft, g_mac = p.gradient()
+        info = p.info()
+    print(json.dumps({"J": J, "dJ_dinv_tau": g_tau, "dJ_dsoft_norm": float(np.linalg.norm(g_soft)),
+                      "dJ_dvx_in_norm": float(np.linalg.norm(g_mac[1])), **info}))
+
+
+if __name__ == "__main__":
+    main()
