@@ -87,7 +87,8 @@ class AdjConfig(C.Structure):
         ("precision", C.c_int32),
         ("storage", C.c_int32),
         ("hbm_budget_bytes", C.c_uint64),
-        ("reserved", C.c_uint32 * 8),
+        ("checkpoint_inner", C.c_int32),
+        ("reserved", C.c_uint32 * 7),
     ]
 
 
@@ -100,7 +101,9 @@ class AdjInfo(C.Structure):
         ("recompute_ms", C.c_float),
         ("adjoint_ms", C.c_float),
         ("steps", C.c_uint64),
-        ("reserved", C.c_uint32 * 8),
+        ("checkpoint_inner", C.c_int32),
+        ("inner_checkpoints", C.c_int32),
+        ("reserved", C.c_uint32 * 6),
     ]
 
 

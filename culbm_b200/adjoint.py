@@ -29,7 +29,7 @@ class AdjointProblem:
 
     def __init__(self, domain: Sequence[int], window=(300, 500), planes=(1, None), inv_tau=0.5,
                  checkpoint_every: int = 50, precision: str = "fp32", storage: Optional[str] = None,
-                 hbm_budget_bytes: int = 0, dev_id: int = 0):
+                 hbm_budget_bytes: int = 0, dev_id: int = 0, checkpoint_inner: int = 0):
         cfg = _capi.AdjConfig()
         check(lib().culbm_adj_config_init(C.byref(cfg)))
         cfg.dev_id = dev_id
@@ -45,6 +45,7 @@ class AdjointProblem:
             storage = "fp64" if precision == "fp64" else "fp32"
         cfg.storage = _capi.STORAGE[storage]
         cfg.hbm_budget_bytes = int(hbm_budget_bytes)
+        cfg.checkpoint_inner = int(checkpoint_inner)
         self.domain = tuple(int(v) for v in domain)
         self.n = self.domain[0] * self.domain[1] * self.domain[2]
         self._h = C.c_void_p()
@@ -98,6 +99,7 @@ class AdjointProblem:
         inf = _capi.AdjInfo()
         check(lib().culbm_adj_get_info(self._h, C.byref(inf)))
         return {"checkpoint_every": inf.checkpoint_every, "checkpoints": inf.checkpoints,
+                "checkpoint_inner": inf.checkpoint_inner, "inner_checkpoints": inf.inner_checkpoints,
                 "device_bytes": inf.device_bytes, "forward_ms": inf.forward_ms, "recompute_ms": inf.recompute_ms,
                 "adjoint_ms": inf.adjoint_ms, "steps": inf.steps}
 
@@ -177,7 +179,9 @@ def main(argv=None):
     ap = argparse.ArgumentParser(prog="python -m culbm_b200.adjoint", description=main.__doc__)
     ap.add_argument("--domain", type=int, nargs=3, default=(128, 64, 64))
     ap.add_argument("--window", type=int, nargs=2, default=(300, 500))
-    ap.add_argument("--checkpoint-every", type=int, default=50)
+    ap.add_argument("--checkpoint-every", type=int, default=50, help="0: smallest plan within --hbm-budget-gb")
+    ap.add_argument("--checkpoint-inner", type=int, default=0)
+    ap.add_argument("--hbm-budget-gb", type=float, default=0.0)
     ap.add_argument("--bumps", type=int, default=16)
     ap.add_argument("--precision", choices=("fp32", "fp64"), default="fp32")
     ap.add_argument("--storage", default=None)
@@ -186,6 +190,7 @@ def main(argv=None):
     sc, soft = scenes.adjoint_channel(*args.domain, u_peak=0.04, bumps=args.bumps)
     f, r, ux, uy, uz = sc.arrays()
     with AdjointProblem(args.domain, window=args.window, checkpoint_every=args.checkpoint_every,
+                        checkpoint_inner=args.checkpoint_inner, hbm_budget_bytes=int(args.hbm_budget_gb * 1e9),
                         precision=args.precision, storage=args.storage, inv_tau=args.inv_tau) as p:
         p.set_state(f, r, ux, uy, uz, soft.reshape(-1))
         J, g_tau, g_soft, g_mac = p.gradient()

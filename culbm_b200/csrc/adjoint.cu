@@ -58,17 +58,21 @@ struct Args {
     double* rho_plane;   // forward: rho of the two measurement planes of the pulled state, this step
                          // (null outside the objective window); [2][ny*nz]
     double* g_tau_block; // adjoint: one FP64 accumulator per thread block
+    const int* equ_cells; // adjoint: the EQU cells, increasing
+    int n_equ;
 };
 
 // Pull of the 27 populations of cell (x, y, z) from the state a.src with the
 // per-axis clamp (the same rule as the plain pull step).
-template <typename S, typename R>
+// With ROWS == ROWS_INNER the cell is known to lie off the y and z faces.
+template <int ROWS = ROWS_OUTER, typename S, typename R>
 __device__ __forceinline__ void pull_state(const Args<S, R>& a, int x, int y, int z, int i, R* f)
 {
     const Domain& D = a.dom;
+    constexpr bool inner = ROWS == ROWS_INNER;
     const int ndx = (x == 0) ? 0 : -1, pdx = (x == D.nx - 1) ? 0 : 1;
-    const int ndy = (y == 0) ? 0 : -D.nx, pdy = (y == D.ny - 1) ? 0 : D.nx;
-    const int ndz = (z == 0) ? 0 : -D.nxy, pdz = (z == D.nz - 1) ? 0 : D.nxy;
+    const int ndy = (!inner && y == 0) ? 0 : -D.nx, pdy = (!inner && y == D.ny - 1) ? 0 : D.nx;
+    const int ndz = (!inner && z == 0) ? 0 : -D.nxy, pdz = (!inner && z == D.nz - 1) ? 0 : D.nxy;
 #pragma unroll
     for (int d = 0; d < 27; ++d) {
         const int ox = cx_of(d) == 1 ? ndx : cx_of(d) == -1 ? pdx : 0;
@@ -256,146 +260,257 @@ __device__ __forceinline__ void block_accumulate(double v, double* slot)
 }
 
 // Adjoint of the stored population d of cell c: the sum of nu_d over the
-// cells whose pull of d reads c (the streaming target and clamp readers).
-template <int d, typename S, typename R>
-__device__ __forceinline__ R gather_lambda(const Args<S, R>& a, const CellCoord& c, bool edge)
+// cells whose pull of d reads c.  Off the y and z faces (ROWS_INNER) these
+// are the streaming target c + c_d, when it lies inside, and at an x-face the
+// cell (x, y + cy, z + cz) whose pull leaves the domain through that face and
+// is clamped back to c.  Cells on a y or z face (ROWS_OUTER) enumerate the
+// clamp readers in general.
+template <int d, int ROWS, typename S, typename R>
+__device__ __forceinline__ R gather_lambda(const Args<S, R>& a, const CellCoord& c)
 {
     const Domain& D = a.dom;
-    if (!edge) return a.nu_in[d][c.i + nb_off(D, d)];
-    R v = inside(D, c.x + cx_of(d), c.y + cy_of(d), c.z + cz_of(d)) ? a.nu_in[d][c.i + nb_off(D, d)] : R(0);
-    for_each_clamp_reader<d>(D, c.x, c.y, c.z,
-                             [&](int yx, int yy, int yz) { v += a.nu_in[d][yx + D.nx * (yy + D.ny * yz)]; });
-    return v;
+    constexpr int cx = cx_of(d);
+    if constexpr (ROWS == ROWS_INNER) {
+        const R* nu = a.nu_in[d] + (c.i + nb_off(D, d));
+        if constexpr (cx == 0) {
+            return *nu;
+        } else {
+            const bool leaves = cx == 1 ? c.x == D.nx - 1 : c.x == 0;
+            const bool clamped = cx == 1 ? c.x == 0 : c.x == D.nx - 1;
+            R v = leaves ? R(0) : *nu;
+            if (clamped) v += *(nu - cx);
+            return v;
+        }
+    } else {
+        R v = inside(D, c.x + cx, c.y + cy_of(d), c.z + cz_of(d)) ? a.nu_in[d][c.i + nb_off(D, d)] : R(0);
+        for_each_clamp_reader<d>(D, c.x, c.y, c.z,
+                                 [&](int yx, int yy, int yz) { v += a.nu_in[d][yx + D.nx * (yy + D.ny * yz)]; });
+        return v;
+    }
 }
 
-// Reverse of one cell update at step t.  Works on direction pairs (d, 26-d)
-// so that the gathered adjoint fills the registers the forward populations
-// free; the linearisation point uses feq in plain arithmetic (the forward
-// pass itself rounds exactly like the plain step).
-template <typename S, typename R>
+// rho and u of f in plain arithmetic (the linearisation point of the adjoint;
+// the forward pass keeps the exactly rounded moments).
+template <typename R>
+__device__ __forceinline__ void lin_moments(const R* f, R& rho, R& ux, R& uy, R& uz)
+{
+    R r = f[0], x = f[2] - f[0], y = f[6] - f[0], z = f[18] - f[0];
+#pragma unroll
+    for (int d = 1; d < 27; ++d) r += f[d];
+#pragma unroll
+    for (int k = 1; k < 9; ++k) {
+        const int lo = 9 * (k / 3) + (k % 3);
+        x += f[3 * k + 2] - f[3 * k];
+        y += f[lo + 6] - f[lo];
+        z += f[18 + k] - f[k];
+    }
+    rho = R(1) + r;
+    R inv;
+    if constexpr (sizeof(R) == 4)
+        inv = __frcp_rn(rho);
+    else
+        inv = R(1) / rho;
+    ux = x * inv;
+    uy = y * inv;
+    uz = z * inv;
+}
+
+template <typename R>
+__device__ __forceinline__ void swap_pairs_if(bool c, R* v)
+{
+#pragma unroll
+    for (int d = 0; d < 13; ++d) {
+        const R p = v[d], q = v[26 - d];
+        v[d] = c ? q : p;
+        v[26 - d] = c ? p : q;
+    }
+}
+
+// Reverse of bounce-back and soft collision for one cell, linearised at f
+// (the populations after the EQU overwrite, before bounce-back; plain
+// arithmetic).  l enters as the adjoint of the stored populations and leaves
+// as the adjoint of f; gs and gw are the cell's dJ/ds and dJ/dw (0 unless it
+// collides).  Straight-line code: the collision is evaluated for every cell
+// and selected.  With P = <l, f2>, Q = <l, B(f2)>, E = <l, feq(f2)>:
+//     dJ/ds = <l, B(f2) - C(f2)> = (Q - P) - w (E - P),
+//     dJ/dw = (1 - s) <l, feq - f2> = (1 - s) (E - P),
+// and E = (rho - 1) a_rho + 3 Lcu + 9/2 Lcu2 - 3/2 |u|^2 L0 comes from the
+// same weighted sums as J_C^T, so no per-direction equilibrium is formed.
+template <typename R>
+__device__ __forceinline__ void reverse_cell(uint8_t op, R w, R s, R* f, R* l, R& gs, R& gw)
+{
+    const bool bb = (op & OP_BB) != 0, col = (op & OP_COLLIDE) && (op & OP_STORE);
+    const R om = R(1) - w;
+    swap_pairs_if(bb, f);
+    R rho, ux, uy, uz;
+    lin_moments(f, rho, ux, uy, uz);
+    const R uu = ux * ux + uy * uy + uz * uz;
+    R P = 0, QmP = 0, L0 = 0, Lx = 0, Ly = 0, Lz = 0, Lcu = 0, Lcu2 = 0, Lcx = 0, Lcy = 0, Lcz = 0;
+#pragma unroll
+    for (int d = 0; d < 13; ++d) {
+        const int e = 26 - d;
+        const R ld = l[d], le = l[e], fd = f[d], fe = f[e];
+        const R cx = R(cx_of(d)), cy = R(cy_of(d)), cz = R(cz_of(d)), wd = weight<R>(d);
+        const R cu = cx * ux + cy * uy + cz * uz;
+        P += ld * fd + le * fe;
+        QmP += (ld - le) * (fe - fd);
+        const R sp = wd * (ld + le), sm = wd * (ld - le);
+        L0 += sp;
+        Lx += cx * sm;
+        Ly += cy * sm;
+        Lz += cz * sm;
+        Lcu += cu * sm;
+        const R cusp = cu * sp;
+        Lcu2 += cu * cusp;
+        Lcx += cx * cusp;
+        Lcy += cy * cusp;
+        Lcz += cz * cusp;
+    }
+    P += l[13] * f[13];
+    L0 += weight<R>(13) * l[13];
+    const R a1 = R(3) * Lcu + R(4.5) * Lcu2 - R(1.5) * uu * L0;
+    const R ar = L0 + a1;
+    const R emp = ((rho - R(1)) * ar + a1) - P;
+    gs = col ? QmP - w * emp : R(0);
+    gw = col ? (R(1) - s) * emp : R(0);
+    // l <- (1-s) J_C^T l + s B(l),  (J_C^T l)_e = (1-w) l_e + w (a_rho + c_e.b - u.b)
+    const R bx = w * (R(3) * Lx + R(9) * Lcx - R(3) * ux * L0);
+    const R by = w * (R(3) * Ly + R(9) * Lcy - R(3) * uy * L0);
+    const R bz = w * (R(3) * Lz + R(9) * Lcz - R(3) * uz * L0);
+    const R q = w * ar - (ux * bx + uy * by + uz * bz);
+#pragma unroll
+    for (int d = 0; d < 13; ++d) {
+        const int e = 26 - d;
+        const R ld = l[d], le = l[e];
+        const R cb = R(cx_of(d)) * bx + R(cy_of(d)) * by + R(cz_of(d)) * bz;
+        const R jd = om * ld + (q + cb);
+        const R je = om * le + (q - cb);
+        l[d] = col ? jd + s * (le - jd) : ld;
+        l[e] = col ? je + s * (ld - je) : le;
+    }
+    const R j13 = om * l[13] + q;
+    l[13] = col ? j13 + s * (l[13] - j13) : l[13];
+    swap_pairs_if(bb, l);
+}
+
+// Reverse of one cell update at step t for a cell without EQU (EQU cells
+// only get nu = dJ/df here; k_adj_equ does the rest of their work).  All
+// loads are issued before any decision on the op byte: the pull and the
+// gather stay inside the domain for every cell.
+template <int ROWS, typename S, typename R>
 __device__ __forceinline__ void adj_cell(const Args<S, R>& a, const CellCoord c, double& gtau_local)
 {
     const uint8_t op = a.ops[c.i];
-    const bool store = (op & OP_STORE) != 0, edge = (op & OP_EDGE) != 0;
-    R f[27];
-    if (op & OP_EQU) {
-        equilibrium<R>(R(a.rho[c.i]), R(a.vx[c.i]), R(a.vy[c.i]), R(a.vz[c.i]), f);
-    } else if (op & OP_LOAD) {
-        pull_state(a, c.x, c.y, c.z, c.i, f);
-    } else {
+    const R s = R(a.soft[c.i]);
+    R f[27], l[27];
+    // warps of inner rows without an x-face lane (a warp-uniform choice) pull
+    // and gather without any clamp handling
+    const int xw = c.x - (threadIdx.x & 31);
+    if (ROWS == ROWS_INNER && xw != 0 && xw + 31 < a.dom.nx - 1) {
 #pragma unroll
-        for (int d = 0; d < 27; ++d) f[d] = R(0);
-    }
-    if (op & OP_BB) {
-#pragma unroll
-        for (int d = 0; d < 13; ++d) {
-            const R t = f[d];
-            f[d] = f[26 - d];
-            f[26 - d] = t;
+        for (int d = 0; d < 27; ++d) {
+            f[d] = Cvt<S, R>::ld(a.src.p[d] + (c.i - nb_off(a.dom, d)));
+            l[d] = a.nu_in[d][c.i + nb_off(a.dom, d)];
         }
-    }
-    R l[27];
-    if (!store) {
-#pragma unroll
-        for (int d = 0; d < 27; ++d) l[d] = R(0);
-    } else if (!(op & OP_COLLIDE)) {
-        for_dirs([&](auto dd) {
-            constexpr int d = decltype(dd)::value;
-            l[d] = gather_lambda<d>(a, c, edge);
-        });
     } else {
-        const R s = R(a.soft[c.i]);
-        const R w = a.inv_tau, om = R(1) - w;
-        R rho, ux, uy, uz;
-        moments(f, rho, ux, uy, uz);
-        const R uu = ux * ux + uy * uy + uz * uz;
-        R gs = 0, gw = 0, L0 = 0, Lx = 0, Ly = 0, Lz = 0, Lcu = 0, Lcu2 = 0, Lcx = 0, Lcy = 0, Lcz = 0;
+        pull_state<ROWS>(a, c.x, c.y, c.z, c.i, f);
         for_dirs([&](auto dd) {
             constexpr int d = decltype(dd)::value;
-            if constexpr (d < 13) {
-                constexpr int e = 26 - d;
-                const R ld = gather_lambda<d>(a, c, edge), le = gather_lambda<e>(a, c, edge);
-                const R cx = R(cx_of(d)), cy = R(cy_of(d)), cz = R(cz_of(d)), wd = weight<R>(d);
-                const R cu = cx * ux + cy * uy + cz * uz;
-                const R base = R(1) + R(4.5) * cu * cu - R(1.5) * uu;
-                const R feqd = wd * (rho * (base + R(3) * cu) - R(1));
-                const R feqe = wd * (rho * (base - R(3) * cu) - R(1));
-                const R Cd = w * feqd + om * f[d], Ce = w * feqe + om * f[e];
-                gs += ld * (f[e] - Cd) + le * (f[d] - Ce);
-                gw += ld * (feqd - f[d]) + le * (feqe - f[e]);
-                const R sp = wd * (ld + le), sm = wd * (ld - le);
-                L0 += sp;
-                Lx += cx * sm;
-                Ly += cy * sm;
-                Lz += cz * sm;
-                Lcu += cu * sm;
-                Lcu2 += cu * cu * sp;
-                Lcx += cx * cu * sp;
-                Lcy += cy * cu * sp;
-                Lcz += cz * cu * sp;
-                l[d] = ld;
-                l[e] = le;
-            } else if constexpr (d == 13) {
-                const R l13 = gather_lambda<13>(a, c, edge);
-                const R w0 = weight<R>(13);
-                const R feq = w0 * (rho * (R(1) - R(1.5) * uu) - R(1));
-                const R C13 = w * feq + om * f[13];
-                gs += l13 * (f[13] - C13);
-                gw += l13 * (feq - f[13]);
-                L0 += w0 * l13;
-                l[13] = l13;
-            }
+            l[d] = gather_lambda<d, ROWS>(a, c);
         });
+    }
+    const bool load = (op & OP_LOAD) != 0, store = (op & OP_STORE) != 0, equ = (op & OP_EQU) != 0;
+#pragma unroll
+    for (int d = 0; d < 27; ++d) {
+        f[d] = load ? f[d] : R(0);
+        l[d] = store ? l[d] : R(0);
+    }
+    R gs, gw;
+    reverse_cell(op, a.inv_tau, s, f, l, gs, gw);
+    if (!equ && (op & OP_COLLIDE) && store) {
         a.g_soft[c.i] += static_cast<double>(gs);
-        gtau_local = static_cast<double>((R(1) - s) * gw);
-        // lambda2 = (1-s) J_C^T lambda + s B(lambda)
-        const R ar = L0 + R(3) * Lcu + R(4.5) * Lcu2 - R(1.5) * uu * L0;
-        const R bx = R(3) * Lx + R(9) * Lcx - R(3) * ux * L0;
-        const R by = R(3) * Ly + R(9) * Lcy - R(3) * uy * L0;
-        const R bz = R(3) * Lz + R(9) * Lcz - R(3) * uz * L0;
-        const R ub = ux * bx + uy * by + uz * bz;
-#pragma unroll
-        for (int d = 0; d < 13; ++d) {
-            const int e = 26 - d;
-            const R ld = l[d], le = l[e];
-            const R cb = R(cx_of(d)) * bx + R(cy_of(d)) * by + R(cz_of(d)) * bz;
-            const R jd = om * ld + w * (ar + cb - ub);
-            const R je = om * le + w * (ar - cb - ub);
-            l[d] = (R(1) - s) * jd + s * le;
-            l[e] = (R(1) - s) * je + s * ld;
-        }
-        l[13] = (R(1) - s) * (om * l[13] + w * (ar - ub)) + s * l[13];
+        gtau_local = static_cast<double>(gw);
     }
-    if (op & OP_BB) {
-#pragma unroll
-        for (int d = 0; d < 13; ++d) {
-            const R t = l[d];
-            l[d] = l[26 - d];
-            l[26 - d] = t;
-        }
-    }
-    if (op & OP_EQU) {
-        const R r_in = R(a.rho[c.i]);
-        R ar, bx, by, bz;
-        feq_vjp(l, R(a.vx[c.i]), R(a.vy[c.i]), R(a.vz[c.i]), ar, bx, by, bz);
-        a.g_mac[0][c.i] += static_cast<double>(ar);
-        a.g_mac[1][c.i] += static_cast<double>(r_in * bx);
-        a.g_mac[2][c.i] += static_cast<double>(r_in * by);
-        a.g_mac[3][c.i] += static_cast<double>(r_in * bz);
-    }
-    const bool pulls = (op & OP_LOAD) && !(op & OP_EQU);
+    const bool pulls = load && !equ;
     const R g = objective_term(a, c.x, op);
 #pragma unroll
     for (int d = 0; d < 27; ++d) a.nu_out[d][c.i] = (pulls ? l[d] : R(0)) + g;
 }
 
+// The EQU cell i of one adjoint step: f1 = feq(rho_in, u_in), the gather
+// with the general clamp rule, the reverse of bounce-back and collision, and
+// dJ/d(rho_in, u_in) from d feq / d(rho, u).  Its nu (no pull, so dJ/df
+// only) is written by adj_cell.
 template <typename S, typename R>
-__global__ void __launch_bounds__(256) k_adj_step(const __grid_constant__ Args<S, R> a)
+__device__ __forceinline__ void adj_equ_cell(const Args<S, R>& a, int i, double& gtau_local)
 {
-    const CellCoord c = cell_of_thread(a.dom);
+    const Domain& D = a.dom;
+    CellCoord c;
+    c.i = i;
+    c.x = i % D.nx;
+    c.y = (i / D.nx) % D.ny;
+    c.z = i / D.nxy;
+    c.valid = true;
+    const uint8_t op = a.ops[i];
+    const R r_in = R(a.rho[i]), vx = R(a.vx[i]), vy = R(a.vy[i]), vz = R(a.vz[i]);
+    R f[27], l[27];
+    equilibrium<R>(r_in, vx, vy, vz, f);
+    const bool store = (op & OP_STORE) != 0;
+    for_dirs([&](auto dd) {
+        constexpr int d = decltype(dd)::value;
+        l[d] = store ? gather_lambda<d, ROWS_OUTER>(a, c) : R(0);
+    });
+    R gs, gw;
+    reverse_cell(op, a.inv_tau, R(a.soft[i]), f, l, gs, gw);
+    if ((op & OP_COLLIDE) && store) {
+        a.g_soft[i] += static_cast<double>(gs);
+        gtau_local = static_cast<double>(gw);
+    }
+    R ar, bx, by, bz;
+    feq_vjp(l, vx, vy, vz, ar, bx, by, bz);
+    a.g_mac[0][i] += static_cast<double>(ar);
+    a.g_mac[1][i] += static_cast<double>(r_in * bx);
+    a.g_mac[2][i] += static_cast<double>(r_in * by);
+    a.g_mac[3][i] += static_cast<double>(r_in * bz);
+}
+
+// Row blocks of one adjoint-step launch: the EQU cells (256 per block, the
+// longest per-thread work, first), then ROWS_OUTER and ROWS_INNER rows.
+struct AdjLayout {
+    int equ_blocks, outer_blocks;
+};
+
+inline AdjLayout adj_layout(const Domain& D, int n_equ)
+{
+    const int gx = (D.nx + 31) / 32;
+    return {((n_equ + 255) / 256 + gx - 1) / gx, row_blocks(D, row_count(D, ROWS_OUTER))};
+}
+
+inline dim3 adj_grid(const Domain& D, int n_equ)
+{
+    const AdjLayout L = adj_layout(D, n_equ);
+    return row_grid(D, L.equ_blocks + L.outer_blocks + row_blocks(D, row_count(D, ROWS_INNER)));
+}
+
+// One adjoint step over all cells (block-uniform roles, see AdjLayout); each
+// block adds its invTau gradient into its own slot of g_tau_block.
+template <typename S, typename R>
+__global__ void __launch_bounds__(256, sizeof(R) == 4 ? 3 : 1)
+    k_adj_step(const __grid_constant__ Args<S, R> a, AdjLayout L)
+{
+    const int rb = row_block();
     double gtau_local = 0.0;
-    if (c.valid) adj_cell(a, c, gtau_local);
-    block_accumulate(gtau_local, a.g_tau_block + (blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)));
+    CellCoord c;
+    if (rb < L.equ_blocks) {
+        const int k = (blockIdx.x + gridDim.x * rb) * 256 + threadIdx.x + 32 * threadIdx.y;
+        if (k < a.n_equ) adj_equ_cell(a, a.equ_cells[k], gtau_local);
+    } else if (rb < L.equ_blocks + L.outer_blocks) {
+        if (row_cell<ROWS_OUTER>(a.dom, c, rb - L.equ_blocks)) adj_cell<ROWS_OUTER>(a, c, gtau_local);
+    } else {
+        if (row_cell<ROWS_INNER>(a.dom, c, rb - L.equ_blocks - L.outer_blocks))
+            adj_cell<ROWS_INNER>(a, c, gtau_local);
+    }
+    block_accumulate(gtau_local, a.g_tau_block + (blockIdx.x + gridDim.x * rb));
 }
 
 template <typename S>
@@ -425,8 +540,10 @@ struct culbm_adj {
     float* d_mac[4] = {};
     float* d_soft = nullptr;
     double inv_tau = 0.5;
-    int K = 0, nckpt = 0, nseg = 0;
-    void* d_ckpt = nullptr;     // nckpt states
+    int K = 0, K2 = 0;          // checkpoint strides: outer, inner (0: one level)
+    int nckpt = 0, ninner = 0, nseg = 0;
+    void* d_ckpt = nullptr;     // nckpt states: F^t for t = 0, K, 2K, ...
+    void* d_inner = nullptr;    // ninner states inside one outer segment (two levels only)
     void* d_seg = nullptr;      // nseg states (at least 2)
     void* d_nu = nullptr;       // 2 x 27 N of the arithmetic type
     double* d_gsoft = nullptr;
@@ -434,7 +551,10 @@ struct culbm_adj {
     double* d_gmac = nullptr;   // 4 N
     double* d_psum = nullptr;   // 2 per time step of the window
     double* d_rho_plane = nullptr;  // window x 2 planes x ny*nz
-    long long n_tau_blocks = 0;
+    long long n_tau_blocks = 0;     // blocks of one adjoint-step launch (one FP64 slot each)
+    long long tau_capacity = 0;
+    int* d_equ = nullptr;           // EQU cells, increasing
+    int n_equ = 0, equ_capacity = 0;
     int n_in = 0, n_out = 0;
     uint64_t device_bytes = 0;
     float t_fwd = 0, t_rec = 0, t_adj = 0;
@@ -467,10 +587,12 @@ void adj_release(culbm_adj* a)
     for (auto& p : a->d_mac) cudaFree(p);
     cudaFree(a->d_soft);
     cudaFree(a->d_ckpt);
+    cudaFree(a->d_inner);
     cudaFree(a->d_seg);
     cudaFree(a->d_nu);
     cudaFree(a->d_gsoft);
     cudaFree(a->d_gtau);
+    cudaFree(a->d_equ);
     cudaFree(a->d_gmac);
     cudaFree(a->d_psum);
     cudaFree(a->d_rho_plane);
@@ -492,10 +614,12 @@ culbm_status adj_with_storage(const culbm_adj* a, F&& f)
     }
 }
 
+enum StateSet { CKPT, INNER, SEG };
+
 template <typename S>
-S* state_ptr(culbm_adj* a, bool ckpt, int slot)
+S* state_ptr(culbm_adj* a, StateSet set, int slot)
 {
-    S* base = static_cast<S*>(ckpt ? a->d_ckpt : a->d_seg);
+    S* base = static_cast<S*>(set == CKPT ? a->d_ckpt : set == INNER ? a->d_inner : a->d_seg);
     return base + static_cast<long long>(slot) * 27 * a->n;
 }
 
@@ -593,24 +717,58 @@ template <typename S>
 culbm_status run_forward(culbm_adj* a, bool checkpoints)
 {
     const int T = a->cfg.window[1], K = a->K;
-    S* s0 = state_ptr<S>(a, true, 0);
+    S* s0 = state_ptr<S>(a, CKPT, 0);
     CULBM_TRY(fill_rest<S>(a, s0));
     auto slot_of = [&](int t) -> S* {
-        if (checkpoints && t % K == 0) return state_ptr<S>(a, true, t / K);
-        return state_ptr<S>(a, false, t & 1);
+        if (checkpoints && t % K == 0) return state_ptr<S>(a, CKPT, t / K);
+        return state_ptr<S>(a, SEG, t & 1);
     };
     return forward_run<S>(a, 0, T, s0, slot_of, true);
+}
+
+// Reverse sweep over the steps t in [tb, te) (te - tb <= nseg + 1) starting
+// from the state F^tb: recompute F^{tb+1} .. F^{te-1} into the segment
+// slots, then run the adjoint steps te-1 .. tb.
+template <typename S>
+culbm_status adjoint_segment(culbm_adj* a, int tb, int te, S* start, adj::Args<S, typename ArithOf<S>::type>& g,
+                             typename ArithOf<S>::type* const nu[2], int& cur, float& rec, float& adjms)
+{
+    using R = typename ArithOf<S>::type;
+    const int t0 = a->cfg.window[0], t1 = a->cfg.window[1];
+    const double nT = t1 - t0 + 1;
+    const R obj_in = static_cast<R>(1.0 / (3.0 * a->n_in * nT));
+    const R obj_out = static_cast<R>(-1.0 / (3.0 * a->n_out * nT));
+    const dim3 block = cell_block();
+    const adj::AdjLayout L = adj::adj_layout(a->dom, a->n_equ);
+    const dim3 gr = adj::adj_grid(a->dom, a->n_equ);
+    auto slot_of = [&](int t) -> S* { return state_ptr<S>(a, SEG, t - tb - 1); };
+    CULBM_TRY(forward_run<S>(a, tb, te - 1, start, slot_of, false));
+    rec += elapsed(a);
+    for (int t = te - 1; t >= tb; --t) {
+        S* st = (t == tb) ? start : state_ptr<S>(a, SEG, t - tb - 1);
+        set_pops<S, R>(g.src, st, a->n);
+        for (int d = 0; d < 27; ++d) {
+            g.nu_in[d] = nu[cur] + d * a->n;
+            g.nu_out[d] = nu[1 - cur] + d * a->n;
+        }
+        const bool in_win = t >= t0 && t <= t1;
+        g.obj_in = in_win ? obj_in : R(0);
+        g.obj_out = in_win ? obj_out : R(0);
+        adj::k_adj_step<S, R><<<gr, block, 0, a->stream>>>(g, L);
+        CULBM_CUDA(cudaGetLastError());
+        cur = 1 - cur;
+    }
+    adjms += elapsed(a);
+    return CULBM_OK;
 }
 
 template <typename S>
 culbm_status run_gradient(culbm_adj* a)
 {
     using R = typename ArithOf<S>::type;
-    const int T = a->cfg.window[1], K = a->K;
+    const int T = a->cfg.window[1], K = a->K, K2 = a->K2;
     const int t0 = a->cfg.window[0], t1 = a->cfg.window[1];
     const double nT = t1 - t0 + 1;
-    const R obj_in = static_cast<R>(1.0 / (3.0 * a->n_in * nT));
-    const R obj_out = static_cast<R>(-1.0 / (3.0 * a->n_out * nT));
     const dim3 grid = cell_grid(a->dom), block = cell_block();
 
     CULBM_CUDA(cudaEventRecord(a->ev[0], a->stream));
@@ -620,14 +778,16 @@ culbm_status run_gradient(culbm_adj* a)
     CULBM_CUDA(cudaMemsetAsync(a->d_gsoft, 0, a->n * sizeof(double), a->stream));
     CULBM_CUDA(cudaMemsetAsync(a->d_gtau, 0, a->n_tau_blocks * sizeof(double), a->stream));
     CULBM_CUDA(cudaMemsetAsync(a->d_gmac, 0, 4 * a->n * sizeof(double), a->stream));
-    R* nu[2] = {static_cast<R*>(a->d_nu), static_cast<R*>(a->d_nu) + 27 * a->n};
+    R* const nu[2] = {static_cast<R*>(a->d_nu), static_cast<R*>(a->d_nu) + 27 * a->n};
     auto g = base_args<S>(a);
     g.g_tau_block = a->d_gtau;
+    g.equ_cells = a->d_equ;
+    g.n_equ = a->n_equ;
     int cur = 0;
     {
         for (int d = 0; d < 27; ++d) g.nu_out[d] = nu[cur] + d * a->n;
-        g.obj_in = (T >= t0 && T <= t1) ? obj_in : R(0);
-        g.obj_out = (T >= t0 && T <= t1) ? obj_out : R(0);
+        g.obj_in = (T >= t0 && T <= t1) ? static_cast<R>(1.0 / (3.0 * a->n_in * nT)) : R(0);
+        g.obj_out = (T >= t0 && T <= t1) ? static_cast<R>(-1.0 / (3.0 * a->n_out * nT)) : R(0);
         adj::k_adj_init<S, R><<<grid, block, 0, a->stream>>>(g);
         CULBM_CUDA(cudaGetLastError());
     }
@@ -635,30 +795,76 @@ culbm_status run_gradient(culbm_adj* a)
     CULBM_CUDA(cudaEventRecord(a->ev[0], a->stream));
     for (int k = (T - 1) / K; k >= 0; --k) {
         const int tb = k * K, te = std::min(T, (k + 1) * K);
-        // recompute F^{tb+1} .. F^{te-1} into segment slots 0..
-        S* ck = state_ptr<S>(a, true, k);
-        auto slot_of = [&](int t) -> S* { return state_ptr<S>(a, false, t - tb - 1); };
-        CULBM_TRY(forward_run<S>(a, tb, te - 1, ck, slot_of, false));
-        rec += elapsed(a);
-        for (int t = te - 1; t >= tb; --t) {
-            S* st = (t == tb) ? ck : state_ptr<S>(a, false, t - tb - 1);
-            set_pops<S, R>(g.src, st, a->n);
-            for (int d = 0; d < 27; ++d) {
-                g.nu_in[d] = nu[cur] + d * a->n;
-                g.nu_out[d] = nu[1 - cur] + d * a->n;
-            }
-            const bool in_win = t >= t0 && t <= t1;
-            g.obj_in = in_win ? obj_in : R(0);
-            g.obj_out = in_win ? obj_out : R(0);
-            adj::k_adj_step<S, R><<<grid, block, 0, a->stream>>>(g);
-            CULBM_CUDA(cudaGetLastError());
-            cur = 1 - cur;
+        S* ck = state_ptr<S>(a, CKPT, k);
+        if (K2 == 0) {
+            CULBM_TRY(adjoint_segment<S>(a, tb, te, ck, g, nu, cur, rec, adjms));
+            continue;
         }
-        adjms += elapsed(a);
+        // two levels: one pass over the outer segment stores F^{tb + j K2},
+        // then each inner segment is swept in reverse
+        const int nin = (te - tb - 1) / K2;
+        if (nin > 0) {
+            auto slot_of = [&](int t) -> S* {
+                const int r = t - tb;
+                return r % K2 == 0 ? state_ptr<S>(a, INNER, r / K2 - 1) : state_ptr<S>(a, SEG, t & 1);
+            };
+            CULBM_TRY(forward_run<S>(a, tb, tb + nin * K2, ck, slot_of, false));
+            rec += elapsed(a);
+        }
+        for (int j = nin; j >= 0; --j) {
+            const int sb = tb + j * K2, se = std::min(te, sb + K2);
+            S* start = j ? state_ptr<S>(a, INNER, j - 1) : ck;
+            CULBM_TRY(adjoint_segment<S>(a, sb, se, start, g, nu, cur, rec, adjms));
+        }
     }
     a->t_rec = rec;
     a->t_adj = adjms;
     return CULBM_OK;
+}
+
+// Checkpoint plan: outer stride K, inner stride K2 (0: one level) and the
+// number of full states each needs.
+struct CkptPlan {
+    int K = 1, K2 = 0, nckpt = 0, ninner = 0, nseg = 0;
+    long long states() const { return 1ll * nckpt + ninner + nseg; }
+};
+
+CkptPlan make_plan(int T, int K, int K2)
+{
+    CkptPlan p;
+    p.K = K;
+    p.K2 = K2;
+    p.nckpt = (T + K - 1) / K + 1;
+    p.ninner = K2 ? (K - 1) / K2 : 0;
+    p.nseg = std::max((K2 ? K2 : K) - 1, 2);
+    return p;
+}
+
+// Smallest plan (in states) of one level, else of two levels, within
+// max_states; one level recomputes every step once, two levels twice.
+bool choose_plan(int T, long long max_states, CkptPlan& out)
+{
+    T = std::max(T, 1);
+    CkptPlan best;
+    bool have = false;
+    for (int K = 1; K <= T; ++K) {
+        const CkptPlan p = make_plan(T, K, 0);
+        if (!have || p.states() < best.states()) best = p, have = true;
+    }
+    if (best.states() <= max_states) {
+        out = best;
+        return true;
+    }
+    have = false;
+    for (int K = 3; K <= T; ++K) {
+        const int s = std::max(1, static_cast<int>(std::lround(std::sqrt(static_cast<double>(K)))));
+        for (int K2 = std::max(1, s / 2); K2 <= std::min(K - 1, 2 * s + 1); ++K2) {
+            const CkptPlan p = make_plan(T, K, K2);
+            if (!have || p.states() < best.states()) best = p, have = true;
+        }
+    }
+    out = best;
+    return have && best.states() <= max_states;
 }
 
 }  // namespace
@@ -718,20 +924,43 @@ culbm_status culbm_adj_create(const culbm_adj_config* cfg, culbm_adj** out)
     a->rsize = f64 ? 8 : 4;
     const int T = c.window[1];
     const double state_bytes = 27.0 * n * a->esize;
-    if (c.checkpoint_every > 0) {
-        a->K = c.checkpoint_every;
-    } else {
-        a->K = std::max(1, static_cast<int>(std::lround(std::sqrt(std::max(T, 1)))));
+    if (c.checkpoint_inner < 0 || (c.checkpoint_inner > 0 && c.checkpoint_inner >= c.checkpoint_every)) {
+        delete a;
+        return fail(CULBM_ERR_INVALID_ARGUMENT, "checkpoint_inner must be 0 or lie in [1, checkpoint_every)");
     }
-    a->nckpt = (T + a->K - 1) / a->K + 1;
-    a->nseg = std::max(a->K - 1, 2);
     auto body = [&]() -> culbm_status {
         CULBM_CUDA(cudaSetDevice(a->dev));
         CULBM_CUDA(cudaStreamCreateWithFlags(&a->stream, cudaStreamNonBlocking));
         CULBM_CUDA(cudaEventCreate(&a->ev[0]));
         CULBM_CUDA(cudaEventCreate(&a->ev[1]));
-        const double need = (a->nckpt + a->nseg) * state_bytes + 2.0 * 27 * n * a->rsize + 5.0 * 8 * n +
-                            16.0 * (c.window[1] - c.window[0] + 1) * c.domain_dim[1] * c.domain_dim[2];
+        // everything but the states (an upper bound): adjoint populations,
+        // per-cell inputs and gradients, EQU list and block slots, objective
+        // planes and sums
+        const double fixed = 2.0 * 27 * n * a->rsize + 5.0 * 8 * n + 27.0 * n +
+                             16.0 * (c.window[1] - c.window[0] + 1) * (1.0 + c.domain_dim[1] * c.domain_dim[2]);
+        double budget = static_cast<double>(c.hbm_budget_bytes);
+        if (budget == 0) {
+            size_t free_b = 0, total_b = 0;
+            CULBM_CUDA(cudaMemGetInfo(&free_b, &total_b));
+            budget = 0.95 * static_cast<double>(free_b) - (256 << 20);
+        }
+        CkptPlan plan;
+        if (c.checkpoint_every > 0) {
+            plan = make_plan(T, c.checkpoint_every, c.checkpoint_inner);
+        } else {
+            const long long max_states = static_cast<long long>(std::max(0.0, (budget - fixed) / state_bytes));
+            if (!choose_plan(T, max_states, plan))
+                return fail(CULBM_ERR_OUT_OF_MEMORY,
+                            "no checkpoint plan fits: the smallest needs " +
+                                std::to_string((plan.states() * state_bytes + fixed) / 1e9) + " GB of " +
+                                std::to_string(budget / 1e9) + " GB");
+        }
+        a->K = plan.K;
+        a->K2 = plan.K2;
+        a->nckpt = plan.nckpt;
+        a->ninner = plan.ninner;
+        a->nseg = plan.nseg;
+        const double need = plan.states() * state_bytes + fixed;
         if (c.hbm_budget_bytes && need > static_cast<double>(c.hbm_budget_bytes))
             return fail(CULBM_ERR_OUT_OF_MEMORY, "adjoint needs " + std::to_string(need / 1e9) +
                                                      " GB, over the HBM budget of " +
@@ -746,16 +975,12 @@ culbm_status culbm_adj_create(const culbm_adj_config* cfg, culbm_adj** out)
         CULBM_TRY(adj_alloc(a, &p, n * sizeof(float), "soft field"));
         a->d_soft = static_cast<float*>(p);
         CULBM_TRY(adj_alloc(a, &a->d_ckpt, static_cast<size_t>(a->nckpt * state_bytes), "checkpoints"));
+        if (a->ninner)
+            CULBM_TRY(adj_alloc(a, &a->d_inner, static_cast<size_t>(a->ninner * state_bytes), "inner checkpoints"));
         CULBM_TRY(adj_alloc(a, &a->d_seg, static_cast<size_t>(a->nseg * state_bytes), "recompute segment"));
         CULBM_TRY(adj_alloc(a, &a->d_nu, 2ull * 27 * n * a->rsize, "adjoint populations"));
         CULBM_TRY(adj_alloc(a, &p, n * sizeof(double), "soft gradient"));
         a->d_gsoft = static_cast<double*>(p);
-        {
-            const dim3 g = cell_grid(a->dom);
-            a->n_tau_blocks = 1ll * g.x * g.y * g.z;
-        }
-        CULBM_TRY(adj_alloc(a, &p, a->n_tau_blocks * sizeof(double), "invTau gradient"));
-        a->d_gtau = static_cast<double*>(p);
         CULBM_TRY(adj_alloc(a, &p, 4 * n * sizeof(double), "EQU input gradients"));
         a->d_gmac = static_cast<double*>(p);
         const long long nt = c.window[1] - c.window[0] + 1;
@@ -797,6 +1022,7 @@ culbm_status culbm_adj_set_state(culbm_adj* a, const uint32_t* flag, const float
     const Domain& D = a->dom;
     const size_t n = static_cast<size_t>(a->n);
     std::vector<uint8_t> ops(n);
+    std::vector<int> equ;
     constexpr uint32_t kFluid = FLAG_LOAD | FLAG_COLLIDE | FLAG_STORE;
     int n_in = 0, n_out = 0;
     for (int z = 0; z < D.nz; ++z)
@@ -807,8 +1033,8 @@ culbm_status culbm_adj_set_state(culbm_adj* a, const uint32_t* flag, const float
                 if ((fl & 0x1Fu) != 0 && !(fl & FLAG_STORE))
                     return fail(CULBM_ERR_INVALID_ARGUMENT, "adjoint model: every active cell needs STORE");
                 uint8_t op = static_cast<uint8_t>(fl & 0x1Fu);
-                if (x == 0 || x == D.nx - 1 || y == 0 || y == D.ny - 1 || z == 0 || z == D.nz - 1) op |= OP_EDGE;
                 ops[i] = op;
+                if (op & OP_EQU) equ.push_back(static_cast<int>(i));
                 if (op & OP_COLLIDE) {
                     n_in += x == a->cfg.plane_x[0];
                     n_out += x == a->cfg.plane_x[1];
@@ -817,6 +1043,39 @@ culbm_status culbm_adj_set_state(culbm_adj* a, const uint32_t* flag, const float
     if (n_in == 0 || n_out == 0) return fail(CULBM_ERR_INVALID_ARGUMENT, "a measurement plane has no COLLIDE cell");
     a->n_in = n_in;
     a->n_out = n_out;
+    CULBM_CUDA(cudaStreamSynchronize(a->stream));
+    const int n_equ = static_cast<int>(equ.size());
+    // the EQU list and the invTau block slots of the adjoint-step launch
+    // (whose grid grows with the EQU count) are sized here
+    a->n_equ = 0;
+    if (n_equ > a->equ_capacity) {
+        CULBM_CUDA(cudaFree(a->d_equ));
+        a->d_equ = nullptr;
+        a->device_bytes -= a->equ_capacity * sizeof(int);
+        a->equ_capacity = 0;
+        void* p = nullptr;
+        CULBM_TRY(adj_alloc(a, &p, n_equ * sizeof(int), "EQU cell list"));
+        a->d_equ = static_cast<int*>(p);
+        a->equ_capacity = n_equ;
+    }
+    {
+        const dim3 gr = adj::adj_grid(a->dom, n_equ);
+        const long long slots = 1ll * gr.x * gr.y * gr.z;
+        if (slots > a->tau_capacity) {
+            CULBM_CUDA(cudaFree(a->d_gtau));
+            a->d_gtau = nullptr;
+            a->device_bytes -= a->tau_capacity * sizeof(double);
+            a->tau_capacity = 0;
+            void* p = nullptr;
+            CULBM_TRY(adj_alloc(a, &p, slots * sizeof(double), "invTau gradient"));
+            a->d_gtau = static_cast<double*>(p);
+            a->tau_capacity = slots;
+        }
+        a->n_tau_blocks = slots;
+    }
+    a->n_equ = n_equ;
+    if (n_equ)
+        CULBM_CUDA(cudaMemcpyAsync(a->d_equ, equ.data(), n_equ * sizeof(int), cudaMemcpyHostToDevice, a->stream));
     CULBM_CUDA(cudaMemcpyAsync(a->d_ops, ops.data(), n, cudaMemcpyHostToDevice, a->stream));
     const float* mac[4] = {rho, vx, vy, vz};
     const float dflt[4] = {1.0f, 0.0f, 0.0f, 0.0f};
@@ -887,6 +1146,8 @@ culbm_status culbm_adj_get_info(culbm_adj* a, culbm_adj_info* info)
     std::memset(info, 0, sizeof(*info));
     info->checkpoint_every = a->K;
     info->checkpoints = a->nckpt;
+    info->checkpoint_inner = a->K2;
+    info->inner_checkpoints = a->ninner;
     info->device_bytes = a->device_bytes;
     info->forward_ms = a->t_fwd;
     info->recompute_ms = a->t_rec;

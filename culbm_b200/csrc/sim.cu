@@ -239,18 +239,15 @@ culbm_status plain_steps(culbm_sim* s, uint32_t nsteps)
         } else {
             auto a = make_args<S>(s, 0, 0);
             a.seed = seed;
-            const int ri = row_count(s->dom, ROWS_INNER), ro = row_count(s->dom, ROWS_OUTER);
-            const dim3 gi((s->dom.nx + 31) / 32, (ri + 7) / 8), go((s->dom.nx + 31) / 32, (ro + 7) / 8);
-            if (s->aa_phase == 0) {
-                if (ri) k_aa_odd<S, R, ROWS_INNER><<<gi, b, 0, s->stream>>>(a);
-                if (ro) k_aa_odd<S, R, ROWS_OUTER><<<go, b, 0, s->stream>>>(a);
-            } else {
-                if (ri) k_aa_even<S, R, ROWS_INNER><<<gi, b, 0, s->stream>>>(a);
-                if (ro) k_aa_even<S, R, ROWS_OUTER><<<go, b, 0, s->stream>>>(a);
-            }
+            const int ob = row_blocks(s->dom, row_count(s->dom, ROWS_OUTER));
+            const int ib = row_blocks(s->dom, row_count(s->dom, ROWS_INNER));
+            const dim3 gr = row_grid(s->dom, ob + ib);
+            if (s->aa_phase == 0)
+                k_aa_odd<S, R><<<gr, b, 0, s->stream>>>(a, ob);
+            else
+                k_aa_even<S, R><<<gr, b, 0, s->stream>>>(a, ob);
             CULBM_CUDA(cudaGetLastError());
             s->aa_phase ^= 1;
-            s->launches += (ri ? 1 : 0) + (ro ? 1 : 0) - 1;
         }
         s->launches += 1;
     }

@@ -238,25 +238,30 @@ __global__ void __launch_bounds__(256) k_pull_step(const __grid_constant__ StepA
 // for_each_clamp_reader) also writes f_d into slot d of each such y: nobody
 // else reads or writes that slot during the step, and y reads it next step.
 //
-// Each in-place step runs as two launches over disjoint sets of x-rows (cells
-// of different rows never touch the same locations in a step's pattern, so
-// the order does not matter):
+// Each in-place step is one launch over two disjoint sets of x-rows, taken
+// block by block (cells of different rows never touch the same locations in
+// a step's pattern, so the order does not matter):
 //   ROWS_INNER: rows with 0 < y < ny-1 and 0 < z < nz-1.  Only the x-faces
 //     of such a row are on the boundary, and there only the x component of a
 //     pull can leave the domain, so the clamp handling reduces to pointer
 //     selects and predicated stores; the code stays straight-line.
 //   ROWS_OUTER: rows on a y or z face, processed with the general per-axis
 //     clamp code (about 2 (ny + nz) of the ny*nz rows).
-// Rows are contiguous in x, so both launches keep warp accesses coalesced.
+// The ROWS_OUTER blocks come first in the launch, so their longer code runs
+// beside the ROWS_INNER blocks instead of as a tail.  Rows are contiguous in
+// x, so warp accesses stay coalesced.
 enum RowSet : int { ROWS_INNER = 0, ROWS_OUTER = 1 };
 
-// Cell of this thread for a row set; false if the thread has none.
+// Row block of this thread block: grid y and z together (see row_grid).
+__device__ __forceinline__ int row_block() { return blockIdx.y + gridDim.y * blockIdx.z; }
+
+// Cell of this thread in row block rb of a row set; false if it has none.
 template <int ROWS>
-__device__ __forceinline__ bool row_cell(const Domain& D, CellCoord& c)
+__device__ __forceinline__ bool row_cell(const Domain& D, CellCoord& c, int rb)
 {
     c.x = blockIdx.x * blockDim.x + threadIdx.x;
     if (c.x >= D.nx) return false;
-    const int r = blockIdx.y * blockDim.y + threadIdx.y;
+    const int r = rb * blockDim.y + threadIdx.y;
     if (ROWS == ROWS_INNER) {
         const int iy = D.ny - 2;
         if (iy <= 0 || D.nz <= 2) return false;
@@ -290,6 +295,17 @@ inline int row_count(const Domain& D, int rows)
     return nzf * D.ny + (D.nz > 2 ? nyf * (D.nz - 2) : 0);
 }
 
+// Row blocks (8 rows of (32, 8) thread blocks) of a row set.
+inline int row_blocks(const Domain& D, int rows) { return (rows + 7) / 8; }
+
+// Launch grid for `blocks` row blocks: spread over grid y and z so that any
+// ny * nz fits the 65535 limit of grid y.
+inline dim3 row_grid(const Domain& D, int blocks)
+{
+    const int gy = blocks < 32768 ? blocks : 32768;
+    return dim3((D.nx + 31) / 32, gy > 0 ? gy : 1, gy > 0 ? (blocks + gy - 1) / gy : 1);
+}
+
 template <typename S>
 __device__ __forceinline__ const S* xface_edge_ptr(const S* edge, const Domain& D, const EdgeLayout& L, int side,
                                                    int d, int y, int z)
@@ -299,11 +315,11 @@ __device__ __forceinline__ const S* xface_edge_ptr(const S* edge, const Domain& 
 }
 
 template <typename S, typename R, int ROWS>
-__global__ void __launch_bounds__(256) k_aa_odd(const __grid_constant__ StepArgs<S, R> a)
+__device__ __forceinline__ void aa_odd_cell(const StepArgs<S, R>& a, int rb)
 {
     CellCoord c;
     const Domain& D = a.dom;
-    if (!row_cell<ROWS>(D, c)) return;
+    if (!row_cell<ROWS>(D, c, rb)) return;
     const uint8_t op = a.ops[c.i];
     const uint32_t hc = cell_hash(static_cast<uint32_t>(c.i), a.seed);
     // Warps without an x-face lane (all but the first and last of a row) take
@@ -362,11 +378,11 @@ __global__ void __launch_bounds__(256) k_aa_odd(const __grid_constant__ StepArgs
 // the edge-buffer slot of (y, d): the next odd step's clamped pull of y reads
 // it there, because slot 26-d of the source is overwritten during that step.
 template <typename S, typename R, int ROWS>
-__global__ void __launch_bounds__(256) k_aa_even(const __grid_constant__ StepArgs<S, R> a)
+__device__ __forceinline__ void aa_even_cell(const StepArgs<S, R>& a, int rb)
 {
     CellCoord c;
     const Domain& D = a.dom;
-    if (!row_cell<ROWS>(D, c)) return;
+    if (!row_cell<ROWS>(D, c, rb)) return;
     const uint8_t op = a.ops[c.i];
     const uint32_t hc = cell_hash(static_cast<uint32_t>(c.i), a.seed);
     R f[27];
@@ -398,6 +414,28 @@ __global__ void __launch_bounds__(256) k_aa_even(const __grid_constant__ StepArg
             });
         });
     }
+}
+
+// In-place steps over both row sets: row blocks below outer_blocks are
+// ROWS_OUTER rows, the rest ROWS_INNER (a block-uniform choice).
+template <typename S, typename R>
+__global__ void __launch_bounds__(256) k_aa_odd(const __grid_constant__ StepArgs<S, R> a, int outer_blocks)
+{
+    const int rb = row_block();
+    if (rb < outer_blocks)
+        aa_odd_cell<S, R, ROWS_OUTER>(a, rb);
+    else
+        aa_odd_cell<S, R, ROWS_INNER>(a, rb - outer_blocks);
+}
+
+template <typename S, typename R>
+__global__ void __launch_bounds__(256) k_aa_even(const __grid_constant__ StepArgs<S, R> a, int outer_blocks)
+{
+    const int rb = row_block();
+    if (rb < outer_blocks)
+        aa_even_cell<S, R, ROWS_OUTER>(a, rb);
+    else
+        aa_even_cell<S, R, ROWS_INNER>(a, rb - outer_blocks);
 }
 
 // Moments of the pulled populations, written where the DUMP bits are set.

@@ -152,7 +152,6 @@ __device__ __forceinline__ void tile_store_global(const TileArgs<S, R>& a, const
 {
     S* base = a.g.base[sel];
     const long long off = gaddr(a.g, a.dom, offz, c.gx, c.gy, c.gz);
-#pragma unroll
     const uint32_t hc = tile_hash(a, c.gi);
 #pragma unroll
     for (int d = 0; d < 27; ++d) gstore<S, R, HINT>(base + d * a.g.stride + off, f[d], hc, d);

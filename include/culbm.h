@@ -236,12 +236,17 @@ typedef struct culbm_adj_config {
     float inv_tau;                 /* default 0.5 */
     int32_t window[2];             /* [t0, t1], states after t steps; the forward runs t1 steps (default 300, 500) */
     int32_t plane_x[2];            /* inlet / outlet measurement planes (default 1 and nx-2) */
-    int32_t checkpoint_every;      /* K; 0 = choose about sqrt(t1) within hbm_budget_bytes */
+    int32_t checkpoint_every;      /* K: states kept every K steps of the forward pass.  0 = the smallest plan
+                                      that fits hbm_budget_bytes: one level (K near sqrt(t1), every step
+                                      recomputed once) if it fits, else two levels (recomputed twice) */
     int32_t precision;             /* 0: FP32 forward and adjoint (default), 1: FP64 */
     int32_t storage;               /* forward states and checkpoints: CULBM_STORAGE_F32 (default), _F16, _F16_SR;
                                       CULBM_STORAGE_F64 with precision 1 */
-    uint64_t hbm_budget_bytes;     /* 0 = no limit */
-    uint32_t reserved[8];
+    uint64_t hbm_budget_bytes;     /* 0 = no limit given; the automatic plan then fits the device's free memory */
+    int32_t checkpoint_inner;      /* K2 with K > 0: two levels.  Each K segment is recomputed once, keeping
+                                      states every K2 steps, then swept K2 steps at a time; 1 <= K2 < K.
+                                      0 = one level (default) */
+    uint32_t reserved[7];
 } culbm_adj_config;
 
 typedef struct culbm_adj culbm_adj;
@@ -254,7 +259,9 @@ typedef struct culbm_adj_info {
     float recompute_ms;            /* forward recomputation between checkpoints */
     float adjoint_ms;              /* adjoint sweep */
     uint64_t steps;                /* forward steps per pass (t1) */
-    uint32_t reserved[8];
+    int32_t checkpoint_inner;      /* K2 of a two-level plan, 0 for one level */
+    int32_t inner_checkpoints;     /* states held for the inner level */
+    uint32_t reserved[6];
 } culbm_adj_info;
 
 culbm_status culbm_adj_config_init(culbm_adj_config* cfg);

@@ -116,3 +116,25 @@ def test_invalid_blocking_rejected_before_device(culbm, dims, tile, inner, needl
     st, msg = _create(cfg)
     assert st == 1, (st, msg)
     assert needle in msg
+
+
+@pytest.mark.parametrize("mutate,needle", [
+    (lambda c: setattr(c, "checkpoint_inner", 50), "checkpoint_inner"),
+    (lambda c: setattr(c, "checkpoint_inner", -1), "checkpoint_inner"),
+    (lambda c: (setattr(c, "checkpoint_every", 0), setattr(c, "checkpoint_inner", 4)), "checkpoint_inner"),
+    (lambda c: c.window.__setitem__(1, 10), "objective window"),
+    (lambda c: setattr(c, "inv_tau", 2.0), "invTau"),
+    (lambda c: setattr(c, "precision", 1), "FP64 precision"),
+    (lambda c: setattr(c, "precision", 2), "precision"),
+    (lambda c: c.domain_dim.__setitem__(2, 0), "domain_dim"),
+])
+def test_adjoint_config_rejected_before_the_device(culbm, mutate, needle):
+    from culbm_b200 import _capi
+    cfg = _capi.AdjConfig()
+    assert _capi.lib().culbm_adj_config_init(C.byref(cfg)) == 0
+    assert cfg.checkpoint_every == 50 and cfg.checkpoint_inner == 0 and list(cfg.window) == [300, 500]
+    mutate(cfg)
+    h = C.c_void_p()
+    st = _capi.lib().culbm_adj_create(C.byref(cfg), C.byref(h))
+    assert st != 0 and not h.value
+    assert needle in _capi.lib().culbm_last_error().decode()

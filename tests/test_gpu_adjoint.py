@@ -119,17 +119,45 @@ def test_fd_inlet_profile(fd_case):
         assert abs(a - b) <= 1e-4 * abs(b), (i, a, b)
 
 
-def test_checkpoint_stride_does_not_change_gradients():
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_checkpoint_plan_does_not_change_gradients(precision):
+    """One level with K = 1, 7, 60 and two levels (K, K2) = (20, 3), (13, 12):
+    recomputation is deterministic, so the gradients agree bit for bit."""
     dims = (20, 10, 10)
     sc, f, r, ux, uy, uz, soft = case(*dims, bumps=4)
     outs = []
-    for K in (1, 7, 60):
-        with AdjointProblem(dims, window=(30, 60), checkpoint_every=K, precision="fp64") as p:
+    for K, K2 in ((1, 0), (7, 0), (60, 0), (20, 3), (13, 12)):
+        with AdjointProblem(dims, window=(30, 60), checkpoint_every=K, checkpoint_inner=K2,
+                            precision=precision) as p:
             p.set_state(f, r, ux, uy, uz, soft)
             outs.append(p.gradient())
+            assert p.info()["checkpoint_inner"] == K2
     for o in outs[1:]:
         assert o[0] == outs[0][0] and o[1] == outs[0][1]
         assert np.array_equal(o[2], outs[0][2]) and np.array_equal(o[3], outs[0][3])
+
+
+def test_automatic_plan_fits_the_budget():
+    """checkpoint_every = 0: one level near sqrt(t1) when it fits, two levels
+    under a budget too small for that, and a clear error below any plan."""
+    dims = (32, 16, 16)
+    sc, f, r, ux, uy, uz, soft = case(*dims, bumps=4)
+    state = 27 * f.size * 4
+    with AdjointProblem(dims, window=(100, 400), checkpoint_every=0) as p:
+        one = p.info()
+        p.set_state(f, r, ux, uy, uz, soft)
+        ref = p.gradient()
+    assert one["checkpoint_inner"] == 0 and 15 <= one["checkpoint_every"] <= 25
+    budget = one["device_bytes"] - 12 * state
+    with AdjointProblem(dims, window=(100, 400), checkpoint_every=0, hbm_budget_bytes=budget) as p:
+        two = p.info()
+        p.set_state(f, r, ux, uy, uz, soft)
+        got = p.gradient()
+    assert two["checkpoint_inner"] > 0 and two["device_bytes"] <= budget
+    assert got[0] == ref[0] and got[1] == ref[1] and np.array_equal(got[2], ref[2])
+    from culbm_b200._capi import CulbmError
+    with pytest.raises(CulbmError, match="no checkpoint plan fits"):
+        AdjointProblem(dims, window=(100, 400), checkpoint_every=0, hbm_budget_bytes=budget // 4)
 
 
 def test_fp32_adjoint_close_to_fp64():
