@@ -211,6 +211,79 @@ def fp64_errors(culbm, steps=1000):
                         f"{steps} steps, vs FP64 storage+arithmetic", "errors": out}
 
 
+def mixed_precision_512(culbm, steps):
+    """The 512x512x256 channel with 120 spheres (radii 6-18): in-place
+    streaming with FP32, FP16 and BF16 storage, plain and L2-blocked."""
+    from culbm_b200 import scenes
+    sc = scenes.spheres_512()
+    peak, _ = peaks()
+    out = {"workload": "512x512x256 channel, 120 seeded spheres r in [6,18], invTau 0.5, ux_in 0.05",
+           "cells": sc.n, "steps": steps, "runs": {}}
+    for name, (op, st, tile) in {
+        "inplace_fp32": (0, "fp32", None),
+        "inplace_fp16": (0, "fp16", None),
+        "inplace_fp16sr": (0, "fp16sr", None),
+        "inplace_bf16": (0, "bf16", None),
+        "inplace_bf16sr": (0, "bf16sr", None),
+        "blocked_inplace_fp32": (3, "fp32", (128, 64, 64)),
+        "blocked_inplace_fp16sr": (3, "fp16sr", (128, 64, 64)),
+    }.items():
+        try:
+            mlups, mps, _ = measure(culbm, sc, 1, op, st, steps, 3, tile=tile, inner=5)
+            out["runs"][name] = {"mlups": round(mlups, 1), "ms_per_step": round(mps, 4),
+                                 "hbm_frac_of_measured": round(mlups * 1e6 * BYTES_PER_LUP[st] / 1e9 / peak, 4),
+                                 "policy": "streamPolicy 1, optPolicy %d" % op +
+                                           (f", tile {tile}, innerLoop 5" if op else "")}
+        except Exception as e:   # report, do not hide
+            out["runs"][name] = {"error": str(e)}
+    return out
+
+
+def adjoint_runs():
+    """Gradient of the pressure drop on the soft-obstacle channels: the
+    128x64x64 case (FP32, window 300-500, checkpoints every 50) and the
+    288x272x280 case (48 bumps, 2000 steps, FP16-SR states, plan chosen for
+    a 120 GB budget) with its gradient error against FP32 states."""
+    from culbm_b200 import scenes
+    from culbm_b200.adjoint import AdjointProblem
+
+    def run(dims, bumps, window, storage, **kw):
+        sc, soft = scenes.adjoint_channel(*dims, u_peak=0.04, bumps=bumps, seed=7)
+        with AdjointProblem(dims, window=window, storage=storage, **kw) as p:
+            p.set_state(*sc.arrays(), soft.reshape(-1))
+            J, gt, gs, gm = p.gradient()
+            inf = p.info()
+        n, T = sc.n, window[1]
+        total = inf["forward_ms"] + inf["recompute_ms"] + inf["adjoint_ms"]
+        summary = {"storage": storage, "J": J, "dJ_dinv_tau": gt,
+                   "checkpoint_every": inf["checkpoint_every"], "checkpoint_inner": inf["checkpoint_inner"],
+                   "device_gb": round(inf["device_bytes"] / 1e9, 2),
+                   "forward_ms": round(inf["forward_ms"], 2), "recompute_ms": round(inf["recompute_ms"], 2),
+                   "adjoint_ms": round(inf["adjoint_ms"], 2),
+                   "cost_ratio": round((inf["recompute_ms"] + inf["adjoint_ms"]) / inf["forward_ms"], 3),
+                   "forward_mlups": round(n * T / (inf["forward_ms"] * 1e-3) / 1e6, 1),
+                   "adjoint_step_mlups": round(n * T / (inf["adjoint_ms"] * 1e-3) / 1e6, 1),
+                   "gradient_mlups": round(n * T / (total * 1e-3) / 1e6, 1)}
+        return summary, (J, gt, gs, gm)
+
+    out = {"cost_ratio_definition": "(recompute + adjoint sweep) / forward pass, device time"}
+    out["channel_128x64x64"], _ = run((128, 64, 64), 16, (300, 500), "fp32", checkpoint_every=50)
+    budget = 120e9
+    big = {}
+    for st in ("fp16sr", "fp32"):
+        big[st] = run((288, 272, 280), 48, (1500, 2000), st, checkpoint_every=0, hbm_budget_bytes=int(budget))
+    g16, g32 = big["fp16sr"][1], big["fp32"][1]
+
+    def rel(a, b):
+        return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / max(np.linalg.norm(np.asarray(b)), 1e-300))
+
+    out["channel_288x272x280"] = {
+        "hbm_budget_gb": budget / 1e9, "fp16sr": big["fp16sr"][0], "fp32": big["fp32"][0],
+        "fp16sr_vs_fp32": {"J_rel": rel(g16[0], g32[0]), "dJ_dinv_tau_rel": rel(g16[1], g32[1]),
+                           "dJ_dsoft_rel_l2": rel(g16[2], g32[2]), "dJ_dvx_in_rel_l2": rel(g16[3][1], g32[3][1])}}
+    return out
+
+
 def e2e_run(culbm, scene, steps, sp=1):
     """Through the public API with host buffers: pinned H2D of the init state,
     `steps` steps, the dump kernel and the D2H read of rho/vx/vy/vz."""
@@ -317,6 +390,14 @@ def run_ours(args):
         errs = fp64_errors(culbm_b200, steps=args.err_steps)
     except Exception as e:
         errs = {"error": str(e)}
+    try:
+        mixed = mixed_precision_512(culbm_b200, max(20, args.steps // 10))
+    except Exception as e:
+        mixed = {"error": str(e)}
+    try:
+        adjoint = adjoint_runs() if not args.no_adjoint else None
+    except Exception as e:
+        adjoint = {"error": str(e)}
     e2e_mlups, h2d, d2h = e2e_run(culbm_b200, sc, args.steps)
     cpu = cpu_baseline(sc) if ws == 1 else None
 
@@ -350,6 +431,8 @@ def run_ours(args):
         "cpu_baseline": cpu,
         "variants": extra,
         "fp64_error": errs,
+        "mixed_precision_512x512x256": mixed,
+        "adjoint": adjoint,
     }
     print(json.dumps(line), flush=True)
 
@@ -411,6 +494,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=50)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--err-steps", type=int, default=1000)
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint runs (about 30 s)")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be at least 3")

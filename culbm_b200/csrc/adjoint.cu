@@ -64,8 +64,9 @@ struct Args {
 
 // Pull of the 27 populations of cell (x, y, z) from the state a.src with the
 // per-axis clamp (the same rule as the plain pull step).
-// With ROWS == ROWS_INNER the cell is known to lie off the y and z faces.
-template <int ROWS = ROWS_OUTER, typename S, typename R>
+// With ROWS == ROWS_INNER the cell is known to lie off the y and z faces;
+// RAW loads the stored values without the format's scale (ld_raw).
+template <int ROWS = ROWS_OUTER, bool RAW = false, typename S, typename R>
 __device__ __forceinline__ void pull_state(const Args<S, R>& a, int x, int y, int z, int i, R* f)
 {
     const Domain& D = a.dom;
@@ -78,7 +79,8 @@ __device__ __forceinline__ void pull_state(const Args<S, R>& a, int x, int y, in
         const int ox = cx_of(d) == 1 ? ndx : cx_of(d) == -1 ? pdx : 0;
         const int oy = cy_of(d) == 1 ? ndy : cy_of(d) == -1 ? pdy : 0;
         const int oz = cz_of(d) == 1 ? ndz : cz_of(d) == -1 ? pdz : 0;
-        f[d] = Cvt<S, R>::ld(a.src.p[d] + (i + ox + oy + oz));
+        const S* p = a.src.p[d] + (i + ox + oy + oz);
+        f[d] = RAW ? ld_raw<S, R>(p) : Cvt<S, R>::ld(p);
     }
 }
 
@@ -292,7 +294,7 @@ __device__ __forceinline__ R gather_lambda(const Args<S, R>& a, const CellCoord&
 // rho and u of f in plain arithmetic (the linearisation point of the adjoint;
 // the forward pass keeps the exactly rounded moments).
 template <typename R>
-__device__ __forceinline__ void lin_moments(const R* f, R& rho, R& ux, R& uy, R& uz)
+__device__ __forceinline__ void lin_moments(const R* f, R fscale, R& rho, R& ux, R& uy, R& uz)
 {
     R r = f[0], x = f[2] - f[0], y = f[6] - f[0], z = f[18] - f[0];
 #pragma unroll
@@ -304,12 +306,13 @@ __device__ __forceinline__ void lin_moments(const R* f, R& rho, R& ux, R& uy, R&
         y += f[lo + 6] - f[lo];
         z += f[18 + k] - f[k];
     }
-    rho = R(1) + r;
+    rho = R(1) + fscale * r;
     R inv;
     if constexpr (sizeof(R) == 4)
         inv = __frcp_rn(rho);
     else
         inv = R(1) / rho;
+    inv *= fscale;
     ux = x * inv;
     uy = y * inv;
     uz = z * inv;
@@ -326,24 +329,26 @@ __device__ __forceinline__ void swap_pairs_if(bool c, R* v)
     }
 }
 
-// Reverse of bounce-back and soft collision for one cell, linearised at f
-// (the populations after the EQU overwrite, before bounce-back; plain
-// arithmetic).  l enters as the adjoint of the stored populations and leaves
-// as the adjoint of f; gs and gw are the cell's dJ/ds and dJ/dw (0 unless it
-// collides).  Straight-line code: the collision is evaluated for every cell
-// and selected.  With P = <l, f2>, Q = <l, B(f2)>, E = <l, feq(f2)>:
+// Reverse of bounce-back and soft collision for one cell, linearised at
+// fscale * f (f: the populations after the EQU overwrite, before bounce-back,
+// possibly without their storage scale; plain arithmetic).  l enters as the
+// adjoint of the stored populations and leaves as the adjoint of f; gs and gw
+// are the cell's dJ/ds and dJ/dw (0 unless it collides).  The sums are
+// evaluated for every cell; bounce-back and the update of l are skipped by
+// (mostly warp-uniform) branches.  With P = <l, f2>, Q = <l, B(f2)>,
+// E = <l, feq(f2)>:
 //     dJ/ds = <l, B(f2) - C(f2)> = (Q - P) - w (E - P),
 //     dJ/dw = (1 - s) <l, feq - f2> = (1 - s) (E - P),
 // and E = (rho - 1) a_rho + 3 Lcu + 9/2 Lcu2 - 3/2 |u|^2 L0 comes from the
 // same weighted sums as J_C^T, so no per-direction equilibrium is formed.
 template <typename R>
-__device__ __forceinline__ void reverse_cell(uint8_t op, R w, R s, R* f, R* l, R& gs, R& gw)
+__device__ __forceinline__ void reverse_cell(uint8_t op, R w, R s, R fscale, R* f, R* l, R& gs, R& gw)
 {
     const bool bb = (op & OP_BB) != 0, col = (op & OP_COLLIDE) && (op & OP_STORE);
     const R om = R(1) - w;
-    swap_pairs_if(bb, f);
+    if (bb) swap_pairs_if(true, f);
     R rho, ux, uy, uz;
-    lin_moments(f, rho, ux, uy, uz);
+    lin_moments(f, fscale, rho, ux, uy, uz);
     const R uu = ux * ux + uy * uy + uz * uz;
     R P = 0, QmP = 0, L0 = 0, Lx = 0, Ly = 0, Lz = 0, Lcu = 0, Lcu2 = 0, Lcx = 0, Lcy = 0, Lcz = 0;
 #pragma unroll
@@ -366,13 +371,18 @@ __device__ __forceinline__ void reverse_cell(uint8_t op, R w, R s, R* f, R* l, R
         Lcy += cy * cusp;
         Lcz += cz * cusp;
     }
-    P += l[13] * f[13];
+    P = fscale * (P + l[13] * f[13]);
+    QmP *= fscale;
     L0 += weight<R>(13) * l[13];
     const R a1 = R(3) * Lcu + R(4.5) * Lcu2 - R(1.5) * uu * L0;
     const R ar = L0 + a1;
     const R emp = ((rho - R(1)) * ar + a1) - P;
     gs = col ? QmP - w * emp : R(0);
     gw = col ? (R(1) - s) * emp : R(0);
+    if (!col) {
+        if (bb) swap_pairs_if(true, l);
+        return;
+    }
     // l <- (1-s) J_C^T l + s B(l),  (J_C^T l)_e = (1-w) l_e + w (a_rho + c_e.b - u.b)
     const R bx = w * (R(3) * Lx + R(9) * Lcx - R(3) * ux * L0);
     const R by = w * (R(3) * Ly + R(9) * Lcy - R(3) * uy * L0);
@@ -385,12 +395,12 @@ __device__ __forceinline__ void reverse_cell(uint8_t op, R w, R s, R* f, R* l, R
         const R cb = R(cx_of(d)) * bx + R(cy_of(d)) * by + R(cz_of(d)) * bz;
         const R jd = om * ld + (q + cb);
         const R je = om * le + (q - cb);
-        l[d] = col ? jd + s * (le - jd) : ld;
-        l[e] = col ? je + s * (ld - je) : le;
+        l[d] = jd + s * (le - jd);
+        l[e] = je + s * (ld - je);
     }
     const R j13 = om * l[13] + q;
-    l[13] = col ? j13 + s * (l[13] - j13) : l[13];
-    swap_pairs_if(bb, l);
+    l[13] = j13 + s * (l[13] - j13);
+    if (bb) swap_pairs_if(true, l);
 }
 
 // Reverse of one cell update at step t for a cell without EQU (EQU cells
@@ -409,24 +419,26 @@ __device__ __forceinline__ void adj_cell(const Args<S, R>& a, const CellCoord c,
     if (ROWS == ROWS_INNER && xw != 0 && xw + 31 < a.dom.nx - 1) {
 #pragma unroll
         for (int d = 0; d < 27; ++d) {
-            f[d] = Cvt<S, R>::ld(a.src.p[d] + (c.i - nb_off(a.dom, d)));
+            f[d] = ld_raw<S, R>(a.src.p[d] + (c.i - nb_off(a.dom, d)));
             l[d] = a.nu_in[d][c.i + nb_off(a.dom, d)];
         }
     } else {
-        pull_state<ROWS>(a, c.x, c.y, c.z, c.i, f);
+        pull_state<ROWS, true>(a, c.x, c.y, c.z, c.i, f);
         for_dirs([&](auto dd) {
             constexpr int d = decltype(dd)::value;
             l[d] = gather_lambda<d, ROWS>(a, c);
         });
     }
     const bool load = (op & OP_LOAD) != 0, store = (op & OP_STORE) != 0, equ = (op & OP_EQU) != 0;
+    if (!load || !store) {
 #pragma unroll
-    for (int d = 0; d < 27; ++d) {
-        f[d] = load ? f[d] : R(0);
-        l[d] = store ? l[d] : R(0);
+        for (int d = 0; d < 27; ++d) {
+            f[d] = load ? f[d] : R(0);
+            l[d] = store ? l[d] : R(0);
+        }
     }
     R gs, gw;
-    reverse_cell(op, a.inv_tau, s, f, l, gs, gw);
+    reverse_cell(op, a.inv_tau, s, R(RawScale<S>::value), f, l, gs, gw);
     if (!equ && (op & OP_COLLIDE) && store) {
         a.g_soft[c.i] += static_cast<double>(gs);
         gtau_local = static_cast<double>(gw);
@@ -461,7 +473,7 @@ __device__ __forceinline__ void adj_equ_cell(const Args<S, R>& a, int i, double&
         l[d] = store ? gather_lambda<d, ROWS_OUTER>(a, c) : R(0);
     });
     R gs, gw;
-    reverse_cell(op, a.inv_tau, R(a.soft[i]), f, l, gs, gw);
+    reverse_cell(op, a.inv_tau, R(a.soft[i]), R(1), f, l, gs, gw);
     if ((op & OP_COLLIDE) && store) {
         a.g_soft[i] += static_cast<double>(gs);
         gtau_local = static_cast<double>(gw);

@@ -14,6 +14,7 @@
 #pragma once
 
 #include <cstdint>
+#include <type_traits>
 
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
@@ -157,6 +158,23 @@ template <> struct Cvt<BF16SR, float> {
     static __device__ __forceinline__ void st_sr(BF16SR* p, float v, uint32_t rnd) { p->bits = enc(v, rnd); }
     static __device__ __forceinline__ void st_sr_cs(BF16SR* p, float v, uint32_t rnd) { __stcs(&p->bits, enc(v, rnd)); }
 };
+
+// Raw load for consumers that are linear in the populations: the stored
+// value without the format's power-of-two scale; f = RawScale<S>::value * raw.
+template <typename S> struct RawScale { static constexpr float value = 1.0f; };
+template <> struct RawScale<__half> { static constexpr float value = kHalfInvScale; };
+template <> struct RawScale<Half16SR> { static constexpr float value = kHalfInvScale; };
+
+template <typename S, typename R>
+__device__ __forceinline__ R ld_raw(const S* p)
+{
+    if constexpr (std::is_same<S, __half>::value)
+        return __half2float(*p);
+    else if constexpr (std::is_same<S, Half16SR>::value)
+        return __half2float(__ushort_as_half(p->bits));
+    else
+        return Cvt<S, R>::ld(p);
+}
 
 // Store of population d of the cell whose cell_hash for this step is hcell:
 // stochastic rounding for the SR formats, the format's plain conversion
