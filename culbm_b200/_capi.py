@@ -32,7 +32,7 @@ FIELD = {"rho": 0, "vx": 1, "vy": 2, "vz": 3}
 EXPORTED = (
     "culbm_config_init", "culbm_create", "culbm_destroy", "culbm_load_state", "culbm_load_state_folder",
     "culbm_step", "culbm_step_timed", "culbm_synchronize", "culbm_moments", "culbm_get_field", "culbm_dump",
-    "culbm_get_step", "culbm_get_pulled_ddf", "culbm_set_ddf", "culbm_mass_momentum", "culbm_get_info",
+    "culbm_get_step", "culbm_get_pulled_ddf", "culbm_set_ddf", "culbm_mass_momentum", "culbm_mass_momentum_noalloc", "culbm_get_info",
     "culbm_last_error", "culbm_status_string", "culbm_abi_version", "culbm_debug_inject_cuda_error",
     "culbm_adj_config_init", "culbm_adj_create", "culbm_adj_destroy", "culbm_adj_set_state",
     "culbm_adj_set_inv_tau", "culbm_adj_forward", "culbm_adj_gradient", "culbm_adj_get_info",
@@ -141,6 +141,7 @@ def lib():
     L.culbm_get_pulled_ddf.argtypes = [vp, vp, C.c_int32]
     L.culbm_set_ddf.argtypes = [vp, vp, C.c_int32]
     L.culbm_mass_momentum.argtypes = [vp, C.POINTER(C.c_double)]
+    L.culbm_mass_momentum_noalloc.argtypes = [vp, C.c_uint64, vp, C.POINTER(C.c_double)]
     L.culbm_get_info.argtypes = [vp, C.POINTER(Info)]
     L.culbm_last_error.restype = C.c_char_p
     L.culbm_status_string.restype = C.c_char_p

@@ -199,6 +199,25 @@ culbm_status culbm_set_ddf(culbm_sim* sim, const void* host_in, int32_t in_type)
  * out[0] = mass, out[1..3] = momentum x,y,z.  No reference counterpart. */
 culbm_status culbm_mass_momentum(culbm_sim* sim, double out[4]);
 
+/*
+ * No reference counterpart.  The reduction of culbm_mass_momentum over a
+ * caller-owned FP32 population buffer in device memory: 27 planes of n
+ * values, plane d at d_ddf + d*n (the layout culbm_get_pulled_ddf writes),
+ * every cell counted: out[0] = sum(1 + sum_d f_d), out[1..3] = sum(c_d f_d).
+ * Runs on the current device and on `stream` (a cudaStream_t; NULL is the
+ * legacy default stream) and blocks until out is written.
+ *
+ * Allocates nothing: the block partial sums live in a fixed 37,920-byte
+ * static device array, so n may not exceed CULBM_NOALLOC_MAX_CELLS
+ * (CULBM_ERR_INVALID_ARGUMENT beyond it).  The first call on a device looks
+ * up that array's address with the device current (cudaGetSymbolAddress);
+ * make that first call before any stream capture.  Calls that overlap on the
+ * GPU (other streams or host threads, same device) share the array and
+ * race: serialise them.  The sum order depends on n alone.
+ */
+#define CULBM_NOALLOC_MAX_CELLS 77594624ull
+culbm_status culbm_mass_momentum_noalloc(const float* d_ddf, uint64_t n, void* stream, double out[4]);
+
 typedef struct culbm_info {
     uint64_t cells;                 /* N */
     uint64_t device_bytes;          /* bytes the library allocated on the device */
