@@ -252,3 +252,73 @@ def read_folder(folder: str, nx: int, ny: int, nz: int) -> Scene:
 def read_dump(folder: str, field_name: str, step: int, nx: int, ny: int, nz: int) -> np.ndarray:
     """A dump file <folder>/<field>_<step>.dat as shape (nz, ny, nx)."""
     return np.fromfile(os.path.join(folder, f"{field_name}_{step}.dat"), dtype="<f4").reshape((nz, ny, nx))
+
+
+# -------------------------------------------------------------------- CLI ---
+
+_KINDS = ("default", "channel", "channel-cube", "correctness", "spheres", "sphere64", "spheres288", "spheres512",
+          "adjoint-channel")
+
+
+def build_scene(kind: str, domain=None, u_in=0.05, spheres=40, radii=(4.0, 12.0), seed=12345, bumps=16,
+                scale=1.0) -> Tuple[Scene, Optional[np.ndarray]]:
+    """A scene by name (see :data:`_KINDS`), and the soft-obstacle field for
+    ``adjoint-channel`` (None otherwise)."""
+    soft = None
+    if kind == "sphere64":
+        return sphere_64(), None
+    if kind == "spheres288":
+        return spheres_288(seed), None
+    if kind == "spheres512":
+        return spheres_512(seed, scale), None
+    if domain is None:
+        raise ValueError(f"--domain is required for {kind}")
+    nx, ny, nz = (int(v) for v in domain)
+    if kind == "default":
+        s = default_scene(nx, ny, nz)
+    elif kind == "channel":
+        s = reference_channel(nx, ny, nz, u_in)
+    elif kind == "channel-cube":
+        s = reference_channel_cube(nx, ny, nz, u_in)
+    elif kind == "correctness":
+        s = correctness_case(nx, ny, nz, u_in, cube=(nx // 6, ny // 3, nz // 3, nx // 3, 2 * ny // 3, 2 * nz // 3))
+    elif kind == "spheres":
+        c, r = random_spheres(nx, ny, nz, spheres, radii[0], radii[1], seed)
+        s = sphere_channel(nx, ny, nz, u_in, c, r)
+    elif kind == "adjoint-channel":
+        s, soft = adjoint_channel(nx, ny, nz, u_peak=u_in, bumps=bumps, seed=seed)
+    else:
+        raise ValueError(f"unknown scene kind {kind!r}; one of {', '.join(_KINDS)}")
+    return s, soft
+
+
+def main(argv=None) -> int:
+    """Writes an init-state folder (flag.dat, rho.dat, vx.dat, vy.dat, vz.dat;
+    soft.dat for adjoint-channel) for single_dev_expt_main --initStateFolder."""
+    import argparse
+    import json
+    ap = argparse.ArgumentParser(prog="python -m culbm_b200.scenes", description=main.__doc__)
+    ap.add_argument("kind", choices=_KINDS)
+    ap.add_argument("out", help="output folder")
+    ap.add_argument("--domain", type=int, nargs=3, metavar=("NX", "NY", "NZ"))
+    ap.add_argument("--u-in", type=float, default=0.05, help="inlet velocity (peak for adjoint-channel)")
+    ap.add_argument("--spheres", type=int, default=40)
+    ap.add_argument("--radii", type=float, nargs=2, default=(4.0, 12.0))
+    ap.add_argument("--seed", type=int, default=12345)
+    ap.add_argument("--bumps", type=int, default=16)
+    ap.add_argument("--scale", type=float, default=1.0, help="spheres512 only")
+    args = ap.parse_args(argv)
+    s, soft = build_scene(args.kind, args.domain, args.u_in, args.spheres, tuple(args.radii), args.seed, args.bumps,
+                          args.scale)
+    write_folder(s, args.out)
+    if soft is not None:
+        np.ascontiguousarray(soft, dtype="<f4").tofile(os.path.join(args.out, "soft.dat"))
+    nz, ny, nx = s.flag.shape
+    print(json.dumps({"folder": args.out, "domainDim": [nx, ny, nz], "cells": int(s.flag.size),
+                      "solid_fraction": round(s.solid_fraction(), 5), **{k: v for k, v in s.meta.items()
+                                                                          if isinstance(v, (int, float, str))}}))
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

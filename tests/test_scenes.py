@@ -58,3 +58,20 @@ def test_soft_field_range():
     assert soft.shape == (16, 16, 32)
     assert soft.min() >= 0 and soft.max() <= 1 and soft.max() > 0.1
     assert (soft[s.flag != S.FLUID] == 0).all()
+
+
+def test_scene_cli_writes_a_folder_the_solver_reads(tmp_path):
+    from culbm_b200 import scenes as S
+    out = tmp_path / "case"
+    assert S.main(["spheres", str(out), "--domain", "48", "40", "36", "--spheres", "4", "--radii", "3", "5",
+                   "--seed", "9"]) == 0
+    got = S.read_folder(str(out), 48, 40, 36)
+    c, r = S.random_spheres(48, 40, 36, 4, 3.0, 5.0, 9)
+    ref = S.sphere_channel(48, 40, 36, 0.05, c, r)
+    for name in ("flag", "rho", "vx", "vy", "vz"):
+        assert np.array_equal(getattr(got, name), getattr(ref, name)), name
+    adj = tmp_path / "adj"
+    assert S.main(["adjoint-channel", str(adj), "--domain", "32", "16", "16", "--u-in", "0.04", "--seed", "7"]) == 0
+    soft = np.fromfile(adj / "soft.dat", dtype="<f4")
+    _, ref_soft = S.adjoint_channel(32, 16, 16, u_peak=0.04, bumps=16, seed=7)
+    assert np.array_equal(soft, ref_soft.reshape(-1).astype(np.float32))
