@@ -659,7 +659,7 @@ adj::Args<S, typename ArithOf<S>::type> base_args(culbm_adj* a)
 template <typename S, typename R>
 void set_pops(Pops<S>& p, S* base, long long n)
 {
-    for (int d = 0; d < 27; ++d) p.p[d] = base + d * n;
+    p.set(base, n);
 }
 
 // Forward steps t in [t_begin, t_end) from state `src`; states written to the

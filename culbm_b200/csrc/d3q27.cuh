@@ -75,17 +75,28 @@ template <> struct Rn<double> {
     static __device__ __forceinline__ double div(double a, double b) { return __ddiv_rn(a, b); }
 };
 
+// Exact power-of-two factors 2^E and 2^-E.
+template <typename R, int E>
+__host__ __device__ constexpr R pow2()
+{
+    R v = R(1);
+    for (int k = 0; k < (E > 0 ? E : -E); ++k) v = E > 0 ? v * R(2) : v / R(2);
+    return v;
+}
+
 // rho = 1 + sum f in the reference's pairing, u = (sum c f) * (1/rho).
 // Same operation order as bgk::detail::calcRhoU<27>,
 // reference src/lbm_core/device_function.hpp:439-463.
-template <typename R>
+// With E > 0, f holds raw values 2^E * f: every sum is the exact 2^E
+// multiple of the unscaled one, so rho and u come out with the same bits.
+template <typename R, int E = 0>
 __device__ __forceinline__ void moments(const R* f, R& rho, R& ux, R& uy, R& uz)
 {
     using A = Rn<R>;
-    R s = A::add(R(1), f[0]);
+    R s = A::add(pow2<R, E>(), f[0]);
 #pragma unroll
     for (int k = 1; k < 27; k += 2) s = A::add(s, A::add(f[k], f[k + 1]));
-    rho = s;
+    rho = E ? A::mul(s, pow2<R, -E>()) : s;
     const R inv = A::div(R(1), rho);
     // x: pairs (3k+2, 3k); y: (9s+6+j, 9s+j); z: (18+j, j).
     R x = A::sub(f[2], f[0]);
@@ -100,6 +111,11 @@ __device__ __forceinline__ void moments(const R* f, R& rho, R& ux, R& uy, R& uz)
     R z = A::sub(f[18], f[0]);
 #pragma unroll
     for (int k = 1; k < 9; ++k) z = A::add(z, A::sub(f[18 + k], f[k]));
+    if (E) {
+        x = A::mul(x, pow2<R, -E>());
+        y = A::mul(y, pow2<R, -E>());
+        z = A::mul(z, pow2<R, -E>());
+    }
     ux = A::mul(x, inv);
     uy = A::mul(y, inv);
     uz = A::mul(z, inv);
@@ -138,11 +154,13 @@ __host__ __device__ constexpr int equ_wcls(int d)
     return k;   // 0 centre, 1 face, 2 edge, 3 corner
 }
 
-template <typename R>
+// With E > 0 the weighted terms rw, rm carry the factor 2^E (exactly), so
+// every equilibrium built from them is the raw value 2^E * feq.
+template <typename R, int E = 0>
 __device__ __forceinline__ void equ_terms(R rho, R ux, R uy, R uz, EquTerms<R>& t)
 {
     using A = Rn<R>;
-    const R WS = R(2) / R(27), WE = R(1) / R(54), WC = R(1) / R(216);
+    const R WS = R(2) / R(27) * pow2<R, E>(), WE = R(1) / R(54) * pow2<R, E>(), WC = R(1) / R(216) * pow2<R, E>();
     const R rhom1 = A::sub(rho, R(1));
     t.c3 = A::mul(R(-3), A::add(A::add(A::mul(ux, ux), A::mul(uy, uy)), A::mul(uz, uz)));
     t.h = R(0.5);
@@ -160,11 +178,11 @@ __device__ __forceinline__ void equ_terms(R rho, R ux, R uy, R uz, EquTerms<R>& 
     t.v[10] = A::sub(A::add(vx, vy), vz);       // v7
     t.v[11] = A::add(A::sub(vx, vy), vz);       // v8
     t.v[12] = A::add(A::sub(vy, vx), vz);       // v9
-    t.rw[0] = rho;                              // centre uses rho directly
+    t.rw[0] = E ? A::mul(rho, pow2<R, E>()) : rho;   // centre uses rho directly
     t.rw[1] = A::mul(WS, rho);
     t.rw[2] = A::mul(WE, rho);
     t.rw[3] = A::mul(WC, rho);
-    t.rm[0] = rhom1;
+    t.rm[0] = E ? A::mul(rhom1, pow2<R, E>()) : rhom1;
     t.rm[1] = A::mul(WS, rhom1);
     t.rm[2] = A::mul(WE, rhom1);
     t.rm[3] = A::mul(WC, rhom1);
@@ -181,17 +199,18 @@ __device__ __forceinline__ R equ_dir(const EquTerms<R>& t, int d)
     return A::fma(t.rw[w], A::fma(t.h, A::fma(v, v, t.c3), sv), t.rm[w]);
 }
 
-// Shifted equilibrium into f, bgk::detail::calcEqu<27> (device_function.hpp:305-398).
-template <typename R>
+// Shifted equilibrium into f, bgk::detail::calcEqu<27> (device_function.hpp:305-398);
+// raw values 2^E * feq with E > 0.
+template <typename R, int E = 0>
 __device__ __forceinline__ void equilibrium(R rho, R ux, R uy, R uz, R* f)
 {
     using A = Rn<R>;
     EquTerms<R> t;
-    equ_terms(rho, ux, uy, uz, t);
+    equ_terms<R, E>(rho, ux, uy, uz, t);
 #pragma unroll
     for (int d = 0; d < 27; ++d) {
         if (d == 13)
-            f[d] = A::mul(R(8) / R(27), A::fma(rho, A::mul(t.h, t.c3), t.rm[0]));
+            f[d] = A::mul(R(8) / R(27), A::fma(t.rw[0], A::mul(t.h, t.c3), t.rm[0]));
         else
             f[d] = equ_dir(t, d);
     }
@@ -221,15 +240,16 @@ __device__ __forceinline__ R bgk_relax(const EquTerms<R>& t, R inv_tau, R om, in
 }
 
 // BGK relaxation on shifted populations, bgk::detail::collision2<27>
-// (device_function.hpp:676-754): f <- invTau*feq + (1-invTau)*f.
-template <typename R>
+// (device_function.hpp:676-754): f <- invTau*feq + (1-invTau)*f; on raw
+// values 2^E * f with E > 0 (same bits after unscaling).
+template <typename R, int E = 0>
 __device__ __forceinline__ void collide(R inv_tau, R* f)
 {
     using A = Rn<R>;
     R rho, ux, uy, uz;
-    moments(f, rho, ux, uy, uz);
+    moments<R, E>(f, rho, ux, uy, uz);
     EquTerms<R> t;
-    equ_terms(rho, ux, uy, uz, t);
+    equ_terms<R, E>(rho, ux, uy, uz, t);
     const R om = A::sub(R(1), inv_tau);
 #pragma unroll
     for (int d = 0; d < 27; ++d) f[d] = bgk_relax(t, inv_tau, om, d, f[d]);
@@ -238,13 +258,14 @@ __device__ __forceinline__ void collide(R inv_tau, R* f)
 // Boundary and collision sequence of one cell after its populations were
 // loaded: EQU overwrite, full-way bounce-back swap d <-> 26-d, BGK.
 // Reference src/simulator/single_dev_expt/kernel.cu:2571-2600.
-template <typename R>
+// With E > 0, f holds raw values 2^E * f in and out.
+template <typename R, int E = 0>
 __device__ __forceinline__ void cell_update(uint8_t op, R inv_tau, const float* __restrict__ rho,
                                             const float* __restrict__ vx, const float* __restrict__ vy,
                                             const float* __restrict__ vz, int64_t i, R* f)
 {
     if (op & OP_EQU) {
-        equilibrium<R>(R(rho[i]), R(vx[i]), R(vy[i]), R(vz[i]), f);
+        equilibrium<R, E>(R(rho[i]), R(vx[i]), R(vy[i]), R(vz[i]), f);
     }
     if (op & OP_BB) {
 #pragma unroll
@@ -255,7 +276,7 @@ __device__ __forceinline__ void cell_update(uint8_t op, R inv_tau, const float* 
         }
     }
     if (op & OP_COLLIDE) {
-        collide<R>(inv_tau, f);
+        collide<R, E>(inv_tau, f);
     }
 }
 

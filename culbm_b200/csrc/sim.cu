@@ -70,10 +70,8 @@ StepArgs<S, typename ArithOf<S>::type> make_args(const culbm_sim* s, int src, in
     a.inv_tau = static_cast<R>(s->cfg.inv_tau);
     S* b0 = static_cast<S*>(s->d_pop[src]);
     S* b1 = static_cast<S*>(s->d_pop[dst]);
-    for (int d = 0; d < 27; ++d) {
-        a.src.p[d] = b0 + static_cast<long long>(d) * stride;
-        a.dst.p[d] = b1 + static_cast<long long>(d) * stride;
-    }
+    a.src.set(b0, stride);
+    a.dst.set(b1, stride);
     a.edge = static_cast<S*>(s->d_edge);
     a.el = s->el;
     a.seed = step_seed(static_cast<uint32_t>(s->step));

@@ -188,6 +188,27 @@ __device__ __forceinline__ void put(S* p, R v, uint32_t hcell, int d)
         Cvt<S, R>::st(p, v);
 }
 
+// The power-of-two exponent E of a format's raw scale (raw = 2^E * f; 15 for
+// the scaled half formats, 0 otherwise).
+template <typename S> struct ScaleExp { static constexpr int value = 0; };
+template <> struct ScaleExp<__half> { static constexpr int value = 15; };
+template <> struct ScaleExp<Half16SR> { static constexpr int value = 15; };
+
+// put() of a raw value v = 2^E * f: the same bits as put(p, f, ...), without
+// the scaling multiply.
+template <typename S, typename R>
+__device__ __forceinline__ void put_raw(S* p, R v, uint32_t hcell, int d)
+{
+    if constexpr (std::is_same<S, __half>::value) {
+        *p = __float2half_rn(v);
+    } else if constexpr (std::is_same<S, Half16SR>::value) {
+        const uint32_t u = __float_as_uint(v) + (dir_bits(hcell, d) >> 19);
+        p->bits = __half_as_ushort(__float2half_rz(__uint_as_float(u)));
+    } else {
+        put(p, v, hcell, d);
+    }
+}
+
 template <typename S, typename R>
 __device__ __forceinline__ void put_cs(S* p, R v, uint32_t hcell, int d)
 {

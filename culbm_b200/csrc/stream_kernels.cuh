@@ -32,9 +32,15 @@ struct Domain {
     int n;     // nx*ny*nz (< 2^31, checked on the host)
 };
 
+// The 27 population planes of one buffer, one base pointer per direction
+// (kernel parameters, so no per-plane offset sits in a register).
 template <typename S>
 struct Pops {
     S* p[27];
+    __host__ void set(S* b, long long stride)
+    {
+        for (int d = 0; d < 27; ++d) p[d] = b + d * stride;
+    }
 };
 
 // Edge buffer: six face blocks (x-low, x-high, y-low, y-high, z-low, z-high),
@@ -149,7 +155,29 @@ __device__ __forceinline__ long long ring_index(const StepArgs<S, R>& a, int x, 
     return (long long)pz * a.dom.nxy + (long long)y * a.dom.nx + x;
 }
 
-template <int LAYOUT, typename S, typename R>
+// Load of a stored population: the value f, or with RAW its raw form
+// 2^E * f (ld_raw, E = ScaleExp<S>) for kernels that fold the scale into the
+// cell update.
+template <bool RAW, typename S, typename R>
+__device__ __forceinline__ R ld_as(const S* p)
+{
+    if constexpr (RAW)
+        return ld_raw<S, R>(p);
+    else
+        return Cvt<S, R>::ld(p);
+}
+
+// Store counterpart of ld_as.
+template <bool RAW, typename S, typename R>
+__device__ __forceinline__ void put_as(S* p, R v, uint32_t hcell, int d)
+{
+    if constexpr (RAW)
+        put_raw(p, v, hcell, d);
+    else
+        put(p, v, hcell, d);
+}
+
+template <int LAYOUT, bool RAW = false, typename S, typename R>
 __device__ __forceinline__ void load_pulled(const StepArgs<S, R>& a, int x, int y, int z, int i, bool edge, R* f)
 {
     const Domain& D = a.dom;
@@ -162,7 +190,7 @@ __device__ __forceinline__ void load_pulled(const StepArgs<S, R>& a, int x, int 
             const int ox = cx_of(d) == 1 ? ndx : cx_of(d) == -1 ? pdx : 0;
             const int oy = cy_of(d) == 1 ? ndy : cy_of(d) == -1 ? pdy : 0;
             const int oz = cz_of(d) == 1 ? ndz : cz_of(d) == -1 ? pdz : 0;
-            f[d] = Cvt<S, R>::ld(a.src.p[d] + (i + ox + oy + oz));
+            f[d] = ld_as<RAW, S, R>(a.src.p[d] + (i + ox + oy + oz));
         }
     } else if (LAYOUT == LAYOUT_PULL_RING) {
 #pragma unroll
@@ -171,24 +199,24 @@ __device__ __forceinline__ void load_pulled(const StepArgs<S, R>& a, int x, int 
             if ((unsigned)sx >= (unsigned)D.nx) sx = x;
             if ((unsigned)sy >= (unsigned)D.ny) sy = y;
             if ((unsigned)sz >= (unsigned)D.nz) sz = z;
-            f[d] = Cvt<S, R>::ld(a.src.p[d] + ring_index(a, sx, sy, sz));
+            f[d] = ld_as<RAW, S, R>(a.src.p[d] + ring_index(a, sx, sy, sz));
         }
     } else if (LAYOUT == LAYOUT_AA_A) {
         if (!edge) {
 #pragma unroll
-            for (int d = 0; d < 27; ++d) f[d] = Cvt<S, R>::ld(a.src.p[26 - d] + (i - nb_off(D, d)));
+            for (int d = 0; d < 27; ++d) f[d] = ld_as<RAW, S, R>(a.src.p[26 - d] + (i - nb_off(D, d)));
         } else {
 #pragma unroll
             for (int d = 0; d < 27; ++d) {
                 if (inside(D, x - cx_of(d), y - cy_of(d), z - cz_of(d)))
-                    f[d] = Cvt<S, R>::ld(a.src.p[26 - d] + (i - nb_off(D, d)));
+                    f[d] = ld_as<RAW, S, R>(a.src.p[26 - d] + (i - nb_off(D, d)));
                 else
-                    f[d] = Cvt<S, R>::ld(a.edge + edge_slot(D, a.el, x, y, z, d));
+                    f[d] = ld_as<RAW, S, R>(a.edge + edge_slot(D, a.el, x, y, z, d));
             }
         }
     } else {
 #pragma unroll
-        for (int d = 0; d < 27; ++d) f[d] = Cvt<S, R>::ld(a.src.p[d] + i);
+        for (int d = 0; d < 27; ++d) f[d] = ld_as<RAW, S, R>(a.src.p[d] + i);
     }
 }
 
@@ -218,15 +246,16 @@ __global__ void __launch_bounds__(256) k_pull_step(const __grid_constant__ StepA
     const uint8_t op = a.ops[c.i];
     R f[27];
     if (op & OP_LOAD) {
-        load_pulled<LAYOUT_PULL>(a, c.x, c.y, c.z, c.i, false, f);
+        load_pulled<LAYOUT_PULL, true>(a, c.x, c.y, c.z, c.i, false, f);
     } else {
 #pragma unroll
         for (int d = 0; d < 27; ++d) f[d] = R(0);
     }
-    cell_update<R>(op, a.inv_tau, a.rho, a.vx, a.vy, a.vz, c.i, f);
+    cell_update<R, ScaleExp<S>::value>(op, a.inv_tau, a.rho, a.vx, a.vy, a.vz, c.i, f);
     if (op & OP_STORE) {
 #pragma unroll
-        for (int d = 0; d < 27; ++d) put(a.dst.p[d] + c.i, f[d], cell_hash(static_cast<uint32_t>(c.i), a.seed), d);
+        for (int d = 0; d < 27; ++d)
+            put_raw(a.dst.p[d] + c.i, f[d], cell_hash(static_cast<uint32_t>(c.i), a.seed), d);
     }
 }
 
@@ -330,44 +359,44 @@ __device__ __forceinline__ void aa_odd_cell(const StepArgs<S, R>& a, int rb)
     if (op & OP_LOAD) {
         if (ROWS == ROWS_INNER && !xface) {
 #pragma unroll
-            for (int d = 0; d < 27; ++d) f[d] = Cvt<S, R>::ld(a.src.p[26 - d] + (c.i - nb_off(D, d)));
+            for (int d = 0; d < 27; ++d) f[d] = ld_raw<S, R>(a.src.p[26 - d] + (c.i - nb_off(D, d)));
         } else if (ROWS == ROWS_INNER) {
 #pragma unroll
             for (int d = 0; d < 27; ++d) {
                 const S* p = a.src.p[26 - d] + (c.i - nb_off(D, d));
                 if (cx_of(d) == 1 && c.x == 0) p = xface_edge_ptr(a.edge, D, a.el, 0, d, c.y, c.z);
                 if (cx_of(d) == -1 && c.x == D.nx - 1) p = xface_edge_ptr(a.edge, D, a.el, 1, d, c.y, c.z);
-                f[d] = Cvt<S, R>::ld(p);
+                f[d] = ld_raw<S, R>(p);
             }
         } else {
-            load_pulled<LAYOUT_AA_A>(a, c.x, c.y, c.z, c.i, true, f);
+            load_pulled<LAYOUT_AA_A, true>(a, c.x, c.y, c.z, c.i, true, f);
         }
     } else {
 #pragma unroll
         for (int d = 0; d < 27; ++d) f[d] = R(0);
     }
-    cell_update<R>(op, a.inv_tau, a.rho, a.vx, a.vy, a.vz, c.i, f);
+    cell_update<R, ScaleExp<S>::value>(op, a.inv_tau, a.rho, a.vx, a.vy, a.vz, c.i, f);
     if (!(op & OP_STORE)) return;
     if (ROWS == ROWS_INNER && !xface) {
 #pragma unroll
-        for (int d = 0; d < 27; ++d) put(a.dst.p[d] + (c.i + nb_off(D, d)), f[d], hc, d);
+        for (int d = 0; d < 27; ++d) put_raw(a.dst.p[d] + (c.i + nb_off(D, d)), f[d], hc, d);
     } else if (ROWS == ROWS_INNER) {
 #pragma unroll
         for (int d = 0; d < 27; ++d) {
             const int cx = cx_of(d);
             S* p = a.dst.p[d] + (c.i + nb_off(D, d));
             // streaming target x + c_d, unless it leaves the domain in x
-            if (cx == 0 || (cx == 1 && c.x < D.nx - 1) || (cx == -1 && c.x > 0)) put(p, f[d], hc, d);
+            if (cx == 0 || (cx == 1 && c.x < D.nx - 1) || (cx == -1 && c.x > 0)) put_raw(p, f[d], hc, d);
             // an x-face cell is the clamped source of the cell on its own face
-            if ((cx == 1 && c.x == 0) || (cx == -1 && c.x == D.nx - 1)) put(p - cx, f[d], hc, d);
+            if ((cx == 1 && c.x == 0) || (cx == -1 && c.x == D.nx - 1)) put_raw(p - cx, f[d], hc, d);
         }
     } else {
         for_dirs([&](auto dd) {
             constexpr int d = decltype(dd)::value;
             if (inside(D, c.x + cx_of(d), c.y + cy_of(d), c.z + cz_of(d)))
-                put(a.dst.p[d] + (c.i + nb_off(D, d)), f[d], hc, d);
+                put_raw(a.dst.p[d] + (c.i + nb_off(D, d)), f[d], hc, d);
             for_each_clamp_reader<d>(D, c.x, c.y, c.z, [&](int yx, int yy, int yz) {
-                put(a.dst.p[d] + (yx + D.nx * (yy + D.ny * yz)), f[d], hc, d);
+                put_raw(a.dst.p[d] + (yx + D.nx * (yy + D.ny * yz)), f[d], hc, d);
             });
         });
     }
@@ -387,30 +416,32 @@ __device__ __forceinline__ void aa_even_cell(const StepArgs<S, R>& a, int rb)
     const uint32_t hc = cell_hash(static_cast<uint32_t>(c.i), a.seed);
     R f[27];
     if (op & OP_LOAD) {
-        load_pulled<LAYOUT_AA_B>(a, c.x, c.y, c.z, c.i, false, f);
+        load_pulled<LAYOUT_AA_B, true>(a, c.x, c.y, c.z, c.i, false, f);
     } else {
 #pragma unroll
         for (int d = 0; d < 27; ++d) f[d] = R(0);
     }
-    cell_update<R>(op, a.inv_tau, a.rho, a.vx, a.vy, a.vz, c.i, f);
+    cell_update<R, ScaleExp<S>::value>(op, a.inv_tau, a.rho, a.vx, a.vy, a.vz, c.i, f);
     if (!(op & OP_STORE)) return;
 #pragma unroll
-    for (int d = 0; d < 27; ++d) put(a.dst.p[26 - d] + c.i, f[d], hc, d);
+    for (int d = 0; d < 27; ++d) put_raw(a.dst.p[26 - d] + c.i, f[d], hc, d);
     if (ROWS == ROWS_INNER) {
         if (c.x != 0 && c.x != D.nx - 1) return;
 #pragma unroll
         for (int d = 0; d < 27; ++d) {
             const int cx = cx_of(d);
             if (cx == 1 && c.x == 0)
-                put(const_cast<S*>(xface_edge_ptr(a.edge, D, a.el, 0, d, c.y + cy_of(d), c.z + cz_of(d))), f[d], hc, d);
+                put_raw(const_cast<S*>(xface_edge_ptr(a.edge, D, a.el, 0, d, c.y + cy_of(d), c.z + cz_of(d))), f[d], hc,
+                        d);
             if (cx == -1 && c.x == D.nx - 1)
-                put(const_cast<S*>(xface_edge_ptr(a.edge, D, a.el, 1, d, c.y + cy_of(d), c.z + cz_of(d))), f[d], hc, d);
+                put_raw(const_cast<S*>(xface_edge_ptr(a.edge, D, a.el, 1, d, c.y + cy_of(d), c.z + cz_of(d))), f[d], hc,
+                        d);
         }
     } else {
         for_dirs([&](auto dd) {
             constexpr int d = decltype(dd)::value;
             for_each_clamp_reader<d>(D, c.x, c.y, c.z, [&](int yx, int yy, int yz) {
-                put(a.edge + edge_slot(D, a.el, yx, yy, yz, d), f[d], hc, d);
+                put_raw(a.edge + edge_slot(D, a.el, yx, yy, yz, d), f[d], hc, d);
             });
         });
     }

@@ -101,10 +101,8 @@ struct TileLauncher {
         a.g.ring_nz = ts->ring_nz;
         a.g.ring_step = ts->ring_step;
         S* t = static_cast<S*>(ts->d_tile);
-        for (int d = 0; d < 27; ++d) {
-            a.t0.p[d] = t + d * ts->tile_n;
-            a.t1.p[d] = t + (27 + d) * ts->tile_n;
-        }
+        a.t0.set(t, ts->tile_n);
+        a.t1.set(t + 27 * ts->tile_n, ts->tile_n);
         a.edge = static_cast<S*>(s->d_edge);
         a.el = s->el;
         a.rs = ts->d_rs;
