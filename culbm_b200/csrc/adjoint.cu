@@ -486,43 +486,46 @@ __device__ __forceinline__ void adj_equ_cell(const Args<S, R>& a, int i, double&
     a.g_mac[3][i] += static_cast<double>(r_in * bz);
 }
 
-// Row blocks of one adjoint-step launch: the EQU cells (256 per block, the
-// longest per-thread work, first), then ROWS_OUTER and ROWS_INNER rows.
+// Grid of one adjoint-step launch: equ_z grid-z slices of blocks that take
+// the EQU cells, 256 per block (the longest per-thread work, scheduled
+// first), then the slices of split_grid (outer rows, then inner rows).
 struct AdjLayout {
-    int equ_blocks, outer_blocks;
+    int equ_z;
 };
 
 inline AdjLayout adj_layout(const Domain& D, int n_equ)
 {
-    const int gx = (D.nx + 31) / 32;
-    return {((n_equ + 255) / 256 + gx - 1) / gx, row_blocks(D, row_count(D, ROWS_OUTER))};
+    const long long per_slice = 1ll * ((D.nx + 31) / 32) * ((D.ny + 7) / 8);
+    const long long equ_blocks = (n_equ + 255) / 256;
+    return {static_cast<int>((equ_blocks + per_slice - 1) / per_slice)};
 }
 
 inline dim3 adj_grid(const Domain& D, int n_equ)
 {
-    const AdjLayout L = adj_layout(D, n_equ);
-    return row_grid(D, L.equ_blocks + L.outer_blocks + row_blocks(D, row_count(D, ROWS_INNER)));
+    const dim3 g = split_grid(D);
+    return dim3(g.x, g.y, g.z + adj_layout(D, n_equ).equ_z);
 }
 
-// One adjoint step over all cells (block-uniform roles, see AdjLayout); each
-// block adds its invTau gradient into its own slot of g_tau_block.
+// One adjoint step over all cells (block-uniform roles); each block adds its
+// invTau gradient into its own slot of g_tau_block.
 template <typename S, typename R>
 __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 3 : 1)
     k_adj_step(const __grid_constant__ Args<S, R> a, AdjLayout L)
 {
-    const int rb = row_block();
     double gtau_local = 0.0;
-    CellCoord c;
-    if (rb < L.equ_blocks) {
-        const int k = (blockIdx.x + gridDim.x * rb) * 256 + threadIdx.x + 32 * threadIdx.y;
+    if (static_cast<int>(blockIdx.z) < L.equ_z) {
+        const int blk = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+        const int k = blk * 256 + threadIdx.x + 32 * threadIdx.y;
         if (k < a.n_equ) adj_equ_cell(a, a.equ_cells[k], gtau_local);
-    } else if (rb < L.equ_blocks + L.outer_blocks) {
-        if (row_cell<ROWS_OUTER>(a.dom, c, rb - L.equ_blocks)) adj_cell<ROWS_OUTER>(a, c, gtau_local);
     } else {
-        if (row_cell<ROWS_INNER>(a.dom, c, rb - L.equ_blocks - L.outer_blocks))
+        CellCoord c;
+        const int kind = split_cell(a.dom, L.equ_z, c);
+        if (kind == ROWS_OUTER)
+            adj_cell<ROWS_OUTER>(a, c, gtau_local);
+        else if (kind == ROWS_INNER)
             adj_cell<ROWS_INNER>(a, c, gtau_local);
     }
-    block_accumulate(gtau_local, a.g_tau_block + (blockIdx.x + gridDim.x * rb));
+    block_accumulate(gtau_local, a.g_tau_block + (blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)));
 }
 
 template <typename S>
@@ -1072,6 +1075,8 @@ culbm_status culbm_adj_set_state(culbm_adj* a, const uint32_t* flag, const float
     }
     {
         const dim3 gr = adj::adj_grid(a->dom, n_equ);
+        if (gr.z > 65535)
+            return fail(CULBM_ERR_INVALID_ARGUMENT, "nz plus the EQU blocks of the adjoint step exceed grid z 65535");
         const long long slots = 1ll * gr.x * gr.y * gr.z;
         if (slots > a->tau_capacity) {
             CULBM_CUDA(cudaFree(a->d_gtau));

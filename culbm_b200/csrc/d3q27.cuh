@@ -15,6 +15,7 @@
 #pragma once
 
 #include <cstdint>
+#include <type_traits>
 #include <cuda_runtime.h>
 
 namespace culbm {
@@ -49,6 +50,16 @@ __host__ __device__ constexpr int cx_of(int d) { return d % 3 - 1; }
 __host__ __device__ constexpr int cy_of(int d) { return (d / 3) % 3 - 1; }
 __host__ __device__ constexpr int cz_of(int d) { return d / 9 - 1; }
 __host__ __device__ constexpr int opp_of(int d) { return 26 - d; }
+
+// Compile-time loop over the 27 directions: f(std::integral_constant<int, d>).
+template <int D_ = 0, class F>
+__device__ __forceinline__ void for_dirs(F&& f)
+{
+    if constexpr (D_ < 27) {
+        f(std::integral_constant<int, D_>{});
+        for_dirs<D_ + 1>(f);
+    }
+}
 
 // Lattice weights w_d (8/27 centre, 2/27 face, 1/54 edge, 1/216 corner).
 template <typename R>
@@ -278,6 +289,137 @@ __device__ __forceinline__ void cell_update(uint8_t op, R inv_tau, const float* 
     if (op & OP_COLLIDE) {
         collide<R, E>(inv_tau, f);
     }
+}
+
+// ---------------------------------------------------------------------------
+// Compact BGK update for 16-bit population storage.  The FP16/BF16 formats
+// store f with about 3 significant digits, so the FP32 cell arithmetic needs
+// no bitwise match with the reference's operation order; this form uses
+// fused multiply-adds and the pair symmetry c_{26-d} = -c_d to do the same
+// update in about 200 instead of 290 instructions.  Every operation is an
+// explicit round-to-nearest intrinsic in a fixed order, so the C oracle
+// (orc_cell_fast_f32) reproduces it bit for bit.  f holds raw values 2^E * f
+// in and out; the result equals 2^E times the E = 0 result exactly.
+//   dr = f_13 + sum_{d<13} (f_d + f_{26-d}),  rho = 1 + dr,
+//   j = sum_{d<13} c_d (f_d - f_{26-d}),
+//   w feq_d = A_k (P + 3 c_d.u) + C_k,  P = 9/2 (c_d.u)^2 - 3/2 |u|^2,
+//   A_k = w W_k 2^E rho, C_k = w W_k 2^E dr,  f_d <- (1 - w) f_d + w feq_d
+// (k the weight class of d; w = 1 gives the equilibrium itself).  Keeping
+// rho - 1 = dr apart, as the reference does, avoids cancelling the 1.
+
+// c_d . u in a fixed order: x, then y, then z; the first non-zero term is
+// taken as is (exact negation), the others added or subtracted.
+template <int D>
+__device__ __forceinline__ float cdot_fast(float ux, float uy, float uz)
+{
+    using A = Rn<float>;
+    constexpr int cx = cx_of(D), cy = cy_of(D), cz = cz_of(D);
+    float v = cx == 1 ? ux : cx == -1 ? -ux : 0.0f;
+    if constexpr (cy != 0) v = cx == 0 ? (cy == 1 ? uy : -uy) : (cy == 1 ? A::add(v, uy) : A::sub(v, uy));
+    if constexpr (cz != 0)
+        v = (cx == 0 && cy == 0) ? (cz == 1 ? uz : -uz) : (cz == 1 ? A::add(v, uz) : A::sub(v, uz));
+    return v;
+}
+
+// Weight-class constants A_k = w W_k 2^E rho and C_k = w W_k 2^E dr.
+template <int E>
+__device__ __forceinline__ void fast_class_terms(float w, float rho, float dr, float* Ak, float* Ck)
+{
+    using A = Rn<float>;
+    const float W[4] = {8.0f / 27.0f, 2.0f / 27.0f, 1.0f / 54.0f, 1.0f / 216.0f};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const float b = A::mul(A::mul(w, W[k]), pow2<float, E>());
+        Ak[k] = A::mul(b, rho);
+        Ck[k] = A::mul(b, dr);
+    }
+}
+
+// f_d <- om f_d + (A_k (P +- 3 c.u) + C_k) for every direction (om = 0 and
+// w = 1 give the equilibrium).
+template <bool RELAX>
+__device__ __forceinline__ void fast_relax(float om, float ux, float uy, float uz, const float* Ak, const float* Ck,
+                                          float* f)
+{
+    using A = Rn<float>;
+    const float uu = A::fma(ux, ux, A::fma(uy, uy, A::mul(uz, uz)));
+    const float base = A::mul(-1.5f, uu);
+    for_dirs([&](auto dd) {
+        constexpr int d = decltype(dd)::value;
+        if constexpr (d < 13) {
+            constexpr int e = 26 - d;
+            constexpr int k = (cx_of(d) != 0) + (cy_of(d) != 0) + (cz_of(d) != 0);
+            const float cu = cdot_fast<d>(ux, uy, uz);
+            const float P = A::fma(A::mul(4.5f, cu), cu, base);
+            const float ed = A::fma(Ak[k], A::fma(3.0f, cu, P), Ck[k]);
+            const float ee = A::fma(Ak[k], A::fma(-3.0f, cu, P), Ck[k]);
+            f[d] = RELAX ? A::fma(om, f[d], ed) : ed;
+            f[e] = RELAX ? A::fma(om, f[e], ee) : ee;
+        }
+    });
+    const float e13 = A::fma(Ak[0], base, Ck[0]);
+    f[13] = RELAX ? A::fma(om, f[13], e13) : e13;
+}
+
+template <int E>
+__device__ __forceinline__ void collide_fast(float w, float* f)
+{
+    using A = Rn<float>;
+    float r = f[13];
+    float jx = 0.0f, jy = 0.0f, jz = 0.0f;
+    bool hx = false, hy = false, hz = false;
+#pragma unroll
+    for (int d = 0; d < 13; ++d) {
+        const float sp = A::add(f[d], f[26 - d]);
+        const float tm = A::sub(f[d], f[26 - d]);
+        r = A::add(r, sp);
+        if (cx_of(d) != 0) {
+            jx = hx ? (cx_of(d) == 1 ? A::add(jx, tm) : A::sub(jx, tm)) : (cx_of(d) == 1 ? tm : -tm);
+            hx = true;
+        }
+        if (cy_of(d) != 0) {
+            jy = hy ? (cy_of(d) == 1 ? A::add(jy, tm) : A::sub(jy, tm)) : (cy_of(d) == 1 ? tm : -tm);
+            hy = true;
+        }
+        if (cz_of(d) != 0) {
+            jz = hz ? (cz_of(d) == 1 ? A::add(jz, tm) : A::sub(jz, tm)) : (cz_of(d) == 1 ? tm : -tm);
+            hz = true;
+        }
+    }
+    const float dr = A::mul(r, pow2<float, -E>());
+    const float rho = A::add(1.0f, dr);
+    const float inv = A::div(1.0f, rho);
+    const float ux = A::mul(A::mul(jx, pow2<float, -E>()), inv);
+    const float uy = A::mul(A::mul(jy, pow2<float, -E>()), inv);
+    const float uz = A::mul(A::mul(jz, pow2<float, -E>()), inv);
+    float Ak[4], Ck[4];
+    fast_class_terms<E>(w, rho, dr, Ak, Ck);
+    fast_relax<true>(A::sub(1.0f, w), ux, uy, uz, Ak, Ck, f);
+}
+
+template <int E>
+__device__ __forceinline__ void equilibrium_fast(float rho, float ux, float uy, float uz, float* f)
+{
+    float Ak[4], Ck[4];
+    fast_class_terms<E>(1.0f, rho, Rn<float>::sub(rho, 1.0f), Ak, Ck);
+    fast_relax<false>(0.0f, ux, uy, uz, Ak, Ck, f);
+}
+
+template <int E>
+__device__ __forceinline__ void cell_update_fast(uint8_t op, float inv_tau, const float* __restrict__ rho,
+                                                 const float* __restrict__ vx, const float* __restrict__ vy,
+                                                 const float* __restrict__ vz, int64_t i, float* f)
+{
+    if (op & OP_EQU) equilibrium_fast<E>(rho[i], vx[i], vy[i], vz[i], f);
+    if (op & OP_BB) {
+#pragma unroll
+        for (int d = 0; d < 13; ++d) {
+            const float tmp = f[d];
+            f[d] = f[26 - d];
+            f[26 - d] = tmp;
+        }
+    }
+    if (op & OP_COLLIDE) collide_fast<E>(inv_tau, f);
 }
 
 }  // namespace culbm

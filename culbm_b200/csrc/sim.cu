@@ -237,13 +237,11 @@ culbm_status plain_steps(culbm_sim* s, uint32_t nsteps)
         } else {
             auto a = make_args<S>(s, 0, 0);
             a.seed = seed;
-            const int ob = row_blocks(s->dom, row_count(s->dom, ROWS_OUTER));
-            const int ib = row_blocks(s->dom, row_count(s->dom, ROWS_INNER));
-            const dim3 gr = row_grid(s->dom, ob + ib);
+            const dim3 gs = split_grid(s->dom);
             if (s->aa_phase == 0)
-                k_aa_odd<S, R><<<gr, b, 0, s->stream>>>(a, ob);
+                k_aa_odd<S, R><<<gs, b, 0, s->stream>>>(a);
             else
-                k_aa_even<S, R><<<gr, b, 0, s->stream>>>(a, ob);
+                k_aa_even<S, R><<<gs, b, 0, s->stream>>>(a);
             CULBM_CUDA(cudaGetLastError());
             s->aa_phase ^= 1;
         }
@@ -270,6 +268,14 @@ culbm_status validate_config(const culbm_config& c)
     const unsigned long long n = 1ull * c.domain_dim[0] * c.domain_dim[1] * c.domain_dim[2];
     if (n >= (1ull << 31)) return fail(CULBM_ERR_INVALID_ARGUMENT, "domain has 2^31 cells or more");
     if (c.domain_dim[2] > 65535) return fail(CULBM_ERR_INVALID_ARGUMENT, "domainDim z above 65535");
+    if (c.stream_policy == CULBM_STREAM_INPLACE) {
+        Domain d{};
+        d.nx = static_cast<int>(c.domain_dim[0]);
+        d.ny = static_cast<int>(c.domain_dim[1]);
+        d.nz = static_cast<int>(c.domain_dim[2]);
+        if (split_grid(d).z > 65535)
+            return fail(CULBM_ERR_INVALID_ARGUMENT, "domainDim z too large for in-place streaming (grid z above 65535)");
+    }
     if (c.vel_set != 0) return fail(CULBM_ERR_INVALID_ARGUMENT, "Unsupport Velocity Set: " + std::to_string(c.vel_set));
     if (c.stream_policy != CULBM_STREAM_PULL && c.stream_policy != CULBM_STREAM_INPLACE)
         return fail(CULBM_ERR_INVALID_ARGUMENT, "streamPolicy must be 0 or 1");

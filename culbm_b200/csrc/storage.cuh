@@ -188,6 +188,9 @@ __device__ __forceinline__ void put(S* p, R v, uint32_t hcell, int d)
         Cvt<S, R>::st(p, v);
 }
 
+// The 16-bit population formats.
+template <typename S> struct Is16 { static constexpr bool value = sizeof(S) == 2; };
+
 // The power-of-two exponent E of a format's raw scale (raw = 2^E * f; 15 for
 // the scaled half formats, 0 otherwise).
 template <typename S> struct ScaleExp { static constexpr int value = 0; };

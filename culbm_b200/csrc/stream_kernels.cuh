@@ -124,16 +124,6 @@ __device__ __forceinline__ void for_each_clamp_reader(const Domain& D, int sx, i
     }
 }
 
-// Compile-time loop over the 27 directions: f(std::integral_constant<int, d>).
-template <int D_ = 0, class F>
-__device__ __forceinline__ void for_dirs(F&& f)
-{
-    if constexpr (D_ < 27) {
-        f(std::integral_constant<int, D_>{});
-        for_dirs<D_ + 1>(f);
-    }
-}
-
 // How the current state stores "the population f_d that cell x pulls next":
 //   LAYOUT_PULL  standard: post-collision f*_d(y) at [d][y]; pull from x - c_d,
 //                clamped per axis at the boundary (pull double buffer, tiles).
@@ -153,6 +143,22 @@ __device__ __forceinline__ long long ring_index(const StepArgs<S, R>& a, int x, 
     int pz = z + a.ring_off;
     if (pz >= a.ring_nz) pz -= a.ring_nz;
     return (long long)pz * a.dom.nxy + (long long)y * a.dom.nx + x;
+}
+
+// The cell update of storage format S on f (raw values 2^E f with RAW, E =
+// ScaleExp<S>): the compact form for the 16-bit formats (their stored
+// rounding dominates, see cell_update_fast), the reference's exact operation
+// order for FP32 and FP64.
+template <typename S, bool RAW, typename R>
+__device__ __forceinline__ void cell_update_for(uint8_t op, R inv_tau, const float* __restrict__ rho,
+                                                const float* __restrict__ vx, const float* __restrict__ vy,
+                                                const float* __restrict__ vz, int64_t i, R* f)
+{
+    constexpr int E = RAW ? ScaleExp<S>::value : 0;
+    if constexpr (Is16<S>::value)
+        cell_update_fast<E>(op, inv_tau, rho, vx, vy, vz, i, f);
+    else
+        cell_update<R, E>(op, inv_tau, rho, vx, vy, vz, i, f);
 }
 
 // Load of a stored population: the value f, or with RAW its raw form
@@ -251,7 +257,7 @@ __global__ void __launch_bounds__(256) k_pull_step(const __grid_constant__ StepA
 #pragma unroll
         for (int d = 0; d < 27; ++d) f[d] = R(0);
     }
-    cell_update<R, ScaleExp<S>::value>(op, a.inv_tau, a.rho, a.vx, a.vy, a.vz, c.i, f);
+    cell_update_for<S, true>(op, a.inv_tau, a.rho, a.vx, a.vy, a.vz, c.i, f);
     if (op & OP_STORE) {
 #pragma unroll
         for (int d = 0; d < 27; ++d)
@@ -267,72 +273,74 @@ __global__ void __launch_bounds__(256) k_pull_step(const __grid_constant__ StepA
 // for_each_clamp_reader) also writes f_d into slot d of each such y: nobody
 // else reads or writes that slot during the step, and y reads it next step.
 //
-// Each in-place step is one launch over two disjoint sets of x-rows, taken
-// block by block (cells of different rows never touch the same locations in
-// a step's pattern, so the order does not matter):
+// Each in-place step is one launch over two disjoint sets of x-rows (cells
+// of different rows never touch the same locations in a step's pattern, so
+// the order does not matter):
 //   ROWS_INNER: rows with 0 < y < ny-1 and 0 < z < nz-1.  Only the x-faces
 //     of such a row are on the boundary, and there only the x component of a
 //     pull can leave the domain, so the clamp handling reduces to pointer
 //     selects and predicated stores; the code stays straight-line.
 //   ROWS_OUTER: rows on a y or z face, processed with the general per-axis
 //     clamp code (about 2 (ny + nz) of the ny*nz rows).
-// The ROWS_OUTER blocks come first in the launch, so their longer code runs
-// beside the ROWS_INNER blocks instead of as a tail.  Rows are contiguous in
-// x, so warp accesses stay coalesced.
+// Grid (split_grid): 32 x 8 blocks, one warp per 32 cells of a row.  The
+// first grid-z slices hold the outer rows (the z = 0 and z = nz-1 planes,
+// then the y-face rows of the interior planes), so their longer code runs
+// beside the inner rows rather than as a tail; each further slice is one
+// interior z-plane of inner rows.  Rows are contiguous in x, so warp
+// accesses stay coalesced, and no thread divides by a runtime value.
 enum RowSet : int { ROWS_INNER = 0, ROWS_OUTER = 1 };
 
-// Row block of this thread block: grid y and z together (see row_grid).
-__device__ __forceinline__ int row_block() { return blockIdx.y + gridDim.y * blockIdx.z; }
+// Grid-z slices of the outer rows.
+__host__ __device__ __forceinline__ int outer_slices(const Domain& D)
+{
+    const int rows_per_slice = ((D.ny + 7) / 8) * 8;
+    const int nzf = D.nz > 1 ? 2 : 1, nyf = D.ny > 1 ? 2 : 1;
+    return nzf + (D.nz > 2 ? (nyf * (D.nz - 2) + rows_per_slice - 1) / rows_per_slice : 0);
+}
 
-// Cell of this thread in row block rb of a row set; false if it has none.
-template <int ROWS>
-__device__ __forceinline__ bool row_cell(const Domain& D, CellCoord& c, int rb)
+inline dim3 split_grid(const Domain& D)
+{
+    return dim3((D.nx + 31) / 32, (D.ny + 7) / 8, outer_slices(D) + (D.nz > 2 ? D.nz - 2 : 0));
+}
+
+// Cell of this thread in a split_grid launch whose grid-z slices start at
+// z0 (slices below z0 belong to another role); returns ROWS_OUTER or
+// ROWS_INNER, or -1 if the thread has no cell.
+__device__ __forceinline__ int split_cell(const Domain& D, int z0, CellCoord& c)
 {
     c.x = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c.x >= D.nx) return false;
-    const int r = rb * blockDim.y + threadIdx.y;
-    if (ROWS == ROWS_INNER) {
-        const int iy = D.ny - 2;
-        if (iy <= 0 || D.nz <= 2) return false;
-        c.y = 1 + r % iy;
-        c.z = 1 + r / iy;
-        if (c.z > D.nz - 2) return false;
-    } else {
-        // z = 0 plane, z = nz-1 plane (all y), then y = 0 and y = ny-1 for 0 < z < nz-1
-        const int nzf = (D.nz > 1 ? 2 : 1);
-        if (r < nzf * D.ny) {
-            c.y = r % D.ny;
-            c.z = (r / D.ny) ? D.nz - 1 : 0;
+    if (c.x >= D.nx) return -1;
+    const int bz = static_cast<int>(blockIdx.z) - z0;
+    const int yy = blockIdx.y * blockDim.y + threadIdx.y;
+    const int nzf = D.nz > 1 ? 2 : 1;
+    const int oz = outer_slices(D);
+    int kind;
+    if (bz < nzf) {
+        if (yy >= D.ny) return -1;
+        c.y = yy;
+        c.z = bz ? D.nz - 1 : 0;
+        kind = ROWS_OUTER;
+    } else if (bz < oz) {
+        const int q = (bz - nzf) * static_cast<int>(gridDim.y * blockDim.y) + yy;
+        if (D.ny > 1) {
+            if (q >= 2 * (D.nz - 2)) return -1;
+            c.z = 1 + (q >> 1);
+            c.y = (q & 1) ? D.ny - 1 : 0;
         } else {
-            const int q = r - nzf * D.ny;
-            const int nyf = (D.ny > 1 ? 2 : 1);
-            if (D.nz <= 2 || q >= nyf * (D.nz - 2)) return false;
-            c.z = 1 + q / nyf;
-            c.y = (q % nyf) ? D.ny - 1 : 0;
+            if (q >= D.nz - 2) return -1;
+            c.z = 1 + q;
+            c.y = 0;
         }
+        kind = ROWS_OUTER;
+    } else {
+        c.z = 1 + (bz - oz);
+        c.y = 1 + yy;
+        if (c.y > D.ny - 2) return -1;
+        kind = ROWS_INNER;
     }
     c.i = c.x + D.nx * (c.y + D.ny * c.z);
     c.valid = true;
-    return true;
-}
-
-// Number of rows in a row set (host side launch size).
-inline int row_count(const Domain& D, int rows)
-{
-    if (rows == ROWS_INNER) return (D.ny > 2 && D.nz > 2) ? (D.ny - 2) * (D.nz - 2) : 0;
-    const int nzf = D.nz > 1 ? 2 : 1, nyf = D.ny > 1 ? 2 : 1;
-    return nzf * D.ny + (D.nz > 2 ? nyf * (D.nz - 2) : 0);
-}
-
-// Row blocks (8 rows of (32, 8) thread blocks) of a row set.
-inline int row_blocks(const Domain& D, int rows) { return (rows + 7) / 8; }
-
-// Launch grid for `blocks` row blocks: spread over grid y and z so that any
-// ny * nz fits the 65535 limit of grid y.
-inline dim3 row_grid(const Domain& D, int blocks)
-{
-    const int gy = blocks < 32768 ? blocks : 32768;
-    return dim3((D.nx + 31) / 32, gy > 0 ? gy : 1, gy > 0 ? (blocks + gy - 1) / gy : 1);
+    return kind;
 }
 
 template <typename S>
@@ -344,11 +352,9 @@ __device__ __forceinline__ const S* xface_edge_ptr(const S* edge, const Domain& 
 }
 
 template <typename S, typename R, int ROWS>
-__device__ __forceinline__ void aa_odd_cell(const StepArgs<S, R>& a, int rb)
+__device__ __forceinline__ void aa_odd_cell(const StepArgs<S, R>& a, const CellCoord c)
 {
-    CellCoord c;
     const Domain& D = a.dom;
-    if (!row_cell<ROWS>(D, c, rb)) return;
     const uint8_t op = a.ops[c.i];
     const uint32_t hc = cell_hash(static_cast<uint32_t>(c.i), a.seed);
     // Warps without an x-face lane (all but the first and last of a row) take
@@ -375,7 +381,7 @@ __device__ __forceinline__ void aa_odd_cell(const StepArgs<S, R>& a, int rb)
 #pragma unroll
         for (int d = 0; d < 27; ++d) f[d] = R(0);
     }
-    cell_update<R, ScaleExp<S>::value>(op, a.inv_tau, a.rho, a.vx, a.vy, a.vz, c.i, f);
+    cell_update_for<S, true>(op, a.inv_tau, a.rho, a.vx, a.vy, a.vz, c.i, f);
     if (!(op & OP_STORE)) return;
     if (ROWS == ROWS_INNER && !xface) {
 #pragma unroll
@@ -407,11 +413,9 @@ __device__ __forceinline__ void aa_odd_cell(const StepArgs<S, R>& a, int rb)
 // the edge-buffer slot of (y, d): the next odd step's clamped pull of y reads
 // it there, because slot 26-d of the source is overwritten during that step.
 template <typename S, typename R, int ROWS>
-__device__ __forceinline__ void aa_even_cell(const StepArgs<S, R>& a, int rb)
+__device__ __forceinline__ void aa_even_cell(const StepArgs<S, R>& a, const CellCoord c)
 {
-    CellCoord c;
     const Domain& D = a.dom;
-    if (!row_cell<ROWS>(D, c, rb)) return;
     const uint8_t op = a.ops[c.i];
     const uint32_t hc = cell_hash(static_cast<uint32_t>(c.i), a.seed);
     R f[27];
@@ -421,7 +425,7 @@ __device__ __forceinline__ void aa_even_cell(const StepArgs<S, R>& a, int rb)
 #pragma unroll
         for (int d = 0; d < 27; ++d) f[d] = R(0);
     }
-    cell_update<R, ScaleExp<S>::value>(op, a.inv_tau, a.rho, a.vx, a.vy, a.vz, c.i, f);
+    cell_update_for<S, true>(op, a.inv_tau, a.rho, a.vx, a.vy, a.vz, c.i, f);
     if (!(op & OP_STORE)) return;
 #pragma unroll
     for (int d = 0; d < 27; ++d) put_raw(a.dst.p[26 - d] + c.i, f[d], hc, d);
@@ -447,26 +451,28 @@ __device__ __forceinline__ void aa_even_cell(const StepArgs<S, R>& a, int rb)
     }
 }
 
-// In-place steps over both row sets: row blocks below outer_blocks are
-// ROWS_OUTER rows, the rest ROWS_INNER (a block-uniform choice).
+// In-place steps over both row sets (split_grid; the row kind is uniform
+// over a block).
 template <typename S, typename R>
-__global__ void __launch_bounds__(256) k_aa_odd(const __grid_constant__ StepArgs<S, R> a, int outer_blocks)
+__global__ void __launch_bounds__(256) k_aa_odd(const __grid_constant__ StepArgs<S, R> a)
 {
-    const int rb = row_block();
-    if (rb < outer_blocks)
-        aa_odd_cell<S, R, ROWS_OUTER>(a, rb);
-    else
-        aa_odd_cell<S, R, ROWS_INNER>(a, rb - outer_blocks);
+    CellCoord c;
+    const int kind = split_cell(a.dom, 0, c);
+    if (kind == ROWS_OUTER)
+        aa_odd_cell<S, R, ROWS_OUTER>(a, c);
+    else if (kind == ROWS_INNER)
+        aa_odd_cell<S, R, ROWS_INNER>(a, c);
 }
 
 template <typename S, typename R>
-__global__ void __launch_bounds__(256) k_aa_even(const __grid_constant__ StepArgs<S, R> a, int outer_blocks)
+__global__ void __launch_bounds__(256) k_aa_even(const __grid_constant__ StepArgs<S, R> a)
 {
-    const int rb = row_block();
-    if (rb < outer_blocks)
-        aa_even_cell<S, R, ROWS_OUTER>(a, rb);
-    else
-        aa_even_cell<S, R, ROWS_INNER>(a, rb - outer_blocks);
+    CellCoord c;
+    const int kind = split_cell(a.dom, 0, c);
+    if (kind == ROWS_OUTER)
+        aa_even_cell<S, R, ROWS_OUTER>(a, c);
+    else if (kind == ROWS_INNER)
+        aa_even_cell<S, R, ROWS_INNER>(a, c);
 }
 
 // Moments of the pulled populations, written where the DUMP bits are set.

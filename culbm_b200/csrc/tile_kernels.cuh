@@ -224,7 +224,7 @@ __global__ void __launch_bounds__(256) k_tile_aa_first(const __grid_constant__ T
 #pragma unroll
         for (int d = 0; d < 27; ++d) f[d] = R(0);
     }
-    cell_update<R>(op, a.inv_tau, a.rho, a.vx, a.vy, a.vz, c.gi, f);
+    cell_update_for<S, false>(op, a.inv_tau, a.rho, a.vx, a.vy, a.vz, c.gi, f);
     if (!(op & OP_STORE)) return;
     if constexpr (ONE) {
         if (c.correct) tile_store_global<S, R, HINT>(a, c, round_dst_sel(a.rs, ring), a.rs->dst_offz, f);
@@ -251,7 +251,7 @@ __global__ void __launch_bounds__(256) k_tile_aa_odd(const __grid_constant__ Til
 #pragma unroll
         for (int d = 0; d < 27; ++d) f[d] = R(0);
     }
-    cell_update<R>(op, a.inv_tau, a.rho, a.vx, a.vy, a.vz, c.gi, f);
+    cell_update_for<S, false>(op, a.inv_tau, a.rho, a.vx, a.vy, a.vz, c.gi, f);
     if (!(op & OP_STORE)) return;
     const bool tile_inner = c.px > 0 && c.px < a.bx - 1 && c.py > 0 && c.py < a.by - 1 && c.pz > 0 && c.pz < a.bz - 1;
     if (!edge && tile_inner) {
@@ -290,7 +290,7 @@ __global__ void __launch_bounds__(256) k_tile_aa_even(const __grid_constant__ Ti
 #pragma unroll
         for (int d = 0; d < 27; ++d) f[d] = R(0);
     }
-    cell_update<R>(op, a.inv_tau, a.rho, a.vx, a.vy, a.vz, c.gi, f);
+    cell_update_for<S, false>(op, a.inv_tau, a.rho, a.vx, a.vy, a.vz, c.gi, f);
     if (!(op & OP_STORE)) return;
 #pragma unroll
     for (int d = 0; d < 27; ++d) put(a.t0.p[26 - d] + c.t, f[d], tile_hash(a, c.gi), d);
@@ -311,7 +311,7 @@ __global__ void __launch_bounds__(256) k_tile_aa_last(const __grid_constant__ Ti
 #pragma unroll
         for (int d = 0; d < 27; ++d) f[d] = R(0);
     }
-    cell_update<R>(op, a.inv_tau, a.rho, a.vx, a.vy, a.vz, c.gi, f);
+    cell_update_for<S, false>(op, a.inv_tau, a.rho, a.vx, a.vy, a.vz, c.gi, f);
     if (op & OP_STORE) tile_store_global<S, R, HINT>(a, c, round_dst_sel(a.rs, a.g.ring_nz), a.rs->dst_offz, f);
 }
 
@@ -357,7 +357,7 @@ __global__ void __launch_bounds__(256) k_tile_pull_first(const __grid_constant__
 #pragma unroll
         for (int d = 0; d < 27; ++d) f[d] = R(0);
     }
-    cell_update<R>(op, a.inv_tau, a.rho, a.vx, a.vy, a.vz, c.gi, f);
+    cell_update_for<S, false>(op, a.inv_tau, a.rho, a.vx, a.vy, a.vz, c.gi, f);
     if (!(op & OP_STORE)) return;
     if constexpr (ONE) {
         if (c.correct) tile_store_global<S, R, HINT>(a, c, round_dst_sel(a.rs, ring), a.rs->dst_offz, f);
@@ -381,7 +381,7 @@ __global__ void __launch_bounds__(256) k_tile_pull_mid(const __grid_constant__ T
 #pragma unroll
         for (int d = 0; d < 27; ++d) f[d] = R(0);
     }
-    cell_update<R>(op, a.inv_tau, a.rho, a.vx, a.vy, a.vz, c.gi, f);
+    cell_update_for<S, false>(op, a.inv_tau, a.rho, a.vx, a.vy, a.vz, c.gi, f);
     if (!(op & OP_STORE)) return;
 #pragma unroll
     for (int d = 0; d < 27; ++d) put(a.t1.p[d] + c.t, f[d], tile_hash(a, c.gi), d);
@@ -400,7 +400,7 @@ __global__ void __launch_bounds__(256) k_tile_pull_last(const __grid_constant__ 
 #pragma unroll
         for (int d = 0; d < 27; ++d) f[d] = R(0);
     }
-    cell_update<R>(op, a.inv_tau, a.rho, a.vx, a.vy, a.vz, c.gi, f);
+    cell_update_for<S, false>(op, a.inv_tau, a.rho, a.vx, a.vy, a.vz, c.gi, f);
     if (op & OP_STORE) tile_store_global<S, R, HINT>(a, c, round_dst_sel(a.rs, a.g.ring_nz), a.rs->dst_offz, f);
 }
 

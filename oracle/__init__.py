@@ -69,6 +69,7 @@ def lib():
         L.orc_step_s16.argtypes = [C.c_int, _i64, _i64, _i64, _u32p, _f32p, _f32p, _f32p, _f32p, C.c_float,
                                    u16p, u16p, C.c_uint32]
         L.orc_decode_s16.argtypes = [C.c_int, _i64, u16p, _f32p]
+        L.orc_cell_fast_f32.argtypes = [C.c_uint32, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float, _f32p]
         L.orc_encode_s16.argtypes = [C.c_int, _i64, _f32p, u16p, C.c_uint32]
         L.orc_step_seed.argtypes = [C.c_uint32]
         L.orc_step_seed.restype = C.c_uint32

@@ -157,6 +157,102 @@ static uint16_t s16_encode(int kind, float v, uint32_t cell, uint32_t d, uint32_
     }
 }
 
+/* ---- compact FP32 update used with 16-bit storage ------------------------
+ * The 16-bit formats keep about three significant digits, so culbm_b200 does
+ * the cell arithmetic of those formats in a shorter form (fused multiply-adds,
+ * pair symmetry c_{26-d} = -c_d) instead of the reference's operation order.
+ * This is that form, operation for operation (compiled without contraction,
+ * explicit fmaf):
+ *   dr = f_13 + sum_{d<13} (f_d + f_{26-d}),  rho = 1 + dr,
+ *   j = sum_{d<13} c_d (f_d - f_{26-d}),
+ *   w feq_d = A_k (P + 3 c_d.u) + C_k,  P = 9/2 (c_d.u)^2 - 3/2 |u|^2,
+ *   A_k = w W_k rho, C_k = w W_k dr,  f_d <- (1 - w) f_d + w feq_d. */
+static float cdot_fast(int d, float ux, float uy, float uz)
+{
+    const int cx = d % 3 - 1, cy = (d / 3) % 3 - 1, cz = d / 9 - 1;
+    float v = cx == 1 ? ux : cx == -1 ? -ux : 0.0f;
+    if (cy != 0) v = cx == 0 ? (cy == 1 ? uy : -uy) : (cy == 1 ? v + uy : v - uy);
+    if (cz != 0) v = (cx == 0 && cy == 0) ? (cz == 1 ? uz : -uz) : (cz == 1 ? v + uz : v - uz);
+    return v;
+}
+
+static void fast_class_terms(float w, float rho, float dr, float *Ak, float *Ck)
+{
+    const float W[4] = {8.0f / 27.0f, 2.0f / 27.0f, 1.0f / 54.0f, 1.0f / 216.0f};
+    for (int k = 0; k < 4; ++k) {
+        const float b = w * W[k];
+        Ak[k] = b * rho;
+        Ck[k] = b * dr;
+    }
+}
+
+static void fast_relax(int relax, float om, float ux, float uy, float uz, const float *Ak, const float *Ck, float *f)
+{
+    const float uu = fmaf(ux, ux, fmaf(uy, uy, uz * uz));
+    const float base = -1.5f * uu;
+    for (int d = 0; d < 13; ++d) {
+        const int e = 26 - d;
+        const int k = (d % 3 != 1) + ((d / 3) % 3 != 1) + (d / 9 != 1);
+        const float cu = cdot_fast(d, ux, uy, uz);
+        const float P = fmaf(4.5f * cu, cu, base);
+        const float ed = fmaf(Ak[k], fmaf(3.0f, cu, P), Ck[k]);
+        const float ee = fmaf(Ak[k], fmaf(-3.0f, cu, P), Ck[k]);
+        f[d] = relax ? fmaf(om, f[d], ed) : ed;
+        f[e] = relax ? fmaf(om, f[e], ee) : ee;
+    }
+    const float e13 = fmaf(Ak[0], base, Ck[0]);
+    f[13] = relax ? fmaf(om, f[13], e13) : e13;
+}
+
+void orc_cell_fast_f32(uint32_t flag, float w, float rho_in, float vx_in, float vy_in, float vz_in, float *f)
+{
+    float Ak[4], Ck[4];
+    if (flag & ORC_EQU) {
+        fast_class_terms(1.0f, rho_in, rho_in - 1.0f, Ak, Ck);
+        fast_relax(0, 0.0f, vx_in, vy_in, vz_in, Ak, Ck, f);
+    }
+    if (flag & ORC_BOUNCE_BACK)
+        for (int d = 0; d < 13; ++d) {
+            const float t = f[d];
+            f[d] = f[26 - d];
+            f[26 - d] = t;
+        }
+    if (!(flag & ORC_COLLIDE)) return;
+    float r = f[13], jx = 0.0f, jy = 0.0f, jz = 0.0f;
+    int hx = 0, hy = 0, hz = 0;
+    for (int d = 0; d < 13; ++d) {
+        const int cx = d % 3 - 1, cy = (d / 3) % 3 - 1, cz = d / 9 - 1;
+        const float sp = f[d] + f[26 - d], tm = f[d] - f[26 - d];
+        r = r + sp;
+        if (cx) { jx = hx ? (cx == 1 ? jx + tm : jx - tm) : (cx == 1 ? tm : -tm); hx = 1; }
+        if (cy) { jy = hy ? (cy == 1 ? jy + tm : jy - tm) : (cy == 1 ? tm : -tm); hy = 1; }
+        if (cz) { jz = hz ? (cz == 1 ? jz + tm : jz - tm) : (cz == 1 ? tm : -tm); hz = 1; }
+    }
+    const float dr = r, rho = 1.0f + dr, inv = 1.0f / rho;
+    const float ux = jx * inv, uy = jy * inv, uz = jz * inv;
+    fast_class_terms(w, rho, dr, Ak, Ck);
+    fast_relax(1, 1.0f - w, ux, uy, uz, Ak, Ck, f);
+}
+
+/* The FP32 pull step of orc_step_f32 with the compact cell update. */
+void orc_step_fast_f32(int64_t nx, int64_t ny, int64_t nz, const uint32_t *flag, const float *rho, const float *vx,
+                       const float *vy, const float *vz, float inv_tau, const float *src, float *dst)
+{
+    const int64_t n = nx * ny * nz;
+    for (int64_t z = 0; z < nz; ++z)
+        for (int64_t y = 0; y < ny; ++y)
+            for (int64_t x = 0; x < nx; ++x) {
+                const int64_t i = (ny * z + y) * nx + x;
+                const uint32_t fl = flag[i];
+                float f[27];
+                for (int d = 0; d < 27; ++d) f[d] = 0;
+                if (fl & ORC_LOAD) orc_pull_f32(nx, ny, nz, x, y, z, src, f);
+                orc_cell_fast_f32(fl, inv_tau, rho[i], vx[i], vy[i], vz[i], f);
+                if (fl & ORC_STORE)
+                    for (int d = 0; d < 27; ++d) dst[d * n + i] = f[d];
+            }
+}
+
 /* One step with 16-bit storage; `t` is the index of the step being taken
  * (0 for the first step after loading), which seeds stochastic rounding. */
 void orc_step_s16(int kind, int64_t nx, int64_t ny, int64_t nz, const uint32_t *flag,
@@ -170,7 +266,7 @@ void orc_step_s16(int kind, int64_t nx, int64_t ny, int64_t nz, const uint32_t *
         a[k] = s16_decode(kind, src[k]);
         b[k] = s16_decode(kind, dst[k]);
     }
-    orc_step_f32(nx, ny, nz, flag, rho, vx, vy, vz, inv_tau, a, b);
+    orc_step_fast_f32(nx, ny, nz, flag, rho, vx, vy, vz, inv_tau, a, b);
     const uint32_t seed = orc_step_seed(t);
     for (int64_t d = 0; d < 27; ++d)
         for (int64_t i = 0; i < n; ++i) {

@@ -100,3 +100,32 @@ def test_blocking_geometry_matches_reference(orc):
                     assert prev == [R.ref_valid_prev(k, blk, num, it, dom) for k in range(num + 1)]
                 assert prev[0] == 0 and prev[-1] == dom
                 assert all(b >= a for a, b in zip(prev, prev[1:]))
+
+
+def test_compact_update_of_16bit_formats_is_the_same_bgk(orc):
+    """The compact cell update used with 16-bit storage (oracle restatement of
+    cell_update_fast) and the reference-order update are the same BGK step up
+    to FP32 rounding.  Judged against the FP64 update, the compact form stays
+    within a few ulp of the largest population (the reference's order loses
+    more to cancellation on these random states)."""
+    L = orc.lib()
+    rng = np.random.default_rng(5)
+    worst = 0.0
+    for flag in (orc.LOAD | orc.COLLIDE | orc.STORE, orc.EQU | orc.COLLIDE | orc.STORE,
+                 orc.LOAD | orc.BOUNCE_BACK | orc.COLLIDE | orc.STORE, orc.EQU | orc.STORE):
+        for _ in range(200):
+            f0 = (0.02 * rng.standard_normal(27)).astype(np.float32)
+            w = np.float32(rng.uniform(0.3, 1.9))
+            r_in, ux, uy, uz = np.float32(1 + 0.02 * rng.standard_normal()), *(0.05 * rng.standard_normal(3)).astype(
+                np.float32)
+            fast, exact = f0.copy(), f0.copy()
+            exact64 = f0.astype(np.float64)
+            L.orc_cell_fast_f32(flag, w, r_in, ux, uy, uz, fast)
+            L.orc_cell_f32(flag, w, r_in, ux, uy, uz, exact)
+            L.orc_cell_f64(flag, float(w), float(r_in), float(ux), float(uy), float(uz), exact64)
+            scale = np.max(np.abs(exact64)) + 1e-30
+            e_fast = np.max(np.abs(fast - exact64)) / scale
+            e_exact = np.max(np.abs(exact - exact64)) / scale
+            assert e_fast < 1e-6 and e_exact < 1e-4, (flag, e_fast, e_exact)
+            worst = max(worst, e_fast)
+    assert worst > 0   # the two forms do differ in rounding
