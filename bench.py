@@ -163,7 +163,8 @@ def traffic_from_profiles(kernel_key):
         return None
     with open(p) as f:
         d = json.load(f)
-    return d.get(kernel_key)
+    entry = d.get(kernel_key)
+    return None if entry is None else entry["bytes"]
 
 
 # ------------------------------------------------------------------- ours ---
@@ -421,7 +422,9 @@ def run_ours(args):
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "peak_kind": f"{peak_kind} copy bandwidth",
                      "algorithmic_bytes_per_lup": BYTES_PER_LUP["fp32"],
-                     "traffic": traffic_from_profiles("inplace_fp32_per_step")},
+                     "traffic": traffic_from_profiles("inplace_fp32_per_step"),
+                     "traffic_unit": "DRAM bytes per launch (ncu, profiles/traffic.json)",
+                     "algorithmic_bytes_per_launch": BYTES_PER_LUP["fp32"] * sc.n},
         "e2e": {"value": round(e2e_mlups, 1), "unit": "MLUPS", "h2d_bytes_per_step": round(h2d / args.steps),
                 "d2h_bytes_per_step": round(d2h / args.steps),
                 "what": f"culbm_load_state from pinned host + {args.steps} steps + culbm_moments + "

@@ -37,6 +37,26 @@ def test_storage16_matches_oracle(culbm, orc, storage, policy):
     assert np.array_equal(bits(got), bits(want)), (storage, policy)
 
 
+@pytest.mark.parametrize("storage", ["fp16", "bf16", "fp16sr", "bf16sr"])
+@pytest.mark.parametrize("dims", [(150, 5, 4), (151, 4, 5), (7, 3, 3), (1, 4, 3), (2, 3, 3)])
+def test_storage16_pull_pairs_and_x_faces(culbm, orc, storage, dims):
+    """The two-cells-per-thread pull of the 16-bit formats: even nx (packed
+    stores) and odd nx (single stores), warps away from and at the x-faces
+    (nx > 128), pairs with a non-storing (solid) cell, single-cell rows."""
+    sc = S.reference_channel(*dims, 0.05)
+    sc.flag[0, :, :] = S.FLUID
+    rng = np.random.default_rng(sum(dims))
+    solid = rng.random(sc.flag.shape) < 0.08
+    sc.flag[solid] = 0
+    nsteps = 5
+    want = oracle_pulled16(orc, sc, storage, 0.7, nsteps)
+    with culbm.Simulation(sc.shape, stream_policy=0, inv_tau=0.7, storage=storage) as sim:
+        sim.load_state(*sc.arrays())
+        sim.step(nsteps)
+        got = sim.pulled_ddf()
+    assert np.array_equal(bits(got), bits(want)), (storage, dims)
+
+
 def test_stochastic_rounding_is_unbiased(culbm):
     """Mean of many stochastically rounded copies of one value tends to the
     value (nearest-even would sit on one side); checked through a state
