@@ -120,7 +120,7 @@ __device__ __forceinline__ void soft_update(uint8_t op, R inv_tau, R s, const fl
 }
 
 template <typename S, typename R>
-__global__ void __launch_bounds__(256) k_soft_step(const __grid_constant__ Args<S, R> a)
+__global__ void __launch_bounds__(256, sizeof(R) == 4 ? 5 : 1) k_soft_step(const __grid_constant__ Args<S, R> a)
 {
     const CellCoord c = cell_of_thread(a.dom);
     if (!c.valid) return;
@@ -734,8 +734,13 @@ culbm_status run_forward(culbm_adj* a, bool checkpoints)
     const int T = a->cfg.window[1], K = a->K;
     S* s0 = state_ptr<S>(a, CKPT, 0);
     CULBM_TRY(fill_rest<S>(a, s0));
+    // With one checkpoint level, the states of the last segment go straight to
+    // the segment slots where its reverse sweep reads them (no recompute).
+    const int tb_last = ((std::max(T, 1) - 1) / K) * K;
+    const bool keep_last = checkpoints && a->K2 == 0;
     auto slot_of = [&](int t) -> S* {
         if (checkpoints && t % K == 0) return state_ptr<S>(a, CKPT, t / K);
+        if (keep_last && t > tb_last) return state_ptr<S>(a, SEG, t - tb_last - 1);
         return state_ptr<S>(a, SEG, t & 1);
     };
     return forward_run<S>(a, 0, T, s0, slot_of, true);
@@ -743,10 +748,12 @@ culbm_status run_forward(culbm_adj* a, bool checkpoints)
 
 // Reverse sweep over the steps t in [tb, te) (te - tb <= nseg + 1) starting
 // from the state F^tb: recompute F^{tb+1} .. F^{te-1} into the segment
-// slots, then run the adjoint steps te-1 .. tb.
+// slots (unless they are already there), then run the adjoint steps
+// te-1 .. tb.
 template <typename S>
 culbm_status adjoint_segment(culbm_adj* a, int tb, int te, S* start, adj::Args<S, typename ArithOf<S>::type>& g,
-                             typename ArithOf<S>::type* const nu[2], int& cur, float& rec, float& adjms)
+                             typename ArithOf<S>::type* const nu[2], int& cur, float& rec, float& adjms,
+                             bool states_present = false)
 {
     using R = typename ArithOf<S>::type;
     const int t0 = a->cfg.window[0], t1 = a->cfg.window[1];
@@ -757,7 +764,7 @@ culbm_status adjoint_segment(culbm_adj* a, int tb, int te, S* start, adj::Args<S
     const adj::AdjLayout L = adj::adj_layout(a->dom, a->n_equ);
     const dim3 gr = adj::adj_grid(a->dom, a->n_equ);
     auto slot_of = [&](int t) -> S* { return state_ptr<S>(a, SEG, t - tb - 1); };
-    CULBM_TRY(forward_run<S>(a, tb, te - 1, start, slot_of, false));
+    if (!states_present) CULBM_TRY(forward_run<S>(a, tb, te - 1, start, slot_of, false));
     rec += elapsed(a);
     for (int t = te - 1; t >= tb; --t) {
         S* st = (t == tb) ? start : state_ptr<S>(a, SEG, t - tb - 1);
@@ -812,7 +819,9 @@ culbm_status run_gradient(culbm_adj* a)
         const int tb = k * K, te = std::min(T, (k + 1) * K);
         S* ck = state_ptr<S>(a, CKPT, k);
         if (K2 == 0) {
-            CULBM_TRY(adjoint_segment<S>(a, tb, te, ck, g, nu, cur, rec, adjms));
+            // the forward pass left the last segment's states in place
+            const bool last = k == (T - 1) / K;
+            CULBM_TRY(adjoint_segment<S>(a, tb, te, ck, g, nu, cur, rec, adjms, last));
             continue;
         }
         // two levels: one pass over the outer segment stores F^{tb + j K2},

@@ -245,7 +245,7 @@ __device__ __forceinline__ CellCoord cell_of_thread(const Domain& D)
 // One pull step src -> dst over the whole domain.
 // Replaces StaticD3Q27PullKernel, reference kernel.cu:2489-2632.
 template <typename S, typename R>
-__global__ void __launch_bounds__(256) k_pull_step(const __grid_constant__ StepArgs<S, R> a)
+__global__ void __launch_bounds__(256, sizeof(R) == 4 ? 5 : 1) k_pull_step(const __grid_constant__ StepArgs<S, R> a)
 {
     const CellCoord c = cell_of_thread(a.dom);
     if (!c.valid) return;
@@ -454,7 +454,7 @@ __device__ __forceinline__ void aa_even_cell(const StepArgs<S, R>& a, const Cell
 // In-place steps over both row sets (split_grid; the row kind is uniform
 // over a block).
 template <typename S, typename R>
-__global__ void __launch_bounds__(256) k_aa_odd(const __grid_constant__ StepArgs<S, R> a)
+__global__ void __launch_bounds__(256, sizeof(R) == 4 ? 5 : 1) k_aa_odd(const __grid_constant__ StepArgs<S, R> a)
 {
     CellCoord c;
     const int kind = split_cell(a.dom, 0, c);
@@ -465,7 +465,7 @@ __global__ void __launch_bounds__(256) k_aa_odd(const __grid_constant__ StepArgs
 }
 
 template <typename S, typename R>
-__global__ void __launch_bounds__(256) k_aa_even(const __grid_constant__ StepArgs<S, R> a)
+__global__ void __launch_bounds__(256, sizeof(R) == 4 ? 5 : 1) k_aa_even(const __grid_constant__ StepArgs<S, R> a)
 {
     CellCoord c;
     const int kind = split_cell(a.dom, 0, c);
