@@ -57,7 +57,7 @@ struct Args {
     uint32_t seed;
     double* rho_plane;   // forward: rho of the two measurement planes of the pulled state, this step
                          // (null outside the objective window); [2][ny*nz]
-    double* g_tau_block; // adjoint: one FP64 accumulator per thread block
+    double* g_tau_block; // adjoint: one FP64 accumulator per warp
     const int* equ_cells; // adjoint: the EQU cells, increasing
     int n_equ;
 };
@@ -242,23 +242,16 @@ __device__ __forceinline__ void feq_vjp(const R* l, R ux, R uy, R uz, R& a_rho, 
     bz = R(3) * Lz + R(9) * Lccz - R(3) * uz * L0;
 }
 
-// FP64 block sum of v into the block's own accumulator (no atomics: each
-// block owns its slot, so the result does not depend on scheduling).
-__device__ __forceinline__ void block_accumulate(double v, double* slot)
+// FP64 warp sum of v added to the warp's own accumulator slots[warp] (no
+// atomics and no block barrier: each warp owns its slot, so the result does
+// not depend on scheduling, and a warp leaves as soon as it is done).  All
+// 32 lanes must arrive.
+__device__ __forceinline__ void warp_accumulate(double v, double* slots)
 {
-    __shared__ double sh[8];
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xFFFFFFFFu, v, o);
-    const int lane = (threadIdx.x + blockDim.x * threadIdx.y) & 31;
-    const int warp = (threadIdx.x + blockDim.x * threadIdx.y) >> 5;
-    if (lane == 0) sh[warp] = v;
-    __syncthreads();
-    if (warp == 0) {
-        double w = lane < 8 ? sh[lane] : 0.0;
-#pragma unroll
-        for (int o = 4; o > 0; o >>= 1) w += __shfl_down_sync(0xFFFFFFFFu, w, o);
-        if (lane == 0) *slot += w;
-    }
+    const int t = threadIdx.x + blockDim.x * threadIdx.y;
+    if ((t & 31) == 0) slots[t >> 5] += v;
 }
 
 // Adjoint of the stored population d of cell c: the sum of nu_d over the
@@ -506,8 +499,8 @@ inline dim3 adj_grid(const Domain& D, int n_equ)
     return dim3(g.x, g.y, g.z + adj_layout(D, n_equ).equ_z);
 }
 
-// One adjoint step over all cells (block-uniform roles); each block adds its
-// invTau gradient into its own slot of g_tau_block.
+// One adjoint step over all cells (block-uniform roles); each warp adds its
+// invTau gradient into its own slot of g_tau_block (8 per block).
 template <typename S, typename R>
 __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 3 : 1)
     k_adj_step(const __grid_constant__ Args<S, R> a, AdjLayout L)
@@ -525,7 +518,7 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 3 : 1)
         else if (kind == ROWS_INNER)
             adj_cell<ROWS_INNER>(a, c, gtau_local);
     }
-    block_accumulate(gtau_local, a.g_tau_block + (blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)));
+    warp_accumulate(gtau_local, a.g_tau_block + 8ll * (blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)));
 }
 
 template <typename S>
@@ -566,7 +559,7 @@ struct culbm_adj {
     double* d_gmac = nullptr;   // 4 N
     double* d_psum = nullptr;   // 2 per time step of the window
     double* d_rho_plane = nullptr;  // window x 2 planes x ny*nz
-    long long n_tau_blocks = 0;     // blocks of one adjoint-step launch (one FP64 slot each)
+    long long n_tau_blocks = 0;     // warps of one adjoint-step launch (one FP64 slot each)
     long long tau_capacity = 0;
     int* d_equ = nullptr;           // EQU cells, increasing
     int n_equ = 0, equ_capacity = 0;
@@ -1086,7 +1079,7 @@ culbm_status culbm_adj_set_state(culbm_adj* a, const uint32_t* flag, const float
         const dim3 gr = adj::adj_grid(a->dom, n_equ);
         if (gr.z > 65535)
             return fail(CULBM_ERR_INVALID_ARGUMENT, "nz plus the EQU blocks of the adjoint step exceed grid z 65535");
-        const long long slots = 1ll * gr.x * gr.y * gr.z;
+        const long long slots = 8ll * gr.x * gr.y * gr.z;   // one per warp
         if (slots > a->tau_capacity) {
             CULBM_CUDA(cudaFree(a->d_gtau));
             a->d_gtau = nullptr;
