@@ -284,32 +284,49 @@ __device__ __forceinline__ R gather_lambda(const Args<S, R>& a, const CellCoord&
     }
 }
 
-// rho and u of f in plain arithmetic (the linearisation point of the adjoint;
-// the forward pass keeps the exactly rounded moments).
+// Shared-memory staging of the populations f1 (after the EQU overwrite,
+// before bounce-back) of the block's 256 cells: direction d of thread t at
+// fs[d * 256 + t], bank-conflict free.  Keeping f out of registers while the
+// 27 adjoint values are held lets four blocks of 256 share an SM.
 template <typename R>
-__device__ __forceinline__ void lin_moments(const R* f, R fscale, R& rho, R& ux, R& uy, R& uz)
-{
-    R r = f[0], x = f[2] - f[0], y = f[6] - f[0], z = f[18] - f[0];
-#pragma unroll
-    for (int d = 1; d < 27; ++d) r += f[d];
-#pragma unroll
-    for (int k = 1; k < 9; ++k) {
-        const int lo = 9 * (k / 3) + (k % 3);
-        x += f[3 * k + 2] - f[3 * k];
-        y += f[lo + 6] - f[lo];
-        z += f[18 + k] - f[k];
+struct FStage {
+    R* fs;
+    int t;
+    __device__ __forceinline__ R& operator[](int d) const { return fs[d * 256 + t]; }
+};
+
+// r = sum f1 and j = sum c f1 accumulated while staging, in direction order.
+template <typename R>
+struct MomentAcc {
+    R r = R(0), x = R(0), y = R(0), z = R(0);
+    template <int d>
+    __device__ __forceinline__ void add(R v)
+    {
+        r += v;
+        if constexpr (cx_of(d) == 1) x += v;
+        if constexpr (cx_of(d) == -1) x -= v;
+        if constexpr (cy_of(d) == 1) y += v;
+        if constexpr (cy_of(d) == -1) y -= v;
+        if constexpr (cz_of(d) == 1) z += v;
+        if constexpr (cz_of(d) == -1) z -= v;
     }
-    rho = R(1) + fscale * r;
-    R inv;
-    if constexpr (sizeof(R) == 4)
-        inv = __frcp_rn(rho);
-    else
-        inv = R(1) / rho;
-    inv *= fscale;
-    ux = x * inv;
-    uy = y * inv;
-    uz = z * inv;
-}
+    // rho and u of f2 = B(f1) if bb else f1 (bounce-back keeps rho and
+    // negates j), f = fscale * the staged values; plain arithmetic (the
+    // linearisation point of the adjoint).
+    __device__ __forceinline__ void finish(R fscale, bool bb, R& rho, R& ux, R& uy, R& uz) const
+    {
+        rho = R(1) + fscale * r;
+        R inv;
+        if constexpr (sizeof(R) == 4)
+            inv = __frcp_rn(rho);
+        else
+            inv = R(1) / rho;
+        inv *= bb ? -fscale : fscale;
+        ux = x * inv;
+        uy = y * inv;
+        uz = z * inv;
+    }
+};
 
 template <typename R>
 __device__ __forceinline__ void swap_pairs_if(bool c, R* v)
@@ -323,31 +340,30 @@ __device__ __forceinline__ void swap_pairs_if(bool c, R* v)
 }
 
 // Reverse of bounce-back and soft collision for one cell, linearised at
-// fscale * f (f: the populations after the EQU overwrite, before bounce-back,
-// possibly without their storage scale; plain arithmetic).  l enters as the
-// adjoint of the stored populations and leaves as the adjoint of f; gs and gw
-// are the cell's dJ/ds and dJ/dw (0 unless it collides).  The sums are
-// evaluated for every cell; bounce-back and the update of l are skipped by
-// (mostly warp-uniform) branches.  With P = <l, f2>, Q = <l, B(f2)>,
-// E = <l, feq(f2)>:
+// f2 = B(f1) if the cell bounces back, else f1, with f = fscale * the staged
+// values (possibly raw 16-bit values) and (rho, u) its moments; plain
+// arithmetic.  l enters as the adjoint of the stored populations and leaves
+// as the adjoint of f1; gs and gw are the cell's dJ/ds and dJ/dw (0 unless it
+// collides).  The sums are evaluated for every cell; the update of l is
+// skipped by a (mostly warp-uniform) branch.  With P = <l, f2>,
+// Q = <l, B(f2)>, E = <l, feq(f2)>:
 //     dJ/ds = <l, B(f2) - C(f2)> = (Q - P) - w (E - P),
 //     dJ/dw = (1 - s) <l, feq - f2> = (1 - s) (E - P),
 // and E = (rho - 1) a_rho + 3 Lcu + 9/2 Lcu2 - 3/2 |u|^2 L0 comes from the
 // same weighted sums as J_C^T, so no per-direction equilibrium is formed.
 template <typename R>
-__device__ __forceinline__ void reverse_cell(uint8_t op, R w, R s, R fscale, R* f, R* l, R& gs, R& gw)
+__device__ __forceinline__ void reverse_cell(uint8_t op, R w, R s, R fscale, const FStage<R>& f1, R rho, R ux, R uy,
+                                             R uz, R* l, R& gs, R& gw)
 {
     const bool bb = (op & OP_BB) != 0, col = (op & OP_COLLIDE) && (op & OP_STORE);
     const R om = R(1) - w;
-    if (bb) swap_pairs_if(true, f);
-    R rho, ux, uy, uz;
-    lin_moments(f, fscale, rho, ux, uy, uz);
     const R uu = ux * ux + uy * uy + uz * uz;
     R P = 0, QmP = 0, L0 = 0, Lx = 0, Ly = 0, Lz = 0, Lcu = 0, Lcu2 = 0, Lcx = 0, Lcy = 0, Lcz = 0;
 #pragma unroll
     for (int d = 0; d < 13; ++d) {
         const int e = 26 - d;
-        const R ld = l[d], le = l[e], fd = f[d], fe = f[e];
+        const R ld = l[d], le = l[e];
+        const R fd = f1[bb ? e : d], fe = f1[bb ? d : e];
         const R cx = R(cx_of(d)), cy = R(cy_of(d)), cz = R(cz_of(d)), wd = weight<R>(d);
         const R cu = cx * ux + cy * uy + cz * uz;
         P += ld * fd + le * fe;
@@ -364,7 +380,7 @@ __device__ __forceinline__ void reverse_cell(uint8_t op, R w, R s, R fscale, R* 
         Lcy += cy * cusp;
         Lcz += cz * cusp;
     }
-    P = fscale * (P + l[13] * f[13]);
+    P = fscale * (P + l[13] * f1[13]);
     QmP *= fscale;
     L0 += weight<R>(13) * l[13];
     const R a1 = R(3) * Lcu + R(4.5) * Lcu2 - R(1.5) * uu * L0;
@@ -397,41 +413,53 @@ __device__ __forceinline__ void reverse_cell(uint8_t op, R w, R s, R fscale, R* 
 }
 
 // Reverse of one cell update at step t for a cell without EQU (EQU cells
-// only get nu = dJ/df here; k_adj_equ does the rest of their work).  All
-// loads are issued before any decision on the op byte: the pull and the
-// gather stay inside the domain for every cell.
+// only get nu = dJ/df here; adj_equ_cell does the rest of their work).  The
+// pull and the gather stay inside the domain for every cell, so all loads
+// are issued without looking at the op byte; f1 goes to the block's stage.
 template <int ROWS, typename S, typename R>
-__device__ __forceinline__ void adj_cell(const Args<S, R>& a, const CellCoord c, double& gtau_local)
+__device__ __forceinline__ void adj_cell(const Args<S, R>& a, const CellCoord c, const FStage<R>& f1,
+                                         double& gtau_local)
 {
+    const Domain& D = a.dom;
     const uint8_t op = a.ops[c.i];
     const R s = R(a.soft[c.i]);
-    R f[27], l[27];
+    const bool load = (op & OP_LOAD) != 0, store = (op & OP_STORE) != 0, equ = (op & OP_EQU) != 0;
+    MomentAcc<R> m;
+    R l[27];
     // warps of inner rows without an x-face lane (a warp-uniform choice) pull
     // and gather without any clamp handling
     const int xw = c.x - (threadIdx.x & 31);
-    if (ROWS == ROWS_INNER && xw != 0 && xw + 31 < a.dom.nx - 1) {
-#pragma unroll
-        for (int d = 0; d < 27; ++d) {
-            f[d] = ld_raw<S, R>(a.src.p[d] + (c.i - nb_off(a.dom, d)));
-            l[d] = a.nu_in[d][c.i + nb_off(a.dom, d)];
-        }
-    } else {
-        pull_state<ROWS, true>(a, c.x, c.y, c.z, c.i, f);
+    if (ROWS == ROWS_INNER && xw != 0 && xw + 31 < D.nx - 1) {
         for_dirs([&](auto dd) {
             constexpr int d = decltype(dd)::value;
+            const R v = ld_raw<S, R>(a.src.p[d] + (c.i - nb_off(D, d)));
+            f1[d] = load ? v : R(0);
+            m.template add<d>(load ? v : R(0));
+            l[d] = a.nu_in[d][c.i + nb_off(D, d)];
+        });
+    } else {
+        constexpr bool inner = ROWS == ROWS_INNER;
+        const int ndx = (c.x == 0) ? 0 : -1, pdx = (c.x == D.nx - 1) ? 0 : 1;
+        const int ndy = (!inner && c.y == 0) ? 0 : -D.nx, pdy = (!inner && c.y == D.ny - 1) ? 0 : D.nx;
+        const int ndz = (!inner && c.z == 0) ? 0 : -D.nxy, pdz = (!inner && c.z == D.nz - 1) ? 0 : D.nxy;
+        for_dirs([&](auto dd) {
+            constexpr int d = decltype(dd)::value;
+            const int ox = cx_of(d) == 1 ? ndx : cx_of(d) == -1 ? pdx : 0;
+            const int oy = cy_of(d) == 1 ? ndy : cy_of(d) == -1 ? pdy : 0;
+            const int oz = cz_of(d) == 1 ? ndz : cz_of(d) == -1 ? pdz : 0;
+            const R v = ld_raw<S, R>(a.src.p[d] + (c.i + ox + oy + oz));
+            f1[d] = load ? v : R(0);
+            m.template add<d>(load ? v : R(0));
             l[d] = gather_lambda<d, ROWS>(a, c);
         });
     }
-    const bool load = (op & OP_LOAD) != 0, store = (op & OP_STORE) != 0, equ = (op & OP_EQU) != 0;
-    if (!load || !store) {
+    if (!store)
 #pragma unroll
-        for (int d = 0; d < 27; ++d) {
-            f[d] = load ? f[d] : R(0);
-            l[d] = store ? l[d] : R(0);
-        }
-    }
-    R gs, gw;
-    reverse_cell(op, a.inv_tau, s, R(RawScale<S>::value), f, l, gs, gw);
+        for (int d = 0; d < 27; ++d) l[d] = R(0);
+    constexpr R fscale = R(RawScale<S>::value);
+    R rho, ux, uy, uz, gs, gw;
+    m.finish(fscale, (op & OP_BB) != 0, rho, ux, uy, uz);
+    reverse_cell(op, a.inv_tau, s, fscale, f1, rho, ux, uy, uz, l, gs, gw);
     if (!equ && (op & OP_COLLIDE) && store) {
         a.g_soft[c.i] += static_cast<double>(gs);
         gtau_local = static_cast<double>(gw);
@@ -447,7 +475,7 @@ __device__ __forceinline__ void adj_cell(const Args<S, R>& a, const CellCoord c,
 // dJ/d(rho_in, u_in) from d feq / d(rho, u).  Its nu (no pull, so dJ/df
 // only) is written by adj_cell.
 template <typename S, typename R>
-__device__ __forceinline__ void adj_equ_cell(const Args<S, R>& a, int i, double& gtau_local)
+__device__ __forceinline__ void adj_equ_cell(const Args<S, R>& a, int i, const FStage<R>& f1, double& gtau_local)
 {
     const Domain& D = a.dom;
     CellCoord c;
@@ -458,15 +486,25 @@ __device__ __forceinline__ void adj_equ_cell(const Args<S, R>& a, int i, double&
     c.valid = true;
     const uint8_t op = a.ops[i];
     const R r_in = R(a.rho[i]), vx = R(a.vx[i]), vy = R(a.vy[i]), vz = R(a.vz[i]);
-    R f[27], l[27];
-    equilibrium<R>(r_in, vx, vy, vz, f);
+    MomentAcc<R> m;
+    {
+        R f[27];
+        equilibrium<R>(r_in, vx, vy, vz, f);
+        for_dirs([&](auto dd) {
+            constexpr int d = decltype(dd)::value;
+            f1[d] = f[d];
+            m.template add<d>(f[d]);
+        });
+    }
+    R l[27];
     const bool store = (op & OP_STORE) != 0;
     for_dirs([&](auto dd) {
         constexpr int d = decltype(dd)::value;
         l[d] = store ? gather_lambda<d, ROWS_OUTER>(a, c) : R(0);
     });
-    R gs, gw;
-    reverse_cell(op, a.inv_tau, R(a.soft[i]), R(1), f, l, gs, gw);
+    R rho, ux, uy, uz, gs, gw;
+    m.finish(R(1), (op & OP_BB) != 0, rho, ux, uy, uz);
+    reverse_cell(op, a.inv_tau, R(a.soft[i]), R(1), f1, rho, ux, uy, uz, l, gs, gw);
     if ((op & OP_COLLIDE) && store) {
         a.g_soft[i] += static_cast<double>(gs);
         gtau_local = static_cast<double>(gw);
@@ -501,22 +539,25 @@ inline dim3 adj_grid(const Domain& D, int n_equ)
 
 // One adjoint step over all cells (block-uniform roles); each warp adds its
 // invTau gradient into its own slot of g_tau_block (8 per block).
+// Dynamic shared memory: the f1 stage, 27 * 256 values of R.
 template <typename S, typename R>
-__global__ void __launch_bounds__(256, sizeof(R) == 4 ? 3 : 1)
+__global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 1)
     k_adj_step(const __grid_constant__ Args<S, R> a, AdjLayout L)
 {
+    extern __shared__ __align__(16) unsigned char adj_stage[];
+    const FStage<R> f1{reinterpret_cast<R*>(adj_stage), static_cast<int>(threadIdx.x + 32 * threadIdx.y)};
     double gtau_local = 0.0;
     if (static_cast<int>(blockIdx.z) < L.equ_z) {
         const int blk = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
         const int k = blk * 256 + threadIdx.x + 32 * threadIdx.y;
-        if (k < a.n_equ) adj_equ_cell(a, a.equ_cells[k], gtau_local);
+        if (k < a.n_equ) adj_equ_cell(a, a.equ_cells[k], f1, gtau_local);
     } else {
         CellCoord c;
         const int kind = split_cell(a.dom, L.equ_z, c);
         if (kind == ROWS_OUTER)
-            adj_cell<ROWS_OUTER>(a, c, gtau_local);
+            adj_cell<ROWS_OUTER>(a, c, f1, gtau_local);
         else if (kind == ROWS_INNER)
-            adj_cell<ROWS_INNER>(a, c, gtau_local);
+            adj_cell<ROWS_INNER>(a, c, f1, gtau_local);
     }
     warp_accumulate(gtau_local, a.g_tau_block + 8ll * (blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)));
 }
@@ -769,7 +810,7 @@ culbm_status adjoint_segment(culbm_adj* a, int tb, int te, S* start, adj::Args<S
         const bool in_win = t >= t0 && t <= t1;
         g.obj_in = in_win ? obj_in : R(0);
         g.obj_out = in_win ? obj_out : R(0);
-        adj::k_adj_step<S, R><<<gr, block, 0, a->stream>>>(g, L);
+        adj::k_adj_step<S, R><<<gr, block, 27 * 256 * sizeof(R), a->stream>>>(g, L);
         CULBM_CUDA(cudaGetLastError());
         cur = 1 - cur;
     }
@@ -794,6 +835,8 @@ culbm_status run_gradient(culbm_adj* a)
     CULBM_CUDA(cudaMemsetAsync(a->d_gtau, 0, a->n_tau_blocks * sizeof(double), a->stream));
     CULBM_CUDA(cudaMemsetAsync(a->d_gmac, 0, 4 * a->n * sizeof(double), a->stream));
     R* const nu[2] = {static_cast<R*>(a->d_nu), static_cast<R*>(a->d_nu) + 27 * a->n};
+    CULBM_CUDA(cudaFuncSetAttribute(adj::k_adj_step<S, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(27 * 256 * sizeof(R))));
     auto g = base_args<S>(a);
     g.g_tau_block = a->d_gtau;
     g.equ_cells = a->d_equ;
