@@ -32,7 +32,8 @@ FIELD = {"rho": 0, "vx": 1, "vy": 2, "vz": 3}
 EXPORTED = (
     "culbm_config_init", "culbm_create", "culbm_destroy", "culbm_load_state", "culbm_load_state_folder",
     "culbm_step", "culbm_step_timed", "culbm_synchronize", "culbm_moments", "culbm_get_field", "culbm_dump",
-    "culbm_get_step", "culbm_get_pulled_ddf", "culbm_set_ddf", "culbm_mass_momentum", "culbm_mass_momentum_noalloc", "culbm_get_info",
+    "culbm_get_step", "culbm_get_pulled_ddf", "culbm_set_ddf", "culbm_mass_momentum", "culbm_mass_momentum_noalloc", "culbm_measure_memory",
+    "culbm_select_tile", "culbm_blocking_speedup", "culbm_get_info",
     "culbm_last_error", "culbm_status_string", "culbm_abi_version", "culbm_debug_inject_cuda_error",
     "culbm_adj_config_init", "culbm_adj_create", "culbm_adj_destroy", "culbm_adj_set_state",
     "culbm_adj_set_inv_tau", "culbm_adj_forward", "culbm_adj_gradient", "culbm_adj_get_info",
@@ -107,6 +108,29 @@ class AdjInfo(C.Structure):
     ]
 
 
+class MemoryConstants(C.Structure):
+    _fields_ = [
+        ("dram_gbs", C.c_double),
+        ("l2_gbs", C.c_double),
+        ("lambda_", C.c_double),
+        ("full_store_ms", C.c_double),
+        ("partial_store_ms", C.c_double),
+        ("gamma", C.c_double),
+        ("l2_bytes", C.c_uint64),
+        ("reserved", C.c_uint32 * 8),
+    ]
+
+
+class TileChoice(C.Structure):
+    _fields_ = [
+        ("tile", C.c_uint32 * 3),
+        ("inner_loop", C.c_int32),
+        ("predicted_speedup", C.c_double),
+        ("predicted_speedup_no_alignment", C.c_double),
+        ("reserved", C.c_uint32 * 8),
+    ]
+
+
 class CulbmError(RuntimeError):
     def __init__(self, status: int, message: str):
         self.status = status
@@ -142,6 +166,11 @@ def lib():
     L.culbm_set_ddf.argtypes = [vp, vp, C.c_int32]
     L.culbm_mass_momentum.argtypes = [vp, C.POINTER(C.c_double)]
     L.culbm_mass_momentum_noalloc.argtypes = [vp, C.c_uint64, vp, C.POINTER(C.c_double)]
+    L.culbm_measure_memory.argtypes = [C.c_int32, C.POINTER(MemoryConstants)]
+    L.culbm_select_tile.argtypes = [C.POINTER(C.c_uint32), C.c_int32, C.c_double, C.c_double, C.c_uint64,
+                                    C.c_uint64, C.POINTER(TileChoice)]
+    L.culbm_blocking_speedup.argtypes = [C.POINTER(C.c_uint32), C.c_int32, C.c_int32, C.c_double, C.c_double,
+                                         C.c_uint64, C.POINTER(C.c_double), C.POINTER(C.c_double)]
     L.culbm_get_info.argtypes = [vp, C.POINTER(Info)]
     L.culbm_last_error.restype = C.c_char_p
     L.culbm_status_string.restype = C.c_char_p

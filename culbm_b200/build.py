@@ -27,7 +27,7 @@ CLI = os.path.join(BIN_DIR, "single_dev_expt_main")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
               "--expt-relaxed-constexpr"]
-LIB_SOURCES = ["sim.cu", "tile_runtime.cu", "adjoint.cu", "noalloc.cu"]
+LIB_SOURCES = ["sim.cu", "tile_runtime.cu", "adjoint.cu", "noalloc.cu", "selector.cu"]
 
 
 def _nvcc() -> str:

@@ -43,6 +43,7 @@ struct Options {
     std::string dump_folder = "data/left_inlet_right_outlet_256_256_256_output";
     bool dump[4] = {false, false, false, false};
     bool help = false;
+    bool auto_block = false;   // --blockDim auto
 };
 
 void usage(std::ostream& os)
@@ -55,7 +56,9 @@ void usage(std::ostream& os)
           "  --dstep UINT [100]        Delta time steps of the simulation.\n"
           "  --nstep UINT [1000]       Total time steps of the simulation.\n"
           "  --invTau FLOAT [0.5]      Reciprocal of Tau.\n"
-          "  --blockDim UINT x 3 [[32,16,2]]   Dimension of blocks per grid.\n"
+          "  --blockDim UINT x 3 [[32,16,2]]   Dimension of blocks per grid; `auto`: the whole domain\n"
+          "                            without blocking, else the tile and innerLoop of the largest\n"
+          "                            modelled speed-up (culbm_select_tile).\n"
           "  --gridDim UINT x 3 [[2,3,19]]     Dimension of grids per kernel.\n"
           "  --domainDim UINT x 3 [[256,256,256]] Dimension of the domain.\n"
           "  --streamPolicy INT [0]    {[0]:PULL_STREAM, [1]:INPLACE_STREAM}.\n"
@@ -157,7 +160,13 @@ Options parse(int argc, char** argv)
         } else if (name == "--invTau") {
             o.cfg.inv_tau = parse_float(name, value());
         } else if (name == "--blockDim") {
-            parse_vec3(name, args, k, has_inline ? &val : nullptr, o.cfg.block_dim);
+            const std::string next = has_inline ? val : (k + 1 < args.size() ? args[k + 1] : std::string());
+            if (next == "auto") {
+                if (!has_inline) ++k;
+                o.auto_block = true;
+            } else {
+                parse_vec3(name, args, k, has_inline ? &val : nullptr, o.cfg.block_dim);
+            }
         } else if (name == "--gridDim") {
             parse_vec3(name, args, k, has_inline ? &val : nullptr, o.cfg.grid_dim);
         } else if (name == "--domainDim") {
@@ -226,8 +235,27 @@ std::string fmt_default(float v)
     return buf;
 }
 
-int run(const Options& o)
+int run(Options o)
 {
+    if (o.auto_block) {
+        if (o.cfg.opt_policy == CULBM_OPT_NONE) {
+            for (int k = 0; k < 3; ++k) {
+                o.cfg.block_dim[k] = o.cfg.domain_dim[k];
+                o.cfg.grid_dim[k] = 1;
+            }
+        } else {
+            culbm_tile_choice t;
+            check(culbm_select_tile(o.cfg.domain_dim, o.cfg.storage, 0.0, 0.0, 0, 0, &t));
+            for (int k = 0; k < 3; ++k) {
+                o.cfg.block_dim[k] = t.tile[k];
+                o.cfg.grid_dim[k] = 1;
+            }
+            o.cfg.inner_loop = t.inner_loop;
+            std::cout << "Auto tile: blockDim [" << t.tile[0] << "," << t.tile[1] << "," << t.tile[2]
+                      << "] gridDim [1,1,1] innerLoop " << t.inner_loop << " (modelled speed-up "
+                      << t.predicted_speedup << " over plain streaming)" << std::endl;
+        }
+    }
     if (o.dstep == 0) throw std::invalid_argument("--dstep must be positive");
     culbm_sim* sim = nullptr;
     check(culbm_create(&o.cfg, &sim));

@@ -19,8 +19,6 @@
 
 namespace culbm {
 
-namespace {
-
 // Blocking geometry, restating blocking_core::validBlkAxisConfig,
 // calcBlkNum and calcValidPrev (src/blocking_core/blocking_alogrithm.hpp:7-41)
 // with the unsigned arithmetic the reference instantiates them with.
@@ -45,6 +43,8 @@ int32_t valid_prev(int32_t idx, int32_t blk, int32_t num, int32_t it, int32_t do
     if (idx == 0) return 0;
     return (blk + 1 - it) + (idx - 1) * (blk + 2 - 2 * it);
 }
+
+namespace {
 
 struct TileGeom {
     int org[3];

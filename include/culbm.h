@@ -218,6 +218,54 @@ culbm_status culbm_mass_momentum(culbm_sim* sim, double out[4]);
 #define CULBM_NOALLOC_MAX_CELLS 77594624ull
 culbm_status culbm_mass_momentum_noalloc(const float* d_ddf, uint64_t n, void* stream, double out[4]);
 
+/*
+ * Tile and innerLoop choice for the L2-blocked policies (--blockDim auto).
+ * Restates the speed-up model of the reference's analysis/selector.py:15-69
+ * (valid fraction of a tile, sector alignment of its valid rows, L2 reuse)
+ * with the constants of this device, restricted to geometries the blocking
+ * engine accepts for the domain (the reference's selector ignores the domain).
+ */
+typedef struct culbm_memory_constants {
+    double dram_gbs;               /* copy bandwidth, two arrays of 3x L2 each */
+    double l2_gbs;                 /* copy bandwidth, two arrays of L2/4 each */
+    double lambda;                 /* dram_gbs / l2_gbs */
+    double full_store_ms;          /* 1 GiB of 128-byte streaming stores, four full sectors each */
+    double partial_store_ms;       /* the same with one partial sector per 128 bytes */
+    double gamma;                  /* 4 partial/full - 3: cost of a partial sector in full sectors */
+    uint64_t l2_bytes;
+    uint32_t reserved[8];
+} culbm_memory_constants;
+
+/* Measures lambda and gamma on device `dev`: the experiments of the
+ * reference's analysis/lambda/measure.cu and analysis/gamma/measure.cu,
+ * written anew (allocates about 1.8 GB for a few seconds). */
+culbm_status culbm_measure_memory(int32_t dev, culbm_memory_constants* out);
+
+typedef struct culbm_tile_choice {
+    uint32_t tile[3];              /* blockDim * gridDim of the chosen tile */
+    int32_t inner_loop;
+    double predicted_speedup;      /* model speed-up over plain streaming (S) */
+    double predicted_speedup_no_alignment;  /* the same without the sector-alignment term (S0) */
+    uint32_t reserved[8];
+} culbm_tile_choice;
+
+/* Constants used when lambda, gamma <= 0: culbm_measure_memory on a B200
+ * (DRAM copy 6.48 TB/s, L2 copy 13.4 TB/s; a partial sector costs 8.8 full ones). */
+#define CULBM_B200_LAMBDA 0.4841
+#define CULBM_B200_GAMMA 8.772
+
+/* The tile and innerLoop of the largest model speed-up for `domain_dim` and
+ * population storage `storage` (CULBM_STORAGE_*).  lambda, gamma <= 0: the
+ * B200 values above; l2_bytes, persist_bytes == 0: the current device's L2
+ * size and persisting-L2 limit. */
+culbm_status culbm_select_tile(const uint32_t domain_dim[3], int32_t storage, double lambda, double gamma,
+                               uint64_t l2_bytes, uint64_t persist_bytes, culbm_tile_choice* out);
+
+/* The model's speed-up S (and S0, without the alignment term) of one tile
+ * and innerLoop; same conventions as culbm_select_tile. */
+culbm_status culbm_blocking_speedup(const uint32_t tile[3], int32_t inner_loop, int32_t storage, double lambda,
+                                    double gamma, uint64_t l2_bytes, double* speedup, double* speedup_no_alignment);
+
 typedef struct culbm_info {
     uint64_t cells;                 /* N */
     uint64_t device_bytes;          /* bytes the library allocated on the device */

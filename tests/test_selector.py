@@ -1,0 +1,53 @@
+"""Tile/innerLoop selector of the L2-blocked policies (culbm_select_tile,
+culbm_blocking_speedup): the model restated in selector.cu against golden
+values of the reference's own analysis/selector.py (tests/golden/
+make_selector_golden.py), on CPU: with the constants given, no device is
+touched."""
+import json
+import os
+
+import pytest
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "selector_reference.json")
+
+
+def cases():
+    with open(GOLDEN) as f:
+        return json.load(f)["cases"]
+
+
+@pytest.mark.parametrize("case", cases(), ids=lambda c: f"lambda{c['lambda']}")
+def test_model_values_match_the_reference(culbm, case):
+    from culbm_b200 import selector
+    for bx, by, bz, it, s_ref, s0_ref in case["points"]:
+        s, s0 = selector.speedup((bx, by, bz), it, "fp32", case["lambda"], case["gamma"], case["l2_bytes"])
+        assert s == pytest.approx(s_ref, rel=1e-12), (bx, by, bz, it)
+        assert s0 == pytest.approx(s0_ref, rel=1e-12), (bx, by, bz, it)
+
+
+@pytest.mark.parametrize("case", cases(), ids=lambda c: f"lambda{c['lambda']}")
+def test_choice_matches_the_reference_on_a_large_domain(culbm, case):
+    """On a domain large enough for every tile the choice is the model's argmax."""
+    from culbm_b200 import selector
+    got = selector.select((4096, 4096, 4096), "fp32", case["lambda"], case["gamma"], case["l2_bytes"],
+                          case["persist_bytes"])
+    assert got["tile"] + [got["inner_loop"]] == case["argmax"]
+    assert got["speedup"] == pytest.approx(case["S_argmax"], rel=1e-12)
+
+
+def test_choice_respects_the_domain_and_storage(culbm):
+    from culbm_b200 import selector
+    from culbm_b200._capi import CulbmError
+    c = cases()[0]
+    big = selector.select((4096, 4096, 4096), "fp32", c["lambda"], c["gamma"], c["l2_bytes"], c["persist_bytes"])
+    half = selector.select((4096, 4096, 4096), "fp16", c["lambda"], c["gamma"], c["l2_bytes"], c["persist_bytes"])
+    # half the bytes per cell: at least as large a tile fits the persisting window
+    assert half["tile"][0] * half["tile"][1] * half["tile"][2] >= big["tile"][0] * big["tile"][1] * big["tile"][2]
+    small = selector.select((64, 40, 40), "fp32", c["lambda"], c["gamma"], c["l2_bytes"], c["persist_bytes"])
+    from culbm_b200 import _capi
+    import oracle
+    L = oracle.lib()
+    for k, dom in enumerate((64, 40, 40)):
+        assert L.orc_valid_blk_axis(dom, small["tile"][k], small["inner_loop"])
+    with pytest.raises(CulbmError):
+        selector.select((4096, 4096, 4096), "fp32", c["lambda"], c["gamma"], c["l2_bytes"], 1000)
