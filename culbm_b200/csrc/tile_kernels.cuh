@@ -136,14 +136,16 @@ __device__ __forceinline__ void tile_pull_global(const TileArgs<S, R>& a, const 
 {
     const Domain& D = a.dom;
     const S* base = a.g.base[sel];
+    // the three clamped source columns, rows and planes (x - c for c = -1, 0, 1
+    // at index 1 - c), the planes through the ring mapping when there is one
+    const int xs[3] = {c.gx == 0 ? c.gx : c.gx - 1, c.gx, c.gx == D.nx - 1 ? c.gx : c.gx + 1};
+    const int ys[3] = {(c.gy == 0 ? c.gy : c.gy - 1) * D.nx, c.gy * D.nx,
+                       (c.gy == D.ny - 1 ? c.gy : c.gy + 1) * D.nx};
+    const long long zs[3] = {gaddr(a.g, D, offz, 0, 0, c.gz == 0 ? c.gz : c.gz - 1), gaddr(a.g, D, offz, 0, 0, c.gz),
+                             gaddr(a.g, D, offz, 0, 0, c.gz == D.nz - 1 ? c.gz : c.gz + 1)};
 #pragma unroll
-    for (int d = 0; d < 27; ++d) {
-        int sx = c.gx - cx_of(d), sy = c.gy - cy_of(d), sz = c.gz - cz_of(d);
-        if ((unsigned)sx >= (unsigned)D.nx) sx = c.gx;
-        if ((unsigned)sy >= (unsigned)D.ny) sy = c.gy;
-        if ((unsigned)sz >= (unsigned)D.nz) sz = c.gz;
-        f[d] = gload<S, R, HINT>(base + d * a.g.stride + gaddr(a.g, D, offz, sx, sy, sz));
-    }
+    for (int d = 0; d < 27; ++d)
+        f[d] = gload<S, R, HINT>(base + d * a.g.stride + zs[1 - cz_of(d)] + (ys[1 - cy_of(d)] + xs[1 - cx_of(d)]));
 }
 
 template <typename S, typename R, bool HINT>
@@ -174,11 +176,18 @@ __device__ __forceinline__ void tile_load_aa(const TileArgs<S, R>& a, const Tile
         for (int d = 0; d < 27; ++d) f[d] = Cvt<S, R>::ld(a.t0.p[d] + c.t);
         return;
     }
-    const bool tile_inner = c.px > 0 && c.px < a.bx - 1 && c.py > 0 && c.py < a.by - 1 && c.pz > 0 && c.pz < a.bz - 1;
-    if (!edge && tile_inner) {
+    if (!edge) {
+        // off the domain faces only the tile's own faces cut pulls off; the
+        // masks are per lane (predicated loads), so warps do not diverge
+        const bool lx = c.px > 0, hx = c.px < a.bx - 1, ly = c.py > 0, hy = c.py < a.by - 1, lz = c.pz > 0,
+                   hz = c.pz < a.bz - 1;
 #pragma unroll
-        for (int d = 0; d < 27; ++d)
-            f[d] = Cvt<S, R>::ld(a.t0.p[26 - d] + (c.t - (cx_of(d) + cy_of(d) * a.bx + cz_of(d) * a.bxy)));
+        for (int d = 0; d < 27; ++d) {
+            const int cx = cx_of(d), cy = cy_of(d), cz = cz_of(d);
+            const bool ok = (cx == 1 ? lx : cx == -1 ? hx : true) && (cy == 1 ? ly : cy == -1 ? hy : true) &&
+                            (cz == 1 ? lz : cz == -1 ? hz : true);
+            f[d] = ok ? Cvt<S, R>::ld(a.t0.p[26 - d] + (c.t - (cx + cy * a.bx + cz * a.bxy))) : R(0);
+        }
         return;
     }
 #pragma unroll
@@ -253,11 +262,19 @@ __global__ void __launch_bounds__(256) k_tile_aa_odd(const __grid_constant__ Til
     }
     cell_update_for<S, false>(op, a.inv_tau, a.rho, a.vx, a.vy, a.vz, c.gi, f);
     if (!(op & OP_STORE)) return;
-    const bool tile_inner = c.px > 0 && c.px < a.bx - 1 && c.py > 0 && c.py < a.by - 1 && c.pz > 0 && c.pz < a.bz - 1;
-    if (!edge && tile_inner) {
+    if (!edge) {
+        // off the domain faces a push only has to stay inside the tile
+        // (predicated stores, no divergence)
+        const bool lx = c.px > 0, hx = c.px < a.bx - 1, ly = c.py > 0, hy = c.py < a.by - 1, lz = c.pz > 0,
+                   hz = c.pz < a.bz - 1;
+        const uint32_t hc = tile_hash(a, c.gi);
 #pragma unroll
-        for (int d = 0; d < 27; ++d)
-            put(a.t0.p[d] + (c.t + cx_of(d) + cy_of(d) * a.bx + cz_of(d) * a.bxy), f[d], tile_hash(a, c.gi), d);
+        for (int d = 0; d < 27; ++d) {
+            const int cx = cx_of(d), cy = cy_of(d), cz = cz_of(d);
+            const bool ok = (cx == 1 ? hx : cx == -1 ? lx : true) && (cy == 1 ? hy : cy == -1 ? ly : true) &&
+                            (cz == 1 ? hz : cz == -1 ? lz : true);
+            if (ok) put(a.t0.p[d] + (c.t + cx + cy * a.bx + cz * a.bxy), f[d], hc, d);
+        }
         return;
     }
     for_dirs([&](auto dd) {
@@ -323,11 +340,18 @@ template <typename S, typename R>
 __device__ __forceinline__ void tile_pull(const TileArgs<S, R>& a, const Pops<S>& src, const TileCell& c, bool edge,
                                           R* f)
 {
-    const bool tile_inner = c.px > 0 && c.px < a.bx - 1 && c.py > 0 && c.py < a.by - 1 && c.pz > 0 && c.pz < a.bz - 1;
-    if (!edge && tile_inner) {
+    if (!edge) {
+        // off the domain faces only the tile's own faces cut pulls off
+        // (per-lane predicated loads, no divergence)
+        const bool lx = c.px > 0, hx = c.px < a.bx - 1, ly = c.py > 0, hy = c.py < a.by - 1, lz = c.pz > 0,
+                   hz = c.pz < a.bz - 1;
 #pragma unroll
-        for (int d = 0; d < 27; ++d)
-            f[d] = Cvt<S, R>::ld(src.p[d] + (c.t - (cx_of(d) + cy_of(d) * a.bx + cz_of(d) * a.bxy)));
+        for (int d = 0; d < 27; ++d) {
+            const int cx = cx_of(d), cy = cy_of(d), cz = cz_of(d);
+            const bool ok = (cx == 1 ? lx : cx == -1 ? hx : true) && (cy == 1 ? ly : cy == -1 ? hy : true) &&
+                            (cz == 1 ? lz : cz == -1 ? hz : true);
+            f[d] = ok ? Cvt<S, R>::ld(src.p[d] + (c.t - (cx + cy * a.bx + cz * a.bxy))) : R(0);
+        }
         return;
     }
 #pragma unroll
