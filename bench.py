@@ -220,21 +220,23 @@ def mixed_precision_512(culbm, steps):
     peak, _ = peaks()
     out = {"workload": "512x512x256 channel, 120 seeded spheres r in [6,18], invTau 0.5, ux_in 0.05",
            "cells": sc.n, "steps": steps, "runs": {}}
-    for name, (op, st, tile) in {
-        "inplace_fp32": (0, "fp32", None),
-        "inplace_fp16": (0, "fp16", None),
-        "inplace_fp16sr": (0, "fp16sr", None),
-        "inplace_bf16": (0, "bf16", None),
-        "inplace_bf16sr": (0, "bf16sr", None),
-        "blocked_inplace_fp32": (3, "fp32", (128, 64, 64)),
-        "blocked_inplace_fp16sr": (3, "fp16sr", (128, 64, 64)),
+    from culbm_b200 import selector
+    s32, s16 = selector.select(sc.shape, "fp32"), selector.select(sc.shape, "fp16sr")
+    for name, (op, st, tile, inner) in {
+        "inplace_fp32": (0, "fp32", None, 5),
+        "inplace_fp16": (0, "fp16", None, 5),
+        "inplace_fp16sr": (0, "fp16sr", None, 5),
+        "inplace_bf16": (0, "bf16", None, 5),
+        "inplace_bf16sr": (0, "bf16sr", None, 5),
+        "blocked_inplace_fp32": (3, "fp32", tuple(s32["tile"]), s32["inner_loop"]),
+        "blocked_inplace_fp16sr": (3, "fp16sr", tuple(s16["tile"]), s16["inner_loop"]),
     }.items():
         try:
-            mlups, mps, _ = measure(culbm, sc, 1, op, st, steps, 3, tile=tile, inner=5)
+            mlups, mps, _ = measure(culbm, sc, 1, op, st, steps, 3, tile=tile, inner=inner)
             out["runs"][name] = {"mlups": round(mlups, 1), "ms_per_step": round(mps, 4),
                                  "hbm_frac_of_measured": round(mlups * 1e6 * BYTES_PER_LUP[st] / 1e9 / peak, 4),
                                  "policy": "streamPolicy 1, optPolicy %d" % op +
-                                           (f", tile {tile}, innerLoop 5" if op else "")}
+                                           (f", tile {tile} (culbm_select_tile), innerLoop {inner}" if op else "")}
         except Exception as e:   # report, do not hide
             out["runs"][name] = {"error": str(e)}
     return out
@@ -371,20 +373,25 @@ def run_ours(args):
     achieved = BYTES_PER_LUP["fp32"] * sc.n / (ms / args.steps * 1e-3) / 1e9
     extra = {}
     k2 = max(20, args.steps // 4)
-    for name, (sp, op, st, tile) in {
-        "pull_fp32": (0, 0, "fp32", None),
-        "inplace_fp16": (1, 0, "fp16", None),
-        "inplace_fp16sr": (1, 0, "fp16sr", None),
-        "inplace_bf16": (1, 0, "bf16", None),
-        "pull_fp16": (0, 0, "fp16", None),
-        "pull_fp16sr": (0, 0, "fp16sr", None),
-        "blocked_inplace_fp32": (1, 3, "fp32", (144, 68, 40)),
+    from culbm_b200 import selector
+    sel = selector.select(sc.shape, "fp32")
+    for name, (sp, op, st, tile, inner) in {
+        "pull_fp32": (0, 0, "fp32", None, 5),
+        "inplace_fp16": (1, 0, "fp16", None, 5),
+        "inplace_fp16sr": (1, 0, "fp16sr", None, 5),
+        "inplace_bf16": (1, 0, "bf16", None, 5),
+        "pull_fp16": (0, 0, "fp16", None, 5),
+        "pull_fp16sr": (0, 0, "fp16sr", None, 5),
+        # the reference README's (1,3) launch shape: tile [32,16,2] x [2,6,38]
+        "blocked_inplace_fp32_readme_tile": (1, 3, "fp32", (64, 96, 76), 5),
+        "blocked_inplace_fp32_selected_tile": (1, 3, "fp32", tuple(sel["tile"]), sel["inner_loop"]),
     }.items():
         try:
-            mlups, mps, inf = measure(culbm_b200, sc, sp, op, st, k2, 3, tile=tile, inner=5)
+            mlups, mps, inf = measure(culbm_b200, sc, sp, op, st, k2, 3, tile=tile, inner=inner)
             extra[name] = {"mlups": round(mlups, 1), "ms_per_step": round(mps, 4),
                            "hbm_frac_of_measured": round(mlups * 1e6 * BYTES_PER_LUP[st] / 1e9 / peak, 4),
-                           "policy": f"streamPolicy {sp}, optPolicy {op}" + (f", tile {tile}, innerLoop 5" if op else "")}
+                           "policy": f"streamPolicy {sp}, optPolicy {op}" +
+                                     (f", tile {tile}, innerLoop {inner}" if op else "")}
         except Exception as e:   # report, do not hide
             extra[name] = {"error": str(e)}
     try:
