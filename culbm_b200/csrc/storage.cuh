@@ -111,9 +111,16 @@ __device__ __forceinline__ uint32_t cell_hash(uint32_t cell, uint32_t seed)
     return h;
 }
 
+// Random bits of direction d: the cell hash times an odd multiplier of its
+// own per direction (one multiply; the high bits are used).
+__host__ __device__ constexpr uint32_t dir_multiplier(uint32_t d)
+{
+    return (0x2C1B3C6Du ^ (d * 0x9E3779B9u)) | 1u;
+}
+
 __device__ __forceinline__ uint32_t dir_bits(uint32_t hcell, uint32_t d)
 {
-    return (hcell ^ (d * 0x9E3779B9u)) * 0x2C1B3C6Du;
+    return hcell * dir_multiplier(d);
 }
 
 template <> struct Cvt<Half16SR, float> {

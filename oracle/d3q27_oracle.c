@@ -95,13 +95,13 @@ uint32_t orc_step_seed(uint32_t t)
 }
 
 /* random bits of population d of `cell` at the step seeded by `seed`: a
- * per-cell finaliser hash, then a per-direction multiplicative hash whose
- * high bits are used */
+ * per-cell finaliser hash times an odd multiplier of direction d (the high
+ * bits are used) */
 uint32_t orc_sr_bits(uint32_t cell, uint32_t d, uint32_t seed)
 {
     uint32_t h = cell * 0x27D4EB2Fu ^ seed;
     h ^= h >> 16; h *= 0x85EBCA6Bu; h ^= h >> 13; h *= 0xC2B2AE35u; h ^= h >> 16;
-    return (h ^ (d * 0x9E3779B9u)) * 0x2C1B3C6Du;
+    return h * ((0x2C1B3C6Du ^ (d * 0x9E3779B9u)) | 1u);
 }
 
 static float h16_decode(uint16_t h)
