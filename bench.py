@@ -147,6 +147,12 @@ def barrier(tdist):
         tdist.barrier()
 
 
+def aggregate_mlups(ws, cells, steps, ms_max):
+    """Whole-job MLUPS of ws independent replicas of `cells` cells run for
+    `steps` steps, timed by the slowest rank (ms_max, device time)."""
+    return ws * cells * steps / (ms_max * 1e-3) / 1e6
+
+
 def pinned(arr):
     """A page-locked host copy of arr (torch pinned memory, viewed by numpy)."""
     import torch
@@ -361,7 +367,7 @@ def run_ours(args):
         info = sim.info()
     barrier(tdist)
     ms_max = max_over_ranks(tdist, ms)
-    value = ws * sc.n * args.steps / (ms_max * 1e-3) / 1e6
+    value = aggregate_mlups(ws, sc.n, args.steps, ms_max)
     ms_per_step = ms_max / args.steps
     launches = int(round(info["launches_per_step"] * args.steps))
 
