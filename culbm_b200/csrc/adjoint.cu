@@ -284,18 +284,21 @@ __device__ __forceinline__ R gather_lambda(const Args<S, R>& a, const CellCoord&
     }
 }
 
-// Shared-memory staging of the populations f1 (after the EQU overwrite,
-// before bounce-back) of the block's 256 cells: direction d of thread t at
-// fs[d * 256 + t], bank-conflict free.  Keeping f out of registers while the
-// 27 adjoint values are held lets four blocks of 256 share an SM.
+// <l, f1> and <l, B(f1)> accumulated while f1 is pulled (l gathered first),
+// so that f1 is never held: with bounce-back f2 = B(f1) they are <l, B(f2)>
+// and <l, f2>.
 template <typename R>
-struct FStage {
-    R* fs;
-    int t;
-    __device__ __forceinline__ R& operator[](int d) const { return fs[d * 256 + t]; }
+struct PullDots {
+    R a = R(0), b = R(0);
+    template <int d>
+    __device__ __forceinline__ void add(const R* l, R v)
+    {
+        a += l[d] * v;
+        b += l[26 - d] * v;
+    }
 };
 
-// r = sum f1 and j = sum c f1 accumulated while staging, in direction order.
+// r = sum f1 and j = sum c f1 accumulated while pulling, in direction order.
 template <typename R>
 struct MomentAcc {
     R r = R(0), x = R(0), y = R(0), z = R(0);
@@ -339,50 +342,79 @@ __device__ __forceinline__ void swap_pairs_if(bool c, R* v)
     }
 }
 
+// The ten weighted sums sum_d w_d c_d^k l_d (k = 0, 1, 2) of l by per-axis
+// factorisation: w_d = W(cx) W(cy) W(cz) with W(0) = 4/6 and W(+-1) = 1/6,
+// so three passes of 1D three-point moments (x, then y, then z) give them,
+// each times 216.  Direction d = (cx+1) + 3 (cy+1) + 9 (cz+1).
+template <typename R>
+struct LSums {
+    R m0, mx, my, mz, mxx, myy, mzz, mxy, mxz, myz;
+};
+
+template <typename R>
+__device__ __forceinline__ LSums<R> weighted_sums(const R* l)
+{
+    R x0[9], x1[9], x2[9];   // per (cy, cz) line: 6 x {W-sum, W-sum cx, W-sum cx^2}
+#pragma unroll
+    for (int j = 0; j < 9; ++j) {
+        const R lo = l[3 * j], mid = l[3 * j + 1], hi = l[3 * j + 2];
+        x2[j] = lo + hi;
+        x0[j] = R(4) * mid + x2[j];
+        x1[j] = hi - lo;
+    }
+    R y00[3], y10[3], y20[3], y01[3], y11[3], y02[3];   // per cz
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const int j = 3 * k;
+        y02[k] = x0[j] + x0[j + 2];
+        y00[k] = R(4) * x0[j + 1] + y02[k];
+        y01[k] = x0[j + 2] - x0[j];
+        y10[k] = R(4) * x1[j + 1] + (x1[j] + x1[j + 2]);
+        y11[k] = x1[j + 2] - x1[j];
+        y20[k] = R(4) * x2[j + 1] + (x2[j] + x2[j + 2]);
+    }
+    LSums<R> m;
+    m.mzz = y00[0] + y00[2];
+    m.m0 = R(4) * y00[1] + m.mzz;
+    m.mz = y00[2] - y00[0];
+    m.mx = R(4) * y10[1] + (y10[0] + y10[2]);
+    m.mxz = y10[2] - y10[0];
+    m.my = R(4) * y01[1] + (y01[0] + y01[2]);
+    m.myz = y01[2] - y01[0];
+    m.mxx = R(4) * y20[1] + (y20[0] + y20[2]);
+    m.myy = R(4) * y02[1] + (y02[0] + y02[2]);
+    m.mxy = R(4) * y11[1] + (y11[0] + y11[2]);
+    return m;
+}
+
 // Reverse of bounce-back and soft collision for one cell, linearised at
-// f2 = B(f1) if the cell bounces back, else f1, with f = fscale * the staged
-// values (possibly raw 16-bit values) and (rho, u) its moments; plain
-// arithmetic.  l enters as the adjoint of the stored populations and leaves
-// as the adjoint of f1; gs and gw are the cell's dJ/ds and dJ/dw (0 unless it
-// collides).  The sums are evaluated for every cell; the update of l is
-// skipped by a (mostly warp-uniform) branch.  With P = <l, f2>,
-// Q = <l, B(f2)>, E = <l, feq(f2)>:
+// f2 = B(f1) if the cell bounces back, else f1, with f = fscale * the pulled
+// values (possibly raw 16-bit values), (rho, u) its moments and
+// dots = (<l, f1>, <l, B(f1)>) of the pulled values; plain arithmetic.  l
+// enters as the adjoint of the stored populations and leaves as the adjoint
+// of f1; gs and gw are the cell's dJ/ds and dJ/dw (0 unless it collides and
+// stores).  With P = <l, f2>, Q = <l, B(f2)>, E = <l, feq(f2)>:
 //     dJ/ds = <l, B(f2) - C(f2)> = (Q - P) - w (E - P),
 //     dJ/dw = (1 - s) <l, feq - f2> = (1 - s) (E - P),
 // and E = (rho - 1) a_rho + 3 Lcu + 9/2 Lcu2 - 3/2 |u|^2 L0 comes from the
-// same weighted sums as J_C^T, so no per-direction equilibrium is formed.
+// same weighted sums as J_C^T, so no per-direction equilibrium is formed:
+// with M = sum w c c^T l, Lcu = u.L, Lccu = M u and Lcu2 = u.M u.
 template <typename R>
-__device__ __forceinline__ void reverse_cell(uint8_t op, R w, R s, R fscale, const FStage<R>& f1, R rho, R ux, R uy,
-                                             R uz, R* l, R& gs, R& gw)
+__device__ __forceinline__ void reverse_cell(uint8_t op, R w, R s, R fscale, const PullDots<R>& dots, R rho, R ux,
+                                             R uy, R uz, R* l, R& gs, R& gw)
 {
     const bool bb = (op & OP_BB) != 0, col = (op & OP_COLLIDE) && (op & OP_STORE);
-    const R om = R(1) - w;
     const R uu = ux * ux + uy * uy + uz * uz;
-    R P = 0, QmP = 0, L0 = 0, Lx = 0, Ly = 0, Lz = 0, Lcu = 0, Lcu2 = 0, Lcx = 0, Lcy = 0, Lcz = 0;
-#pragma unroll
-    for (int d = 0; d < 13; ++d) {
-        const int e = 26 - d;
-        const R ld = l[d], le = l[e];
-        const R fd = f1[bb ? e : d], fe = f1[bb ? d : e];
-        const R cx = R(cx_of(d)), cy = R(cy_of(d)), cz = R(cz_of(d)), wd = weight<R>(d);
-        const R cu = cx * ux + cy * uy + cz * uz;
-        P += ld * fd + le * fe;
-        QmP += (ld - le) * (fe - fd);
-        const R sp = wd * (ld + le), sm = wd * (ld - le);
-        L0 += sp;
-        Lx += cx * sm;
-        Ly += cy * sm;
-        Lz += cz * sm;
-        Lcu += cu * sm;
-        const R cusp = cu * sp;
-        Lcu2 += cu * cusp;
-        Lcx += cx * cusp;
-        Lcy += cy * cusp;
-        Lcz += cz * cusp;
-    }
-    P = fscale * (P + l[13] * f1[13]);
-    QmP *= fscale;
-    L0 += weight<R>(13) * l[13];
+    const R P = fscale * (bb ? dots.b : dots.a);
+    const R QmP = fscale * (bb ? dots.a - dots.b : dots.b - dots.a);
+    const LSums<R> m = weighted_sums(l);
+    constexpr R k216 = R(1) / R(216);
+    const R L0 = k216 * m.m0, Lx = k216 * m.mx, Ly = k216 * m.my, Lz = k216 * m.mz;
+    const R Mux = k216 * (m.mxx * ux + m.mxy * uy + m.mxz * uz);
+    const R Muy = k216 * (m.mxy * ux + m.myy * uy + m.myz * uz);
+    const R Muz = k216 * (m.mxz * ux + m.myz * uy + m.mzz * uz);
+    const R Lcu = ux * Lx + uy * Ly + uz * Lz;
+    const R Lcu2 = ux * Mux + uy * Muy + uz * Muz;
     const R a1 = R(3) * Lcu + R(4.5) * Lcu2 - R(1.5) * uu * L0;
     const R ar = L0 + a1;
     const R emp = ((rho - R(1)) * ar + a1) - P;
@@ -392,39 +424,55 @@ __device__ __forceinline__ void reverse_cell(uint8_t op, R w, R s, R fscale, con
         if (bb) swap_pairs_if(true, l);
         return;
     }
-    // l <- (1-s) J_C^T l + s B(l),  (J_C^T l)_e = (1-w) l_e + w (a_rho + c_e.b - u.b)
-    const R bx = w * (R(3) * Lx + R(9) * Lcx - R(3) * ux * L0);
-    const R by = w * (R(3) * Ly + R(9) * Lcy - R(3) * uy * L0);
-    const R bz = w * (R(3) * Lz + R(9) * Lcz - R(3) * uz * L0);
-    const R q = w * ar - (ux * bx + uy * by + uz * bz);
+    // l <- (1-s) J_C^T l + s B(l),  (J_C^T l)_e = (1-w) l_e + w (a_rho + c_e.b - u.b):
+    // l_e <- (1-s)(1-w) l_e + s l_{26-e} + t_e,  t_e = (1-s) w (a_rho - u.b + c_e.b)
+    const R bx = w * (R(3) * Lx + R(9) * Mux - R(3) * ux * L0);
+    const R by = w * (R(3) * Ly + R(9) * Muy - R(3) * uy * L0);
+    const R bz = w * (R(3) * Lz + R(9) * Muz - R(3) * uz * L0);
+    const R sc = R(1) - s;
+    const R q = sc * (w * ar - (ux * bx + uy * by + uz * bz));
+    const R tx = sc * bx, ty = sc * by, tz = sc * bz;
+    const R keep = sc * (R(1) - w);
+    R t[27];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const R qz = k == 1 ? q : (k == 0 ? q - tz : q + tz);
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            const R qy = j == 1 ? qz : (j == 0 ? qz - ty : qz + ty);
+            const int d = 3 * j + 9 * k;
+            t[d] = qy - tx;
+            t[d + 1] = qy;
+            t[d + 2] = qy + tx;
+        }
+    }
 #pragma unroll
     for (int d = 0; d < 13; ++d) {
         const int e = 26 - d;
         const R ld = l[d], le = l[e];
-        const R cb = R(cx_of(d)) * bx + R(cy_of(d)) * by + R(cz_of(d)) * bz;
-        const R jd = om * ld + (q + cb);
-        const R je = om * le + (q - cb);
-        l[d] = jd + s * (le - jd);
-        l[e] = je + s * (ld - je);
+        l[d] = keep * ld + (s * le + t[d]);
+        l[e] = keep * le + (s * ld + t[e]);
     }
-    const R j13 = om * l[13] + q;
-    l[13] = j13 + s * (l[13] - j13);
+    l[13] = keep * l[13] + (s * l[13] + t[13]);
     if (bb) swap_pairs_if(true, l);
 }
 
 // Reverse of one cell update at step t for a cell without EQU (EQU cells
 // only get nu = dJ/df here; adj_equ_cell does the rest of their work).  The
 // pull and the gather stay inside the domain for every cell, so all loads
-// are issued without looking at the op byte; f1 goes to the block's stage.
+// are issued without looking at the op byte.  l is gathered first and the
+// pulled values are folded into the moments and dots as they arrive.  l is
+// left unmasked for cells that do not store: their gs and gw are zero and
+// their nu is dJ/df alone.
 template <int ROWS, typename S, typename R>
-__device__ __forceinline__ void adj_cell(const Args<S, R>& a, const CellCoord c, const FStage<R>& f1,
-                                         double& gtau_local)
+__device__ __forceinline__ void adj_cell(const Args<S, R>& a, const CellCoord c, double& gtau_local)
 {
     const Domain& D = a.dom;
     const uint8_t op = a.ops[c.i];
     const R s = R(a.soft[c.i]);
     const bool load = (op & OP_LOAD) != 0, store = (op & OP_STORE) != 0, equ = (op & OP_EQU) != 0;
     MomentAcc<R> m;
+    PullDots<R> dots;
     R l[27];
     // warps of inner rows without an x-face lane (a warp-uniform choice) pull
     // and gather without any clamp handling
@@ -432,10 +480,13 @@ __device__ __forceinline__ void adj_cell(const Args<S, R>& a, const CellCoord c,
     if (ROWS == ROWS_INNER && xw != 0 && xw + 31 < D.nx - 1) {
         for_dirs([&](auto dd) {
             constexpr int d = decltype(dd)::value;
-            const R v = ld_raw<S, R>(a.src.p[d] + (c.i - nb_off(D, d)));
-            f1[d] = load ? v : R(0);
-            m.template add<d>(load ? v : R(0));
             l[d] = a.nu_in[d][c.i + nb_off(D, d)];
+        });
+        for_dirs([&](auto dd) {
+            constexpr int d = decltype(dd)::value;
+            const R v = ld_raw<S, R>(a.src.p[d] + (c.i - nb_off(D, d)));
+            m.template add<d>(load ? v : R(0));
+            dots.template add<d>(l, load ? v : R(0));
         });
     } else {
         constexpr bool inner = ROWS == ROWS_INNER;
@@ -444,27 +495,27 @@ __device__ __forceinline__ void adj_cell(const Args<S, R>& a, const CellCoord c,
         const int ndz = (!inner && c.z == 0) ? 0 : -D.nxy, pdz = (!inner && c.z == D.nz - 1) ? 0 : D.nxy;
         for_dirs([&](auto dd) {
             constexpr int d = decltype(dd)::value;
+            l[d] = gather_lambda<d, ROWS>(a, c);
+        });
+        for_dirs([&](auto dd) {
+            constexpr int d = decltype(dd)::value;
             const int ox = cx_of(d) == 1 ? ndx : cx_of(d) == -1 ? pdx : 0;
             const int oy = cy_of(d) == 1 ? ndy : cy_of(d) == -1 ? pdy : 0;
             const int oz = cz_of(d) == 1 ? ndz : cz_of(d) == -1 ? pdz : 0;
             const R v = ld_raw<S, R>(a.src.p[d] + (c.i + ox + oy + oz));
-            f1[d] = load ? v : R(0);
             m.template add<d>(load ? v : R(0));
-            l[d] = gather_lambda<d, ROWS>(a, c);
+            dots.template add<d>(l, load ? v : R(0));
         });
     }
-    if (!store)
-#pragma unroll
-        for (int d = 0; d < 27; ++d) l[d] = R(0);
     constexpr R fscale = R(RawScale<S>::value);
     R rho, ux, uy, uz, gs, gw;
     m.finish(fscale, (op & OP_BB) != 0, rho, ux, uy, uz);
-    reverse_cell(op, a.inv_tau, s, fscale, f1, rho, ux, uy, uz, l, gs, gw);
+    reverse_cell(op, a.inv_tau, s, fscale, dots, rho, ux, uy, uz, l, gs, gw);
     if (!equ && (op & OP_COLLIDE) && store) {
         a.g_soft[c.i] += static_cast<double>(gs);
         gtau_local = static_cast<double>(gw);
     }
-    const bool pulls = load && !equ;
+    const bool pulls = load && store && !equ;
     const R g = objective_term(a, c.x, op);
 #pragma unroll
     for (int d = 0; d < 27; ++d) a.nu_out[d][c.i] = (pulls ? l[d] : R(0)) + g;
@@ -475,7 +526,7 @@ __device__ __forceinline__ void adj_cell(const Args<S, R>& a, const CellCoord c,
 // dJ/d(rho_in, u_in) from d feq / d(rho, u).  Its nu (no pull, so dJ/df
 // only) is written by adj_cell.
 template <typename S, typename R>
-__device__ __forceinline__ void adj_equ_cell(const Args<S, R>& a, int i, const FStage<R>& f1, double& gtau_local)
+__device__ __forceinline__ void adj_equ_cell(const Args<S, R>& a, int i, double& gtau_local)
 {
     const Domain& D = a.dom;
     CellCoord c;
@@ -486,25 +537,26 @@ __device__ __forceinline__ void adj_equ_cell(const Args<S, R>& a, int i, const F
     c.valid = true;
     const uint8_t op = a.ops[i];
     const R r_in = R(a.rho[i]), vx = R(a.vx[i]), vy = R(a.vy[i]), vz = R(a.vz[i]);
-    MomentAcc<R> m;
-    {
-        R f[27];
-        equilibrium<R>(r_in, vx, vy, vz, f);
-        for_dirs([&](auto dd) {
-            constexpr int d = decltype(dd)::value;
-            f1[d] = f[d];
-            m.template add<d>(f[d]);
-        });
-    }
     R l[27];
     const bool store = (op & OP_STORE) != 0;
     for_dirs([&](auto dd) {
         constexpr int d = decltype(dd)::value;
         l[d] = store ? gather_lambda<d, ROWS_OUTER>(a, c) : R(0);
     });
+    MomentAcc<R> m;
+    PullDots<R> dots;
+    {
+        R f[27];
+        equilibrium<R>(r_in, vx, vy, vz, f);
+        for_dirs([&](auto dd) {
+            constexpr int d = decltype(dd)::value;
+            m.template add<d>(f[d]);
+            dots.template add<d>(l, f[d]);
+        });
+    }
     R rho, ux, uy, uz, gs, gw;
     m.finish(R(1), (op & OP_BB) != 0, rho, ux, uy, uz);
-    reverse_cell(op, a.inv_tau, R(a.soft[i]), R(1), f1, rho, ux, uy, uz, l, gs, gw);
+    reverse_cell(op, a.inv_tau, R(a.soft[i]), R(1), dots, rho, ux, uy, uz, l, gs, gw);
     if ((op & OP_COLLIDE) && store) {
         a.g_soft[i] += static_cast<double>(gs);
         gtau_local = static_cast<double>(gw);
@@ -539,25 +591,22 @@ inline dim3 adj_grid(const Domain& D, int n_equ)
 
 // One adjoint step over all cells (block-uniform roles); each warp adds its
 // invTau gradient into its own slot of g_tau_block (8 per block).
-// Dynamic shared memory: the f1 stage, 27 * 256 values of R.
 template <typename S, typename R>
 __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 1)
     k_adj_step(const __grid_constant__ Args<S, R> a, AdjLayout L)
 {
-    extern __shared__ __align__(16) unsigned char adj_stage[];
-    const FStage<R> f1{reinterpret_cast<R*>(adj_stage), static_cast<int>(threadIdx.x + 32 * threadIdx.y)};
     double gtau_local = 0.0;
     if (static_cast<int>(blockIdx.z) < L.equ_z) {
         const int blk = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
         const int k = blk * 256 + threadIdx.x + 32 * threadIdx.y;
-        if (k < a.n_equ) adj_equ_cell(a, a.equ_cells[k], f1, gtau_local);
+        if (k < a.n_equ) adj_equ_cell(a, a.equ_cells[k], gtau_local);
     } else {
         CellCoord c;
         const int kind = split_cell(a.dom, L.equ_z, c);
         if (kind == ROWS_OUTER)
-            adj_cell<ROWS_OUTER>(a, c, f1, gtau_local);
+            adj_cell<ROWS_OUTER>(a, c, gtau_local);
         else if (kind == ROWS_INNER)
-            adj_cell<ROWS_INNER>(a, c, f1, gtau_local);
+            adj_cell<ROWS_INNER>(a, c, gtau_local);
     }
     warp_accumulate(gtau_local, a.g_tau_block + 8ll * (blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)));
 }
@@ -810,7 +859,7 @@ culbm_status adjoint_segment(culbm_adj* a, int tb, int te, S* start, adj::Args<S
         const bool in_win = t >= t0 && t <= t1;
         g.obj_in = in_win ? obj_in : R(0);
         g.obj_out = in_win ? obj_out : R(0);
-        adj::k_adj_step<S, R><<<gr, block, 27 * 256 * sizeof(R), a->stream>>>(g, L);
+        adj::k_adj_step<S, R><<<gr, block, 0, a->stream>>>(g, L);
         CULBM_CUDA(cudaGetLastError());
         cur = 1 - cur;
     }
@@ -835,8 +884,6 @@ culbm_status run_gradient(culbm_adj* a)
     CULBM_CUDA(cudaMemsetAsync(a->d_gtau, 0, a->n_tau_blocks * sizeof(double), a->stream));
     CULBM_CUDA(cudaMemsetAsync(a->d_gmac, 0, 4 * a->n * sizeof(double), a->stream));
     R* const nu[2] = {static_cast<R*>(a->d_nu), static_cast<R*>(a->d_nu) + 27 * a->n};
-    CULBM_CUDA(cudaFuncSetAttribute(adj::k_adj_step<S, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    static_cast<int>(27 * 256 * sizeof(R))));
     auto g = base_args<S>(a);
     g.g_tau_block = a->d_gtau;
     g.equ_cells = a->d_equ;
