@@ -485,8 +485,8 @@ __device__ __forceinline__ void adj_cell(const Args<S, R>& a, const CellCoord c,
         for_dirs([&](auto dd) {
             constexpr int d = decltype(dd)::value;
             const R v = ld_raw<S, R>(a.src.p[d] + (c.i - nb_off(D, d)));
-            m.template add<d>(load ? v : R(0));
-            dots.template add<d>(l, load ? v : R(0));
+            m.template add<d>(v);
+            dots.template add<d>(l, v);
         });
     } else {
         constexpr bool inner = ROWS == ROWS_INNER;
@@ -503,9 +503,14 @@ __device__ __forceinline__ void adj_cell(const Args<S, R>& a, const CellCoord c,
             const int oy = cy_of(d) == 1 ? ndy : cy_of(d) == -1 ? pdy : 0;
             const int oz = cz_of(d) == 1 ? ndz : cz_of(d) == -1 ? pdz : 0;
             const R v = ld_raw<S, R>(a.src.p[d] + (c.i + ox + oy + oz));
-            m.template add<d>(load ? v : R(0));
-            dots.template add<d>(l, load ? v : R(0));
+            m.template add<d>(v);
+            dots.template add<d>(l, v);
         });
+    }
+    // a cell that does not load has f1 = 0: its sums restart from zero
+    if (!load) {
+        m = MomentAcc<R>{};
+        dots = PullDots<R>{};
     }
     constexpr R fscale = R(RawScale<S>::value);
     R rho, ux, uy, uz, gs, gw;
@@ -517,8 +522,14 @@ __device__ __forceinline__ void adj_cell(const Args<S, R>& a, const CellCoord c,
     }
     const bool pulls = load && store && !equ;
     const R g = objective_term(a, c.x, op);
+    if (!pulls)
 #pragma unroll
-    for (int d = 0; d < 27; ++d) a.nu_out[d][c.i] = (pulls ? l[d] : R(0)) + g;
+        for (int d = 0; d < 27; ++d) l[d] = R(0);
+    if (g != R(0))
+#pragma unroll
+        for (int d = 0; d < 27; ++d) l[d] += g;
+#pragma unroll
+    for (int d = 0; d < 27; ++d) a.nu_out[d][c.i] = l[d];
 }
 
 // The EQU cell i of one adjoint step: f1 = feq(rho_in, u_in), the gather
