@@ -47,6 +47,7 @@ struct TileArgs {
     Domain dom;
     int bx, by, bz, bxy;    // tile extent
     int ox, oy, oz;         // tile origin (global)
+    int sx, sy, sz;         // origin of this launch's box inside the tile (tile coordinates)
     int vlo[3], vhi[3];     // valid box [vlo, vhi) (global)
     const uint8_t* ops;
     const float* rho;
@@ -111,9 +112,9 @@ template <typename S, typename R>
 __device__ __forceinline__ TileCell tile_cell(const TileArgs<S, R>& a)
 {
     TileCell c;
-    c.px = blockIdx.x * blockDim.x + threadIdx.x;
-    c.py = blockIdx.y * blockDim.y + threadIdx.y;
-    c.pz = blockIdx.z;
+    c.px = a.sx + static_cast<int>(blockIdx.x * blockDim.x + threadIdx.x);
+    c.py = a.sy + static_cast<int>(blockIdx.y * blockDim.y + threadIdx.y);
+    c.pz = a.sz + static_cast<int>(blockIdx.z);
     c.t = c.px + a.bx * (c.py + a.by * c.pz);
     c.gx = a.ox + c.px;
     c.gy = a.oy + c.py;
@@ -128,6 +129,17 @@ __device__ __forceinline__ TileCell tile_cell(const TileArgs<S, R>& a)
 __device__ __forceinline__ bool in_tile(int px, int py, int pz, int bx, int by, int bz)
 {
     return (unsigned)px < (unsigned)bx && (unsigned)py < (unsigned)by && (unsigned)pz < (unsigned)bz;
+}
+
+// Programmatic dependent launch: the tile steps of a round are launched
+// with programmatic stream serialisation, so the next step's blocks may start
+// while this grid's last blocks run.  Each step lets its dependents start at
+// once and waits for the previous grid (complete, its memory visible) before
+// touching memory; the wait is the hardware's own and always ends.
+__device__ __forceinline__ void tile_step_enter()
+{
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
 }
 
 // Pull of all 27 populations from the global state with the domain clamp.
@@ -222,6 +234,7 @@ __device__ __forceinline__ void tile_file_clamp_sources(const TileArgs<S, R>& a,
 template <typename S, typename R, bool ONE, bool HINT>
 __global__ void __launch_bounds__(256) k_tile_aa_first(const __grid_constant__ TileArgs<S, R> a)
 {
+    tile_step_enter();
     const TileCell c = tile_cell(a);
     if (!c.active) return;
     const int ring = a.g.ring_nz;
@@ -248,6 +261,7 @@ __global__ void __launch_bounds__(256) k_tile_aa_first(const __grid_constant__ T
 template <typename S, typename R>
 __global__ void __launch_bounds__(256) k_tile_aa_odd(const __grid_constant__ TileArgs<S, R> a)
 {
+    tile_step_enter();
     const TileCell c = tile_cell(a);
     if (!c.active) return;
     const Domain& D = a.dom;
@@ -297,6 +311,7 @@ __global__ void __launch_bounds__(256) k_tile_aa_odd(const __grid_constant__ Til
 template <typename S, typename R>
 __global__ void __launch_bounds__(256) k_tile_aa_even(const __grid_constant__ TileArgs<S, R> a)
 {
+    tile_step_enter();
     const TileCell c = tile_cell(a);
     if (!c.active) return;
     const uint8_t op = a.ops[c.gi];
@@ -318,6 +333,7 @@ __global__ void __launch_bounds__(256) k_tile_aa_even(const __grid_constant__ Ti
 template <int LAYOUT, typename S, typename R, bool HINT>
 __global__ void __launch_bounds__(256) k_tile_aa_last(const __grid_constant__ TileArgs<S, R> a)
 {
+    tile_step_enter();
     const TileCell c = tile_cell(a);
     if (!c.active || !c.correct) return;
     const uint8_t op = a.ops[c.gi];
@@ -370,6 +386,7 @@ __device__ __forceinline__ void tile_pull(const TileArgs<S, R>& a, const Pops<S>
 template <typename S, typename R, bool ONE, bool HINT>
 __global__ void __launch_bounds__(256) k_tile_pull_first(const __grid_constant__ TileArgs<S, R> a)
 {
+    tile_step_enter();
     const TileCell c = tile_cell(a);
     if (!c.active) return;
     const int ring = a.g.ring_nz;
@@ -395,6 +412,7 @@ __global__ void __launch_bounds__(256) k_tile_pull_first(const __grid_constant__
 template <typename S, typename R>
 __global__ void __launch_bounds__(256) k_tile_pull_mid(const __grid_constant__ TileArgs<S, R> a)
 {
+    tile_step_enter();
     const TileCell c = tile_cell(a);
     if (!c.active) return;
     const uint8_t op = a.ops[c.gi];
@@ -414,6 +432,7 @@ __global__ void __launch_bounds__(256) k_tile_pull_mid(const __grid_constant__ T
 template <typename S, typename R, bool HINT>
 __global__ void __launch_bounds__(256) k_tile_pull_last(const __grid_constant__ TileArgs<S, R> a)
 {
+    tile_step_enter();
     const TileCell c = tile_cell(a);
     if (!c.active || !c.correct) return;
     const uint8_t op = a.ops[c.gi];

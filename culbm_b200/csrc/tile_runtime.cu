@@ -44,6 +44,10 @@ int32_t valid_prev(int32_t idx, int32_t blk, int32_t num, int32_t it, int32_t do
     return (blk + 1 - it) + (idx - 1) * (blk + 2 - 2 * it);
 }
 
+// Streams over which the tiles of one round are spread (double-buffered
+// global state only).
+constexpr int kTileLanes = 2;
+
 namespace {
 
 struct TileGeom {
@@ -59,7 +63,20 @@ struct TileState {
     int I = 1;
     long long tile_n = 0;
     std::vector<TileGeom> tiles;
-    void* d_tile = nullptr;      // one block: tile buffer 0 (and 1 for pull)
+    // Tiles of a round run on `lanes` streams at once (tile i on lane i mod
+    // lanes), each lane with its own tile buffers and, in place, its own
+    // edge buffer (scratch of one tile's round).  Two lanes let one tile's
+    // DRAM-bound first and last steps overlap another tile's L2-bound middle
+    // steps; they are used when both lanes' tile buffers fit in 70 % of L2
+    // (else the lanes evict each other's tiles) and not with the ring
+    // buffer, whose in-place result writes are placed for tiles taken in
+    // order.
+    int lanes = 1;
+    cudaStream_t side = nullptr;     // lane 1's stream (lane 0: the simulation's)
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    void* d_edge1 = nullptr;         // lane 1's edge buffer
+    size_t lane_bytes = 0;           // tile buffers of one lane
+    void* d_tile = nullptr;      // lanes x (tile buffer 0, and 1 for pull)
     RoundState* d_rs = nullptr;
     RoundState h_rs{};
     int ring_nz = 0, ring_step = 0;
@@ -109,19 +126,38 @@ struct TileLauncher {
         return a;
     }
 
+    // Launch of one step of the round on the part of the tile that later
+    // steps still read: the valid box grown by e = (steps left after this
+    // one), clipped to the tile and the domain.  A cell outside it only
+    // feeds cells farther than e from the valid box, whose values are never
+    // used, so the valid cells get the same bits as with whole-tile steps.
     template <typename K>
-    culbm_status launch(K kernel, const TileArgs<S, R>& a)
+    culbm_status launch(K kernel, TileArgs<S, R> a, const TileGeom& g, int e, cudaStream_t stream)
     {
+        int lo[3], n[3];
+        for (int q = 0; q < 3; ++q) {
+            const int dom_q = q == 0 ? s->dom.nx : q == 1 ? s->dom.ny : s->dom.nz;
+            lo[q] = std::max(0, g.vlo[q] - g.org[q] - e);
+            const int hi = std::min(std::min(ts->B[q], dom_q - g.org[q]), g.vhi[q] - g.org[q] + e);
+            n[q] = hi - lo[q];
+            if (n[q] <= 0) return CULBM_OK;
+        }
+        a.sx = lo[0];
+        a.sy = lo[1];
+        a.sz = lo[2];
         cudaLaunchConfig_t lc{};
-        lc.gridDim = dim3((ts->B[0] + 31) / 32, (ts->B[1] + 7) / 8, ts->B[2]);
+        lc.gridDim = dim3((n[0] + 31) / 32, (n[1] + 7) / 8, n[2]);
         lc.blockDim = dim3(32, 8, 1);
-        lc.stream = s->stream;
-        cudaLaunchAttribute attr[1];
+        lc.stream = stream;
+        cudaLaunchAttribute attr[2];
+        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[0].val.programmaticStreamSerializationAllowed = 1;
+        lc.attrs = attr;
+        lc.numAttrs = 1;
         if (ts->window) {
-            attr[0].id = cudaLaunchAttributeAccessPolicyWindow;
-            attr[0].val.accessPolicyWindow = ts->apw;
-            lc.attrs = attr;
-            lc.numAttrs = 1;
+            attr[1].id = cudaLaunchAttributeAccessPolicyWindow;
+            attr[1].val.accessPolicyWindow = ts->apw;
+            lc.numAttrs = 2;
         }
         CULBM_CUDA(cudaLaunchKernelEx(&lc, kernel, a));
         s->launches += 1;
@@ -129,12 +165,29 @@ struct TileLauncher {
     }
 
     // All tiles for one round of k <= I steps, then the round-state advance.
+    // Step j of a tile (0-based) covers the valid box grown by k - 1 - j.
+    // With two lanes, lane 1 forks from and joins the simulation's stream
+    // (recorded into the round's graph when captured).
     culbm_status round(int k)
     {
         const bool hint = s->cfg.cache_hints != 0;
         const bool inplace = s->cfg.stream_policy == CULBM_STREAM_INPLACE;
-        TileArgs<S, R> a = base_args();
-        for (const TileGeom& g : ts->tiles) {
+        const TileArgs<S, R> base = base_args();
+        if (ts->lanes > 1) {
+            CULBM_CUDA(cudaEventRecord(ts->ev_fork, s->stream));
+            CULBM_CUDA(cudaStreamWaitEvent(ts->side, ts->ev_fork, 0));
+        }
+        for (size_t ti = 0; ti < ts->tiles.size(); ++ti) {
+            const TileGeom& g = ts->tiles[ti];
+            const int lane = static_cast<int>(ti % static_cast<size_t>(ts->lanes));
+            const cudaStream_t st = lane ? ts->side : s->stream;
+            TileArgs<S, R> a = base;
+            if (lane) {
+                S* t = reinterpret_cast<S*>(static_cast<char*>(ts->d_tile) + ts->lane_bytes);
+                a.t0.set(t, ts->tile_n);
+                a.t1.set(t + 27 * ts->tile_n, ts->tile_n);
+                a.edge = static_cast<S*>(ts->d_edge1);
+            }
             a.ox = g.org[0];
             a.oy = g.org[1];
             a.oz = g.org[2];
@@ -145,41 +198,45 @@ struct TileLauncher {
             a.j = 0;
             if (inplace) {
                 if (k == 1) {
-                    CULBM_TRY(hint ? launch(k_tile_aa_first<S, R, true, true>, a)
-                                   : launch(k_tile_aa_first<S, R, true, false>, a));
+                    CULBM_TRY(hint ? launch(k_tile_aa_first<S, R, true, true>, a, g, 0, st)
+                                   : launch(k_tile_aa_first<S, R, true, false>, a, g, 0, st));
                     continue;
                 }
-                CULBM_TRY(hint ? launch(k_tile_aa_first<S, R, false, true>, a)
-                               : launch(k_tile_aa_first<S, R, false, false>, a));
+                CULBM_TRY(hint ? launch(k_tile_aa_first<S, R, false, true>, a, g, k - 1, st)
+                               : launch(k_tile_aa_first<S, R, false, false>, a, g, k - 1, st));
                 for (int j = 2; j < k; ++j) {
                     a.j = j - 1;
-                    if (j % 2 == 0) CULBM_TRY(launch(k_tile_aa_odd<S, R>, a));
-                    else CULBM_TRY(launch(k_tile_aa_even<S, R>, a));
+                    if (j % 2 == 0) CULBM_TRY(launch(k_tile_aa_odd<S, R>, a, g, k - j, st));
+                    else CULBM_TRY(launch(k_tile_aa_even<S, R>, a, g, k - j, st));
                 }
                 a.j = k - 1;
                 if (k % 2 == 0)
-                    CULBM_TRY(hint ? launch(k_tile_aa_last<LAYOUT_AA_A, S, R, true>, a)
-                                   : launch(k_tile_aa_last<LAYOUT_AA_A, S, R, false>, a));
+                    CULBM_TRY(hint ? launch(k_tile_aa_last<LAYOUT_AA_A, S, R, true>, a, g, 0, st)
+                                   : launch(k_tile_aa_last<LAYOUT_AA_A, S, R, false>, a, g, 0, st));
                 else
-                    CULBM_TRY(hint ? launch(k_tile_aa_last<LAYOUT_AA_B, S, R, true>, a)
-                                   : launch(k_tile_aa_last<LAYOUT_AA_B, S, R, false>, a));
+                    CULBM_TRY(hint ? launch(k_tile_aa_last<LAYOUT_AA_B, S, R, true>, a, g, 0, st)
+                                   : launch(k_tile_aa_last<LAYOUT_AA_B, S, R, false>, a, g, 0, st));
             } else {
                 if (k == 1) {
-                    CULBM_TRY(hint ? launch(k_tile_pull_first<S, R, true, true>, a)
-                                   : launch(k_tile_pull_first<S, R, true, false>, a));
+                    CULBM_TRY(hint ? launch(k_tile_pull_first<S, R, true, true>, a, g, 0, st)
+                                   : launch(k_tile_pull_first<S, R, true, false>, a, g, 0, st));
                     continue;
                 }
-                TileArgs<S, R> b = a;
-                CULBM_TRY(hint ? launch(k_tile_pull_first<S, R, false, true>, b)
-                               : launch(k_tile_pull_first<S, R, false, false>, b));
+                CULBM_TRY(hint ? launch(k_tile_pull_first<S, R, false, true>, a, g, k - 1, st)
+                               : launch(k_tile_pull_first<S, R, false, false>, a, g, k - 1, st));
                 for (int j = 2; j < k; ++j) {
-                    b.j = j - 1;
-                    CULBM_TRY(launch(k_tile_pull_mid<S, R>, b));
-                    std::swap(b.t0, b.t1);
+                    a.j = j - 1;
+                    CULBM_TRY(launch(k_tile_pull_mid<S, R>, a, g, k - j, st));
+                    std::swap(a.t0, a.t1);
                 }
-                b.j = k - 1;
-                CULBM_TRY(hint ? launch(k_tile_pull_last<S, R, true>, b) : launch(k_tile_pull_last<S, R, false>, b));
+                a.j = k - 1;
+                CULBM_TRY(hint ? launch(k_tile_pull_last<S, R, true>, a, g, 0, st)
+                               : launch(k_tile_pull_last<S, R, false>, a, g, 0, st));
             }
+        }
+        if (ts->lanes > 1) {
+            CULBM_CUDA(cudaEventRecord(ts->ev_join, ts->side));
+            CULBM_CUDA(cudaStreamWaitEvent(s->stream, ts->ev_join, 0));
         }
         k_tile_advance<<<1, 32, 0, s->stream>>>(ts->d_rs, ts->ring_nz, ts->ring_step, k);
         CULBM_CUDA(cudaGetLastError());
@@ -309,10 +366,23 @@ culbm_status tiles_create(culbm_sim* s)
             }
     ts->tile_n = 1ll * ts->B[0] * ts->B[1] * ts->B[2];
     const bool inplace = c.stream_policy == CULBM_STREAM_INPLACE;
-    const size_t tile_bytes = (inplace ? 1 : 2) * 27ull * ts->tile_n * s->esize;
+    ts->lane_bytes = ((inplace ? 1 : 2) * 27ull * ts->tile_n * s->esize + 255) / 256 * 256;
+    {
+        // a second lane only when both lanes' tile buffers stay well inside L2
+        int l2 = 0;
+        CULBM_CUDA(cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, s->dev));
+        const bool fits = kTileLanes * ts->lane_bytes <= static_cast<size_t>(0.7 * static_cast<double>(l2));
+        ts->lanes = (!c.use_ring_ddf_buf && ts->tiles.size() > 1 && fits) ? kTileLanes : 1;
+    }
+    const size_t tile_bytes = ts->lanes * ts->lane_bytes;
     void* p = nullptr;
     CULBM_TRY(dev_alloc(s, &p, tile_bytes, "tile buffers"));
     ts->d_tile = p;
+    if (ts->lanes > 1) {
+        CULBM_CUDA(cudaStreamCreateWithFlags(&ts->side, cudaStreamNonBlocking));
+        CULBM_CUDA(cudaEventCreateWithFlags(&ts->ev_fork, cudaEventDisableTiming));
+        CULBM_CUDA(cudaEventCreateWithFlags(&ts->ev_join, cudaEventDisableTiming));
+    }
     CULBM_TRY(dev_alloc(s, &p, sizeof(RoundState), "round state"));
     ts->d_rs = static_cast<RoundState*>(p);
 
@@ -352,6 +422,7 @@ culbm_status tiles_create(culbm_sim* s)
         s->el.off[5] = 2 * fx + 2 * fy + fz;
         s->edge_elems = 2 * (fx + fy + fz);
         CULBM_TRY(dev_alloc(s, &s->d_edge, s->edge_elems * s->esize, "edge buffer"));
+        if (ts->lanes > 1) CULBM_TRY(dev_alloc(s, &ts->d_edge1, s->edge_elems * s->esize, "lane edge buffer"));
     }
 
     // Keep the tile buffers resident: persisting set-aside + access-policy
@@ -383,6 +454,10 @@ void tiles_destroy(culbm_sim* s)
     if (ts->graph) cudaGraphExecDestroy(ts->graph);
     cudaFree(ts->d_tile);
     cudaFree(ts->d_rs);
+    cudaFree(ts->d_edge1);
+    if (ts->side) cudaStreamDestroy(ts->side);
+    if (ts->ev_fork) cudaEventDestroy(ts->ev_fork);
+    if (ts->ev_join) cudaEventDestroy(ts->ev_join);
     if (ts->window) {
         cudaCtxResetPersistingL2Cache();
         cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, 0);
