@@ -389,7 +389,7 @@ culbm_status culbm_config_init(culbm_config* cfg)
     cfg->inv_tau = 0.5f;
     cfg->use_ring_ddf_buf = 0;
     cfg->storage = CULBM_STORAGE_F32;
-    cfg->persist_l2 = 1;
+    cfg->persist_l2 = 0;
     cfg->cache_hints = 1;
     cfg->use_graphs = 1;
     return CULBM_OK;

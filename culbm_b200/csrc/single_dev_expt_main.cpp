@@ -7,8 +7,8 @@
 // lines ("Init ... successfully", "speed = X (MLUPS)"), dump files
 // <dumpFolder>/<field>_<step>.dat and exit codes (0; 1 with the message on
 // stderr for a runtime failure; the CLI11 parse-error codes for bad argv).
-// Additions: --storage fp32|fp16|bf16|fp64, --noPersistL2, --noCacheHints,
-// --noGraphs.
+// Additions: --storage fp32|fp16|bf16|fp64, --persistL2 (--noPersistL2, the
+// default, is accepted), --noCacheHints, --noGraphs.
 #include <cerrno>
 #include <cmath>
 #include <cstdint>
@@ -73,7 +73,8 @@ void usage(std::ostream& os)
           "  --useRingDDFBuf           One global DDF ring buffer for in-place dynamic L2 blocking.\n"
           "  --innerLoop INT [5]       # of iterations in halo-blocking.\n"
           "  --storage TEXT [fp32]     Population storage: fp32, fp16, bf16, fp64, fp16sr or bf16sr.\n"
-          "  --noPersistL2             No persisting-L2 window over tile buffers.\n"
+          "  --persistL2               Persisting-L2 window over tile buffers (off by default: slower on B200).\n"
+          "  --noPersistL2             No persisting-L2 window (the default).\n"
           "  --noCacheHints            No evict-first/evict-last cache hints.\n"
           "  --noGraphs                Launch tile sequences directly instead of CUDA graphs.\n";
 }
@@ -210,6 +211,9 @@ Options parse(int argc, char** argv)
         } else if (name == "--noPersistL2") {
             flag();
             o.cfg.persist_l2 = 0;
+        } else if (name == "--persistL2") {
+            flag();
+            o.cfg.persist_l2 = 1;
         } else if (name == "--noCacheHints") {
             flag();
             o.cfg.cache_hints = 0;

@@ -65,17 +65,18 @@ struct TileState {
     std::vector<TileGeom> tiles;
     // Tiles of a round run on `lanes` streams at once (tile i on lane i mod
     // lanes), each lane with its own tile buffers and, in place, its own
-    // edge buffer (scratch of one tile's round).  Two lanes let one tile's
-    // DRAM-bound first and last steps overlap another tile's L2-bound middle
-    // steps; they are used when both lanes' tile buffers fit in 70 % of L2
-    // (else the lanes evict each other's tiles) and not with the ring
-    // buffer, whose in-place result writes are placed for tiles taken in
-    // order.
+    // edge buffer (scratch of one tile's round).  Concurrent tiles let one
+    // tile's DRAM-bound first and last steps overlap other tiles' L2-bound
+    // middle steps.  Not with the ring buffer, whose in-place result writes
+    // are placed for tiles taken in order; under a persisting-L2 window only
+    // when all lanes' tile buffers fit in 70 % of L2 (the window's set-aside
+    // otherwise makes the lanes evict each other's tiles).
     int lanes = 1;
-    cudaStream_t side = nullptr;     // lane 1's stream (lane 0: the simulation's)
-    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
-    void* d_edge1 = nullptr;         // lane 1's edge buffer
-    size_t lane_bytes = 0;           // tile buffers of one lane
+    cudaStream_t side[kTileLanes] = {};      // streams of lanes 1.. (lane 0: the simulation's)
+    cudaEvent_t ev_fork = nullptr;
+    cudaEvent_t ev_join[kTileLanes] = {};
+    void* d_edge_lane[kTileLanes] = {};      // edge buffers of lanes 1.. (lane 0: the simulation's)
+    size_t lane_bytes = 0;                   // tile buffers of one lane
     void* d_tile = nullptr;      // lanes x (tile buffer 0, and 1 for pull)
     RoundState* d_rs = nullptr;
     RoundState h_rs{};
@@ -175,18 +176,18 @@ struct TileLauncher {
         const TileArgs<S, R> base = base_args();
         if (ts->lanes > 1) {
             CULBM_CUDA(cudaEventRecord(ts->ev_fork, s->stream));
-            CULBM_CUDA(cudaStreamWaitEvent(ts->side, ts->ev_fork, 0));
+            for (int l = 1; l < ts->lanes; ++l) CULBM_CUDA(cudaStreamWaitEvent(ts->side[l], ts->ev_fork, 0));
         }
         for (size_t ti = 0; ti < ts->tiles.size(); ++ti) {
             const TileGeom& g = ts->tiles[ti];
             const int lane = static_cast<int>(ti % static_cast<size_t>(ts->lanes));
-            const cudaStream_t st = lane ? ts->side : s->stream;
+            const cudaStream_t st = lane ? ts->side[lane] : s->stream;
             TileArgs<S, R> a = base;
             if (lane) {
-                S* t = reinterpret_cast<S*>(static_cast<char*>(ts->d_tile) + ts->lane_bytes);
+                S* t = reinterpret_cast<S*>(static_cast<char*>(ts->d_tile) + lane * ts->lane_bytes);
                 a.t0.set(t, ts->tile_n);
                 a.t1.set(t + 27 * ts->tile_n, ts->tile_n);
-                a.edge = static_cast<S*>(ts->d_edge1);
+                a.edge = static_cast<S*>(ts->d_edge_lane[lane]);
             }
             a.ox = g.org[0];
             a.oy = g.org[1];
@@ -234,9 +235,9 @@ struct TileLauncher {
                                : launch(k_tile_pull_last<S, R, false>, a, g, 0, st));
             }
         }
-        if (ts->lanes > 1) {
-            CULBM_CUDA(cudaEventRecord(ts->ev_join, ts->side));
-            CULBM_CUDA(cudaStreamWaitEvent(s->stream, ts->ev_join, 0));
+        for (int l = 1; l < ts->lanes; ++l) {
+            CULBM_CUDA(cudaEventRecord(ts->ev_join[l], ts->side[l]));
+            CULBM_CUDA(cudaStreamWaitEvent(s->stream, ts->ev_join[l], 0));
         }
         k_tile_advance<<<1, 32, 0, s->stream>>>(ts->d_rs, ts->ring_nz, ts->ring_step, k);
         CULBM_CUDA(cudaGetLastError());
@@ -368,20 +369,22 @@ culbm_status tiles_create(culbm_sim* s)
     const bool inplace = c.stream_policy == CULBM_STREAM_INPLACE;
     ts->lane_bytes = ((inplace ? 1 : 2) * 27ull * ts->tile_n * s->esize + 255) / 256 * 256;
     {
-        // a second lane only when both lanes' tile buffers stay well inside L2
         int l2 = 0;
         CULBM_CUDA(cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, s->dev));
-        const bool fits = kTileLanes * ts->lane_bytes <= static_cast<size_t>(0.7 * static_cast<double>(l2));
-        ts->lanes = (!c.use_ring_ddf_buf && ts->tiles.size() > 1 && fits) ? kTileLanes : 1;
+        const int want = static_cast<int>(std::min<size_t>(kTileLanes, ts->tiles.size()));
+        const bool fits = want * ts->lane_bytes <= static_cast<size_t>(0.7 * static_cast<double>(l2));
+        ts->lanes = (!c.use_ring_ddf_buf && (!c.persist_l2 || fits)) ? std::max(want, 1) : 1;
     }
     const size_t tile_bytes = ts->lanes * ts->lane_bytes;
     void* p = nullptr;
     CULBM_TRY(dev_alloc(s, &p, tile_bytes, "tile buffers"));
     ts->d_tile = p;
     if (ts->lanes > 1) {
-        CULBM_CUDA(cudaStreamCreateWithFlags(&ts->side, cudaStreamNonBlocking));
         CULBM_CUDA(cudaEventCreateWithFlags(&ts->ev_fork, cudaEventDisableTiming));
-        CULBM_CUDA(cudaEventCreateWithFlags(&ts->ev_join, cudaEventDisableTiming));
+        for (int l = 1; l < ts->lanes; ++l) {
+            CULBM_CUDA(cudaStreamCreateWithFlags(&ts->side[l], cudaStreamNonBlocking));
+            CULBM_CUDA(cudaEventCreateWithFlags(&ts->ev_join[l], cudaEventDisableTiming));
+        }
     }
     CULBM_TRY(dev_alloc(s, &p, sizeof(RoundState), "round state"));
     ts->d_rs = static_cast<RoundState*>(p);
@@ -422,7 +425,8 @@ culbm_status tiles_create(culbm_sim* s)
         s->el.off[5] = 2 * fx + 2 * fy + fz;
         s->edge_elems = 2 * (fx + fy + fz);
         CULBM_TRY(dev_alloc(s, &s->d_edge, s->edge_elems * s->esize, "edge buffer"));
-        if (ts->lanes > 1) CULBM_TRY(dev_alloc(s, &ts->d_edge1, s->edge_elems * s->esize, "lane edge buffer"));
+        for (int l = 1; l < ts->lanes; ++l)
+            CULBM_TRY(dev_alloc(s, &ts->d_edge_lane[l], s->edge_elems * s->esize, "lane edge buffer"));
     }
 
     // Keep the tile buffers resident: persisting set-aside + access-policy
@@ -454,10 +458,12 @@ void tiles_destroy(culbm_sim* s)
     if (ts->graph) cudaGraphExecDestroy(ts->graph);
     cudaFree(ts->d_tile);
     cudaFree(ts->d_rs);
-    cudaFree(ts->d_edge1);
-    if (ts->side) cudaStreamDestroy(ts->side);
+    for (int l = 1; l < kTileLanes; ++l) {
+        cudaFree(ts->d_edge_lane[l]);
+        if (ts->side[l]) cudaStreamDestroy(ts->side[l]);
+        if (ts->ev_join[l]) cudaEventDestroy(ts->ev_join[l]);
+    }
     if (ts->ev_fork) cudaEventDestroy(ts->ev_fork);
-    if (ts->ev_join) cudaEventDestroy(ts->ev_join);
     if (ts->window) {
         cudaCtxResetPersistingL2Cache();
         cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, 0);

@@ -33,7 +33,7 @@ class Simulation:
                  inv_tau: float = 0.5, inner_loop: int = 5, storage: str = "fp32",
                  block_dim: Optional[Sequence[int]] = None, grid_dim: Optional[Sequence[int]] = None,
                  tile: Optional[Sequence[int]] = None, use_ring: bool = False, dev_id: int = 0,
-                 persist_l2: bool = True, cache_hints: bool = True, use_graphs: bool = True,
+                 persist_l2: bool = False, cache_hints: bool = True, use_graphs: bool = True,
                  kernel_variant: int = 0):
         cfg = _capi.default_config()
         cfg.dev_id = dev_id

@@ -99,8 +99,9 @@ typedef struct culbm_config {
     int32_t use_ring_ddf_buf;  /* --useRingDDFBuf */
     /* additions */
     int32_t storage;           /* culbm_storage, default F32 */
-    int32_t persist_l2;        /* 1 (default): L2 persisting window over tile buffers
-                                  (reference build switch CULBM_EXPT_ENABLE_PERSISTENT_L2) */
+    int32_t persist_l2;        /* 1: L2 persisting window over tile buffers (reference build
+                                  switch CULBM_EXPT_ENABLE_PERSISTENT_L2, on in its default
+                                  build); 0 (default): none, which is faster on B200 */
     int32_t cache_hints;       /* 1 (default): evict-first/evict-last hints on global/tile traffic
                                   (reference build switch CULBM_EXPT_CACHE_HINT_POLICY) */
     int32_t use_graphs;        /* 1 (default): tile launch sequences replayed as CUDA graphs */

@@ -26,9 +26,9 @@ def oracle_pulled(orc, scene, inv_tau, nsteps, state0=None, dtype=np.float32):
 
 
 def run_blocked(culbm, scene, sp, op, tile, inner, nsteps, inv_tau=0.6, ring=False, state0=None, storage="fp32",
-                graphs=True, splits=None):
+                graphs=True, splits=None, persist=False):
     with culbm.Simulation(scene.shape, stream_policy=sp, opt_policy=op, inv_tau=inv_tau, inner_loop=inner,
-                          tile=tile, use_ring=ring, storage=storage, use_graphs=graphs) as sim:
+                          tile=tile, use_ring=ring, storage=storage, use_graphs=graphs, persist_l2=persist) as sim:
         sim.load_state(*scene.arrays())
         if state0 is not None:
             sim.set_ddf(state0)
@@ -79,6 +79,24 @@ def test_blocked_graphs_off_and_split_steps(culbm, orc):
     for graphs, splits in ((False, [13]), (True, [4, 9]), (True, [1, 1, 11])):
         got, _ = run_blocked(culbm, sc, 1, 3, (16, 12, 10), 3, 13, inv_tau=0.5, graphs=graphs, splits=splits)
         assert np.array_equal(bits(got), bits(want)), (graphs, splits)
+
+
+@pytest.mark.parametrize("sp", [1, 0])
+def test_blocked_tile_lanes_and_persisting_window(culbm, orc, sp):
+    """Tiles of a round run on two streams (each with its own tile and edge
+    buffers) unless the ring buffer is on; with the persisting-L2 window they
+    do so only when both lanes' buffers fit in L2.  An odd tile count leaves
+    the lanes uneven.  Every combination gives the plain pull's bits."""
+    sc = S.reference_channel_cube(45, 30, 26, 0.05)
+    want = oracle_pulled(orc, sc, 0.5, 8)
+    for persist in (False, True):
+        for graphs in (True, False):
+            got, info = run_blocked(culbm, sc, sp, 3, (18, 14, 12), 3, 8, inv_tau=0.5, graphs=graphs,
+                                    persist=persist)
+            assert np.array_equal(bits(got), bits(want)), (persist, graphs)
+            if not persist:
+                assert info["persisting_l2_bytes"] == 0
+        assert info["blocking_num"][0] * info["blocking_num"][1] * info["blocking_num"][2] % 2 == 1
 
 
 def test_blocked_fp64_and_moments(culbm, orc):
