@@ -84,6 +84,7 @@ struct TileState {
     long long gstride = 0;
     cudaGraphExec_t graph = nullptr;
     int graph_I = 0;
+    uint64_t graph_launches = 0;     // kernel launches in the captured round
     bool window = false;
     cudaAccessPolicyWindow apw{};
     size_t persist_bytes = 0;
@@ -285,9 +286,10 @@ culbm_status tiles_step_typed(culbm_sim* s, uint32_t nsteps)
             cudaGraphDestroy(g);
             if (ie != cudaSuccess) return cuda_fail(ie, "cudaGraphInstantiate", __FILE__, __LINE__);
             ts->graph_I = ts->I;
+            ts->graph_launches = s->launches - launches0;
             s->launches = launches0;
         }
-        const uint64_t per_round = ts->tiles.size() * static_cast<uint64_t>(ts->I) + 1;
+        const uint64_t per_round = ts->graph_launches;
         for (uint32_t r = 0; r < full; ++r) {
             CULBM_CUDA(cudaGraphLaunch(ts->graph, s->stream));
             s->launches += per_round;
