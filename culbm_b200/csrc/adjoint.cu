@@ -6,8 +6,11 @@
 //     f1 = EQU ? feq(rho_in, u_in) : f          (f pulled from the state)
 //     f2 = BOUNCE_BACK ? B(f1) : f1              (B(g)_d = g_{26-d})
 //     f3 = COLLIDE ? C(f2) + s (B(f2) - C(f2)) : f2,   C = BGK with rate w = invTau
-// stored back for every STORE cell.  With s = 0 this is the plain step bit
-// for bit (the soft term is skipped, not multiplied by zero).
+// stored back for every STORE cell.  With s = 0 and FP32 or FP64 storage
+// this is the plain step bit for bit (the soft term is skipped, not
+// multiplied by zero).  With a 16-bit storage format the cell arithmetic is
+// still the reference-order FP32 update, not the compact form the plain
+// 16-bit step uses; loads and stores round as the plain step does.
 //
 // Adjoint step (reverse time, one thread per cell s):
 //   * gather: lambda_d(s) = sum of nu_d(y) over the cells y whose pull of
