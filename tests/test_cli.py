@@ -55,3 +55,12 @@ def test_vector_syntaxes_accepted(form):
     r = run(*form, "--blockDim", "[8,8,8]", "--gridDim", "[1,1,1]")
     assert r.returncode == 1
     assert "Dimension of domain doesn't match computation grid!" in r.stderr
+
+
+@pytest.mark.parametrize("flag", ["--persistL2", "--noPersistL2", "--noCacheHints", "--noGraphs"])
+def test_addition_flags_parse(flag):
+    # Accepted flags reach the geometry check, which stops the run before the device.
+    r = run(flag, "--domainDim", "[64,48,40]", "--blockDim", "[8,8,8]", "--gridDim", "[1,1,1]")
+    assert r.returncode == 1, (r.returncode, r.stderr)
+    assert "Dimension of domain doesn't match computation grid!" in r.stderr
+    assert "--persistL2" in run("--help").stdout
