@@ -114,3 +114,35 @@ def test_blocked_fp64_and_moments(culbm, orc):
             sim.moments()
             for k, w in zip(("rho", "vx", "vy", "vz"), want):
                 assert np.array_equal(bits(sim.field(k)), bits(w)), (ring, k)
+
+
+def _valid_axis(dom, blk, it):
+    """blocking_core::validBlkAxisConfig and the engine's extra check (the
+    tile must be large enough for innerLoop when more than two are needed)."""
+    if blk < dom and blk + 1 <= it:
+        return False
+    if 2 * (blk + 1 - it) < dom and blk + 2 <= it:
+        return False
+    if dom > blk and dom > 2 * (blk + 1 - it) and blk + 2 - 2 * it <= 0:
+        return False
+    return True
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_blocked_random_geometries(culbm, orc, seed):
+    """Seeded random domains, tile extents and innerLoops with several tiles
+    per axis (two concurrent tile lanes), in-place and pull tiles, graphs on
+    and off, against the oracle's pull bit for bit."""
+    rng = np.random.default_rng(1000 + seed)
+    while True:
+        dims = tuple(int(v) for v in rng.integers(14, 41, size=3))
+        inner = int(rng.integers(2, 6))
+        tile = tuple(int(rng.integers(max(2 * inner, 6), max(2 * inner + 1, d // 2 + 3))) for d in dims)
+        if all(_valid_axis(d, b, inner) for d, b in zip(dims, tile)):
+            break
+    sc = S.reference_channel_cube(*dims, 0.05)
+    nsteps = 2 * inner + int(rng.integers(0, inner))
+    want = oracle_pulled(orc, sc, 0.6, nsteps)
+    for sp in (1, 0):
+        got, info = run_blocked(culbm, sc, sp, 3, tile, inner, nsteps, graphs=bool(seed % 2))
+        assert np.array_equal(bits(got), bits(want)), (dims, tile, inner, sp)
