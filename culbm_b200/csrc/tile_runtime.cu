@@ -1,5 +1,6 @@
 // Host side of the blocked policies (optPolicy 1, 2, 3): tile geometry, tile
-// buffers kept in L2 by an access-policy window, the per-round launch
+// buffers per lane (tiles of a round run on two streams), the optional
+// persisting-L2 access-policy window over them, the per-round launch
 // sequence (replayed as one CUDA graph), and the ring-buffer option.
 //
 // Replaces the reference's haloBlocking*Run lambdas and initBlockingFlag /
