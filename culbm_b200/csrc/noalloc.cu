@@ -2,7 +2,10 @@
 // culbm_mass_momentum (sim.cu, k_mass_momentum + k_sum_partials) over a
 // caller-owned FP32 population buffer, with its block partial sums in a
 // fixed file-scope device array instead of memory from cudaMalloc.  No
-// reference counterpart.
+// reference counterpart.  It is for callers that must not allocate device
+// memory: a framework process (PyTorch, say) whose device memory belongs to
+// its caching allocator, where cudaMalloc would take memory behind the
+// allocator's back and cudaMalloc/cudaFree synchronise the device.
 //
 // Work split: thread block b covers cells [b * kCellsPerBlock, (b + 1) *
 // kCellsPerBlock), thread t of it the cells b * kCellsPerBlock + t + 256 k.

@@ -208,9 +208,18 @@ culbm_status culbm_mass_momentum(culbm_sim* sim, double out[4]);
  * Runs on the current device and on `stream` (a cudaStream_t; NULL is the
  * legacy default stream) and blocks until out is written.
  *
+ * For callers that keep the populations in their own device memory and must
+ * not allocate: a PyTorch (or other framework) process whose device memory
+ * belongs to its caching allocator, or code inside a memory budget it does
+ * not control.  There, cudaMalloc would take memory behind the allocator's
+ * back, and cudaMalloc/cudaFree synchronise the whole device; a culbm_sim
+ * would also hold a second copy of the state.
+ *
  * Allocates nothing: the block partial sums live in a fixed 37,920-byte
  * static device array, so n may not exceed CULBM_NOALLOC_MAX_CELLS
- * (CULBM_ERR_INVALID_ARGUMENT beyond it).  The first call on a device looks
+ * (CULBM_ERR_INVALID_ARGUMENT beyond it).  Every GPU that loads the library
+ * holds that array until the process exits, and it keeps the last call's
+ * contents (each call writes every slot it reads).  The first call on a device looks
  * up that array's address with the device current (cudaGetSymbolAddress);
  * make that first call before any stream capture.  Calls that overlap on the
  * GPU (other streams or host threads, same device) share the array and

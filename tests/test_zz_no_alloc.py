@@ -1,7 +1,10 @@
 """culbm_mass_momentum_noalloc: the FP64 mass/momentum reduction over a
 caller-owned device population buffer, with its scratch in a fixed static
-device array (no device allocation).  Collected last so that it also runs
-after every other test has used the library on the same device."""
+device array (no device allocation).  It serves callers that must not
+allocate device memory themselves, such as a PyTorch process whose memory
+belongs to the caching allocator (cudaMalloc would bypass it, and
+cudaMalloc/cudaFree synchronise the device).  Collected last so that it also
+runs after every other test has used the library on the same device."""
 import ctypes as C
 
 import numpy as np
