@@ -33,7 +33,7 @@ EXPORTED = (
     "culbm_config_init", "culbm_create", "culbm_destroy", "culbm_load_state", "culbm_load_state_folder",
     "culbm_step", "culbm_step_timed", "culbm_synchronize", "culbm_moments", "culbm_get_field", "culbm_dump",
     "culbm_get_step", "culbm_get_pulled_ddf", "culbm_set_ddf", "culbm_mass_momentum", "culbm_mass_momentum_noalloc", "culbm_measure_memory",
-    "culbm_select_tile", "culbm_blocking_speedup", "culbm_get_info",
+    "culbm_select_tile", "culbm_blocking_speedup", "culbm_blocking_axis", "culbm_get_info",
     "culbm_last_error", "culbm_status_string", "culbm_abi_version", "culbm_debug_inject_cuda_error",
     "culbm_adj_config_init", "culbm_adj_create", "culbm_adj_destroy", "culbm_adj_set_state",
     "culbm_adj_set_inv_tau", "culbm_adj_forward", "culbm_adj_gradient", "culbm_adj_get_info",
@@ -171,6 +171,8 @@ def lib():
                                     C.c_uint64, C.POINTER(TileChoice)]
     L.culbm_blocking_speedup.argtypes = [C.POINTER(C.c_uint32), C.c_int32, C.c_int32, C.c_double, C.c_double,
                                          C.c_uint64, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    L.culbm_blocking_axis.argtypes = [C.c_uint32, C.c_uint32, C.c_int32, C.POINTER(C.c_uint32),
+                                      C.POINTER(C.c_int32), C.c_uint32]
     L.culbm_get_info.argtypes = [vp, C.POINTER(Info)]
     L.culbm_last_error.restype = C.c_char_p
     L.culbm_status_string.restype = C.c_char_p

@@ -324,22 +324,28 @@ __global__ void k_fill_dirs(S* base, long long stride, typename ArithOf<S>::type
 
 }  // namespace
 
+// One axis of a blocked geometry: tile extent b (blockDim*gridDim) over
+// domain extent dom with innerLoop I >= 1.
+static culbm_status validate_axis(uint32_t dom, unsigned long long b, uint32_t I)
+{
+    if (b > 65535) return fail(CULBM_ERR_INVALID_ARGUMENT, "tile extent blockDim*gridDim above 65535");
+    const uint32_t B = static_cast<uint32_t>(b);
+    if (!valid_blk_axis(dom, B, I))
+        return fail(CULBM_ERR_INVALID_ARGUMENT, "<Domain Dimension, Blocking Dimension and InnerLoop> don't match!");
+    // The reference's check lets B + 2 - 2I <= 0 through when more than
+    // two tiles are needed, and calcBlkNum then divides by it.
+    if (dom > B && dom > 2 * (B + 1 - I) && static_cast<long long>(B) + 2 - 2ll * I <= 0)
+        return fail(CULBM_ERR_INVALID_ARGUMENT,
+                    "<Domain Dimension, Blocking Dimension and InnerLoop> don't match! (tile too small for innerLoop)");
+    return CULBM_OK;
+}
+
 culbm_status validate_blocking(const culbm_config& c)
 {
     if (c.inner_loop < 1) return fail(CULBM_ERR_INVALID_ARGUMENT, "innerLoop must be at least 1");
     const uint32_t I = static_cast<uint32_t>(c.inner_loop);
-    for (int k = 0; k < 3; ++k) {
-        const unsigned long long b = 1ull * c.block_dim[k] * c.grid_dim[k];
-        if (b > 65535) return fail(CULBM_ERR_INVALID_ARGUMENT, "tile extent blockDim*gridDim above 65535");
-        const uint32_t dom = c.domain_dim[k], B = static_cast<uint32_t>(b);
-        if (!valid_blk_axis(dom, B, I))
-            return fail(CULBM_ERR_INVALID_ARGUMENT, "<Domain Dimension, Blocking Dimension and InnerLoop> don't match!");
-        // The reference's check lets B + 2 - 2I <= 0 through when more than
-        // two tiles are needed, and calcBlkNum then divides by it.
-        if (dom > B && dom > 2 * (B + 1 - I) && static_cast<long long>(B) + 2 - 2ll * I <= 0)
-            return fail(CULBM_ERR_INVALID_ARGUMENT,
-                        "<Domain Dimension, Blocking Dimension and InnerLoop> don't match! (tile too small for innerLoop)");
-    }
+    for (int k = 0; k < 3; ++k)
+        CULBM_TRY(validate_axis(c.domain_dim[k], 1ull * c.block_dim[k] * c.grid_dim[k], I));
     if (c.use_ring_ddf_buf && 1ull * c.block_dim[2] * c.grid_dim[2] < I)
         return fail(CULBM_ERR_INVALID_ARGUMENT, "ring buffer needs blockDim.z*gridDim.z >= innerLoop");
     return CULBM_OK;
@@ -522,3 +528,24 @@ void tiles_info(const culbm_sim* s, culbm_info* info)
 }
 
 }  // namespace culbm
+
+extern "C" culbm_status culbm_blocking_axis(uint32_t domain, uint32_t tile, int32_t inner_loop, uint32_t* num_tiles,
+                                            int32_t* valid_starts, uint32_t capacity)
+{
+    using namespace culbm;
+    if (num_tiles == nullptr) return fail(CULBM_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (inner_loop < 1) return fail(CULBM_ERR_INVALID_ARGUMENT, "innerLoop must be at least 1");
+    if (domain < 1 || domain > 0x7FFFFFFFu || tile < 1)
+        return fail(CULBM_ERR_INVALID_ARGUMENT, "domain and tile extents must be in [1, 2^31)");
+    const uint32_t I = static_cast<uint32_t>(inner_loop);
+    CULBM_TRY(validate_axis(domain, tile, I));
+    const uint32_t num = blk_num(domain, tile, I);
+    *num_tiles = num;
+    if (valid_starts == nullptr) return CULBM_OK;
+    if (capacity < num + 1ull)
+        return fail(CULBM_ERR_INVALID_ARGUMENT, "valid_starts needs " + std::to_string(num + 1ull) + " entries");
+    for (uint32_t k = 0; k <= num; ++k)
+        valid_starts[k] = valid_prev(static_cast<int32_t>(k), static_cast<int32_t>(tile), static_cast<int32_t>(num),
+                                     inner_loop, static_cast<int32_t>(domain));
+    return CULBM_OK;
+}

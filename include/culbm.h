@@ -276,6 +276,21 @@ culbm_status culbm_select_tile(const uint32_t domain_dim[3], int32_t storage, do
 culbm_status culbm_blocking_speedup(const uint32_t tile[3], int32_t inner_loop, int32_t storage, double lambda,
                                     double gamma, uint64_t l2_bytes, double* speedup, double* speedup_no_alignment);
 
+/*
+ * Tile geometry of one axis under the blocked policies, as the blocking
+ * engine computes it: replaces blocking_core::validBlkAxisConfig, calcBlkNum
+ * and calcValidPrev (src/blocking_core/blocking_alogrithm.hpp:7-41).  For a
+ * domain extent `domain`, tile extent `tile` (blockDim*gridDim) and
+ * `inner_loop`, writes the tile count to *num_tiles and, when `valid_starts`
+ * is not NULL, the num_tiles + 1 valid-region bounds valid_starts[k] =
+ * calcValidPrev(k) (tile k stores cells [valid_starts[k], valid_starts[k+1]))
+ * into an array of `capacity` entries.  Returns CULBM_ERR_INVALID_ARGUMENT
+ * (with the message culbm_create gives) for a geometry culbm_create rejects,
+ * and when the bounds do not fit in `capacity`.  Host only; no device needed.
+ */
+culbm_status culbm_blocking_axis(uint32_t domain, uint32_t tile, int32_t inner_loop, uint32_t* num_tiles,
+                                 int32_t* valid_starts, uint32_t capacity);
+
 typedef struct culbm_info {
     uint64_t cells;                 /* N */
     uint64_t device_bytes;          /* bytes the library allocated on the device */

@@ -138,3 +138,59 @@ def test_adjoint_config_rejected_before_the_device(culbm, mutate, needle):
     st = _capi.lib().culbm_adj_create(C.byref(cfg), C.byref(h))
     assert st != 0 and not h.value
     assert needle in _capi.lib().culbm_last_error().decode()
+
+
+def test_blocking_axis_matches_the_reference_geometry(culbm, orc):
+    """culbm_blocking_axis (the blocking engine's own geometry) against the
+    reference's blocking_core compiled for the host (when oracle/_ref is
+    built) and the oracle's restatement: same accept/reject decision as
+    culbm_create, same tile count, same valid-region bounds."""
+    from culbm_b200 import _capi
+    lib = _capi.lib()
+    L = orc.lib()
+    R = orc.ref() if orc.ref_available() else None
+    cap = 4096
+    starts = (C.c_int32 * cap)()
+    num = C.c_uint32()
+    checked = 0
+    for dom in (1, 2, 7, 13, 64, 96, 280, 288, 384, 768, 1000):
+        for blk in (1, 2, 3, 4, 7, 16, 36, 64, 76, 96, 128, 160, 288):
+            for it in (1, 2, 3, 4, 5, 9):
+                st = lib.culbm_blocking_axis(dom, blk, it, C.byref(num), starts, cap)
+                ok = bool(L.orc_valid_blk_axis(dom, blk, it))
+                if R is not None:
+                    assert ok == bool(R.ref_valid_blk_axis(dom, blk, it)), (dom, blk, it)
+                # Admitted by validBlkAxisConfig but rejected here: calcBlkNum
+                # would divide by blk + 2 - 2*it <= 0.
+                degenerate = dom > blk and dom > 2 * (blk + 1 - it) and blk + 2 - 2 * it <= 0
+                if not ok or degenerate:
+                    assert st == 1, (dom, blk, it)
+                    assert "don't match" in lib.culbm_last_error().decode()
+                    continue
+                assert st == 0, (dom, blk, it, lib.culbm_last_error().decode())
+                n = num.value
+                assert n == L.orc_blk_num(dom, blk, it)
+                got = list(starts[:n + 1])
+                assert got == [L.orc_valid_prev(k, blk, n, it, dom) for k in range(n + 1)]
+                if R is not None:
+                    assert n == R.ref_blk_num(dom, blk, it)
+                    assert got == [R.ref_valid_prev(k, blk, n, it, dom) for k in range(n + 1)]
+                assert got[0] == 0 and got[-1] == dom and all(b > a for a, b in zip(got, got[1:]))
+                checked += 1
+    assert checked > 300
+
+
+def test_blocking_axis_argument_errors(culbm):
+    from culbm_b200 import _capi
+    lib = _capi.lib()
+    num = C.c_uint32()
+    small = (C.c_int32 * 2)()
+    assert lib.culbm_blocking_axis(288, 64, 5, None, None, 0) == 1
+    assert lib.culbm_blocking_axis(288, 64, 0, C.byref(num), None, 0) == 1
+    assert "innerLoop" in lib.culbm_last_error().decode()
+    assert lib.culbm_blocking_axis(0, 64, 5, C.byref(num), None, 0) == 1
+    assert lib.culbm_blocking_axis(288, 70000, 5, C.byref(num), None, 0) == 1
+    assert "65535" in lib.culbm_last_error().decode()
+    assert lib.culbm_blocking_axis(288, 64, 5, C.byref(num), None, 0) == 0 and num.value == 5
+    assert lib.culbm_blocking_axis(288, 64, 5, C.byref(num), small, 2) == 1
+    assert "6 entries" in lib.culbm_last_error().decode()
