@@ -1,0 +1,51 @@
+"""The reference arm of the benchmark (``bench.py --impl reference``) on the
+CPU: the reference's own lbm_core step compiled for the host, timed on the
+same 288x272x280 workload and metric as the CUDA arm, one JSON line from
+rank 0, nothing from the other ranks."""
+import json
+import os
+import subprocess
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _bench(args, **env):
+    e = dict(os.environ)
+    e.update({k: str(v) for k, v in env.items()})
+    return subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), *args], cwd=ROOT, env=e,
+                          capture_output=True, text=True, timeout=600)
+
+
+def test_reference_arm_prints_one_contract_line(orc):
+    if not orc.ref_available():
+        pytest.skip("oracle/_ref not built (make -C oracle ref-cpu)")
+    sys.path.insert(0, ROOT)
+    import bench
+    r = _bench(["--impl", "reference", "--steps", "3", "--warmup", "3"], WORLD_SIZE=1, RANK=0)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1
+    line = json.loads(lines[0])
+    assert line["impl"] == "reference"
+    assert line["metric"] == bench.METRIC and line["unit"] == "MLUPS" and line["higher_is_better"] is True
+    assert line["n_gpus"] == 1 and line["steps"] == 3 and line["warmup"] == 3
+    assert line["value"] > 0 and line["ms_per_step"] > 0
+    assert line["config"]["workload"] == bench.WORKLOAD and line["config"]["cells"] == 288 * 272 * 280
+    cb = line["cpu_baseline"]
+    assert cb["kind"] == "reference" and cb["value"] == line["value"] and cb["cores"] >= 1 and cb["sample"]
+    assert line["e2e"] == {"value": line["value"], "unit": "MLUPS", "h2d_bytes_per_step": 0,
+                           "d2h_bytes_per_step": 0}
+
+
+def test_reference_arm_other_ranks_exit_quietly():
+    r = _bench(["--impl", "reference", "--gpus", "2", "--steps", "3", "--warmup", "3"], WORLD_SIZE=2, RANK=1)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert r.stdout.strip() == ""
+
+
+def test_fewer_than_three_warmup_steps_rejected():
+    r = _bench(["--impl", "reference", "--steps", "3", "--warmup", "2"], WORLD_SIZE=1, RANK=0)
+    assert r.returncode == 2 and "warmup" in r.stderr
