@@ -1,7 +1,8 @@
-"""The reference arm of the benchmark (``bench.py --impl reference``) on the
-CPU: the reference's own lbm_core step compiled for the host, timed on the
-same 288x272x280 workload and metric as the CUDA arm, one JSON line from
-rank 0, nothing from the other ranks."""
+"""Host logic of the benchmark on the CPU.  The reference arm (``bench.py
+--impl reference``): the reference's own lbm_core step compiled for the host,
+timed on the same 288x272x280 workload and metric as the CUDA arm, one JSON
+line from rank 0, nothing from the other ranks.  The clock summary and the
+roofline's traffic figure of the CUDA arm."""
 import json
 import os
 import subprocess
@@ -49,3 +50,25 @@ def test_reference_arm_other_ranks_exit_quietly():
 def test_fewer_than_three_warmup_steps_rejected():
     r = _bench(["--impl", "reference", "--steps", "3", "--warmup", "2"], WORLD_SIZE=1, RANK=0)
     assert r.returncode == 2 and "warmup" in r.stderr
+
+
+def test_clock_summary_names_throttle_reasons():
+    sys.path.insert(0, ROOT)
+    import bench
+    c = bench.ClockSampler()
+    assert c.summary()["reasons"] == ["no samples"]
+    c.max_mhz = 1965
+    c.samples = [(1965.0, 0), (1800.0, 0x4), (1700.0, 0x4 | 0x8), (1965.0, 0x40)]
+    s = c.summary()
+    assert s["sm_mhz"] == 1882.5 and s["sm_max_mhz"] == 1965 and s["samples"] == 4
+    assert s["reasons"] == ["hw_slowdown", "hw_thermal_slowdown", "sw_power_cap"]
+
+
+def test_roofline_traffic_is_the_committed_profile():
+    sys.path.insert(0, ROOT)
+    import bench
+    with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+        d = json.load(f)["inplace_fp32_per_step"]
+    assert bench.traffic_from_profiles("inplace_fp32_per_step") == d["bytes"]
+    assert d["algorithmic_bytes"] == 216 * 288 * 272 * 280
+    assert bench.traffic_from_profiles("no such kernel") is None
