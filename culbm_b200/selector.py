@@ -48,6 +48,18 @@ def speedup(tile: Sequence[int], inner_loop: int, storage: str = "fp32", lam: fl
     return s.value, s0.value
 
 
+def blocking_axis(domain: int, tile: int, inner_loop: int) -> list:
+    """Valid-region bounds of the tiles along one axis, [0, ..., domain]
+    (tile k stores cells [b[k], b[k+1])), as the blocking engine computes
+    them (``culbm_blocking_axis``: blocking_core's calcBlkNum and
+    calcValidPrev).  Raises CulbmError for a geometry culbm_create rejects."""
+    num = C.c_uint32()
+    check(lib().culbm_blocking_axis(int(domain), int(tile), int(inner_loop), C.byref(num), None, 0))
+    starts = (C.c_int32 * (num.value + 1))()
+    check(lib().culbm_blocking_axis(int(domain), int(tile), int(inner_loop), C.byref(num), starts, num.value + 1))
+    return list(starts)
+
+
 def main(argv: Optional[Sequence[str]] = None) -> int:
     import argparse
     import json
@@ -66,6 +78,8 @@ def main(argv: Optional[Sequence[str]] = None) -> int:
         lam, gam = out["measured"]["lambda"], out["measured"]["gamma"]
     out["choice"] = select(args.domain, args.storage, lam, gam)
     t = out["choice"]["tile"]
+    out["tiles_per_axis"] = [len(blocking_axis(d, b, out["choice"]["inner_loop"])) - 1
+                             for d, b in zip(args.domain, t)]
     out["cli"] = (f"--blockDim [{t[0]},{t[1]},{t[2]}] --gridDim [1,1,1] --innerLoop {out['choice']['inner_loop']} "
                   f"--streamPolicy 1 --optPolicy 3")
     print(json.dumps(out))

@@ -51,3 +51,13 @@ def test_choice_respects_the_domain_and_storage(culbm):
         assert L.orc_valid_blk_axis(dom, small["tile"][k], small["inner_loop"])
     with pytest.raises(CulbmError):
         selector.select((4096, 4096, 4096), "fp32", c["lambda"], c["gamma"], c["l2_bytes"], 1000)
+
+
+def test_blocking_axis_bounds(culbm):
+    from culbm_b200 import _capi, selector
+    # 288 cells, tile 64, innerLoop 5: first valid region 64 + 1 - 5 = 60
+    # cells, then 64 + 2 - 10 = 56 per tile, the last tile takes the rest.
+    assert selector.blocking_axis(288, 64, 5) == [0, 60, 116, 172, 228, 288]
+    assert selector.blocking_axis(280, 288, 3) == [0, 280]
+    with pytest.raises(_capi.CulbmError, match="don't match"):
+        selector.blocking_axis(64, 4, 3)
