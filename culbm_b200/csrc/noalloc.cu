@@ -13,6 +13,7 @@
 // the result, are the same on every device.  Every partial slot that the sum
 // kernel reads is written by the first kernel of the same call, and the sum
 // kernel writes the four result slots: nothing has to start at zero.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -33,7 +34,46 @@ static __device__ __align__(256) double g_noalloc_scratch[4 * kMaxBlocks + 4];
 
 constexpr int kMaxDevices = 64;
 std::mutex g_mutex;
-double* g_scratch_ptr[kMaxDevices] = {};
+
+// The scratch address is kept per device together with the unique ID of the
+// context it was looked up in.  A context made after cudaDeviceReset, or one
+// made with cuCtxCreate, may place the array elsewhere: its ID differs, so
+// the address is looked up again in it before any launch.
+struct ScratchAddr {
+    unsigned long long ctx_id = 0;
+    double* ptr = nullptr;
+};
+ScratchAddr g_scratch[kMaxDevices];
+
+// cuCtxGetCurrent / cuCtxGetId through the runtime's driver entry points, so
+// the library needs no link against libcuda.
+using PfnCtxGetCurrent = CUresult (*)(CUcontext*);
+using PfnCtxGetId = CUresult (*)(CUcontext, unsigned long long*);
+PfnCtxGetCurrent g_ctx_get_current = nullptr;
+PfnCtxGetId g_ctx_get_id = nullptr;
+
+// ID of the context current on this thread; 0 when none is current yet.
+culbm_status current_context_id(unsigned long long* id)
+{
+    if (g_ctx_get_current == nullptr || g_ctx_get_id == nullptr) {
+        void* fc = nullptr;
+        void* fi = nullptr;
+        cudaDriverEntryPointQueryResult qc{}, qi{};
+        CULBM_CUDA(cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &fc, 12000, cudaEnableDefault, &qc));
+        CULBM_CUDA(cudaGetDriverEntryPointByVersion("cuCtxGetId", &fi, 12000, cudaEnableDefault, &qi));
+        if (qc != cudaDriverEntryPointSuccess || qi != cudaDriverEntryPointSuccess || !fc || !fi)
+            return culbm::fail(CULBM_ERR_CUDA, "culbm_mass_momentum_noalloc: driver lacks cuCtxGetId");
+        g_ctx_get_current = reinterpret_cast<PfnCtxGetCurrent>(fc);
+        g_ctx_get_id = reinterpret_cast<PfnCtxGetId>(fi);
+    }
+    CUcontext ctx = nullptr;
+    if (g_ctx_get_current(&ctx) != CUDA_SUCCESS)
+        return culbm::fail(CULBM_ERR_CUDA, "culbm_mass_momentum_noalloc: cuCtxGetCurrent failed");
+    *id = 0;
+    if (ctx != nullptr && g_ctx_get_id(ctx, id) != CUDA_SUCCESS)
+        return culbm::fail(CULBM_ERR_CUDA, "culbm_mass_momentum_noalloc: cuCtxGetId failed");
+    return CULBM_OK;
+}
 
 __global__ void __launch_bounds__(kThreads) k_mass_momentum_noalloc(const float* ddf, long long n, double* partial)
 {
@@ -76,8 +116,9 @@ __global__ void k_sum_partials_noalloc(const double* partial, int nblocks, doubl
     }
 }
 
-// Device address of the scratch array on the current device, looked up once
-// per device (with that device current) and cached.
+// Device address of the scratch array in the current context: looked up
+// (cudaGetSymbolAddress, with the device current) on the first call in each
+// context, then reused while that context stays current.
 culbm_status scratch_on_current_device(double** out)
 {
     int dev = 0;
@@ -86,12 +127,17 @@ culbm_status scratch_on_current_device(double** out)
         return culbm::fail(CULBM_ERR_UNSUPPORTED, "device ordinal " + std::to_string(dev) + " above " +
                                                       std::to_string(kMaxDevices - 1));
     std::lock_guard<std::mutex> lock(g_mutex);
-    if (g_scratch_ptr[dev] == nullptr) {
+    unsigned long long id = 0;
+    CULBM_TRY(current_context_id(&id));
+    if (id == 0 || g_scratch[dev].ptr == nullptr || g_scratch[dev].ctx_id != id) {
+        // Also makes the device's primary context current when none is yet.
         void* p = nullptr;
         CULBM_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
-        g_scratch_ptr[dev] = static_cast<double*>(p);
+        CULBM_TRY(current_context_id(&id));
+        g_scratch[dev].ctx_id = id;
+        g_scratch[dev].ptr = static_cast<double*>(p);
     }
-    *out = g_scratch_ptr[dev];
+    *out = g_scratch[dev].ptr;
     return CULBM_OK;
 }
 

@@ -219,13 +219,14 @@ culbm_status culbm_mass_momentum(culbm_sim* sim, double out[4]);
  * static device array, so n may not exceed CULBM_NOALLOC_MAX_CELLS
  * (CULBM_ERR_INVALID_ARGUMENT beyond it).  Every GPU that loads the library
  * holds that array until the process exits, and it keeps the last call's
- * contents (each call writes every slot it reads).  The first call on a
- * device looks up that array's address with the device current
- * (cudaGetSymbolAddress); make that first call before any stream capture.
- * The address is kept for the life of the process: do not call this entry
- * point on a device after cudaDeviceReset of that device.  Calls that
- * overlap on the GPU (other streams or host threads, same device) share the
- * array and race: serialise them.  The sum order depends on n alone.
+ * contents (each call writes every slot it reads).  The first call in each
+ * CUDA context (a device's primary context, the one made again after
+ * cudaDeviceReset, or one made with cuCtxCreate) looks up that array's
+ * address with the device current (cudaGetSymbolAddress) and keeps it for
+ * that context; make that first call before any stream capture.  Every call
+ * waits for `stream` and then copies the four results into `out`.  Calls
+ * that overlap on the GPU (other streams or host threads, same device) share
+ * the array and race: serialise them.  The sum order depends on n alone.
  */
 #define CULBM_NOALLOC_MAX_CELLS 77594624ull
 culbm_status culbm_mass_momentum_noalloc(const float* d_ddf, uint64_t n, void* stream, double out[4]);

@@ -14,7 +14,7 @@ import sys
 
 import numpy as np
 
-ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("CULBM_REFERENCE", "/root/reference")
 g = runpy.run_path(os.path.join(ref, "analysis", "selector.py"))
 
 out = {"source": "analysis/selector.py", "cell_bytes": int(g["CELL_BYTES"]), "cases": []}

@@ -57,3 +57,34 @@ def test_matches_the_sim_reduction_on_two_calls_in_a_row(culbm):
             again = (C.c_double * 4)()
             assert _call(lib, buf.data_ptr(), n, again) == 0
             assert np.array_equal(np.array(again[:]), got)
+
+
+def _numpy_sums(pops):
+    """FP64 mass and momentum of a (27, n) FP32 population array."""
+    d = np.arange(27)
+    c = np.stack([d % 3 - 1, (d // 3) % 3 - 1, d // 9 - 1]).astype(np.float64)
+    p = pops.astype(np.float64)
+    return np.array([p.shape[1] + p.sum(), *(c @ p.sum(axis=1))])
+
+
+@pytest.mark.gpu
+def test_caller_stream_and_a_smaller_call_after_a_larger_one(culbm):
+    """The caller's own stream is honoured, and a call over fewer blocks
+    after one over many reads none of the earlier call's partial sums."""
+    import torch
+    from culbm_b200 import _capi
+    lib = _capi.lib()
+    rng = np.random.default_rng(5)
+    stream = torch.cuda.Stream()
+    for n in (300_000, 1_000, 131_073):
+        pops = (0.01 * rng.standard_normal((27, n))).astype(np.float32)
+        with torch.cuda.stream(stream):
+            buf = torch.from_numpy(pops.reshape(-1)).to("cuda", non_blocking=False)
+        got = (C.c_double * 4)()
+        rc = lib.culbm_mass_momentum_noalloc(C.c_void_p(buf.data_ptr()), C.c_uint64(n),
+                                             C.c_void_p(stream.cuda_stream), got)
+        assert rc == 0, lib.culbm_last_error().decode()
+        want = _numpy_sums(pops)
+        got = np.array(got[:])
+        assert abs(got[0] - want[0]) <= 1e-12 * abs(want[0])
+        assert np.allclose(got[1:], want[1:], rtol=1e-9, atol=1e-9 * abs(want[0]))
