@@ -35,6 +35,7 @@ EXPORTED = (
     "culbm_get_step", "culbm_get_pulled_ddf", "culbm_set_ddf", "culbm_mass_momentum", "culbm_mass_momentum_noalloc", "culbm_measure_memory",
     "culbm_select_tile", "culbm_blocking_speedup", "culbm_blocking_axis", "culbm_get_info",
     "culbm_last_error", "culbm_status_string", "culbm_abi_version", "culbm_debug_inject_cuda_error",
+    "culbm_debug_row_wait_extra_bytes",
     "culbm_adj_config_init", "culbm_adj_create", "culbm_adj_destroy", "culbm_adj_set_state",
     "culbm_adj_set_inv_tau", "culbm_adj_forward", "culbm_adj_gradient", "culbm_adj_get_info",
 )
@@ -180,6 +181,8 @@ def lib():
     L.culbm_abi_version.restype = C.c_int32
     L.culbm_debug_inject_cuda_error.argtypes = [C.c_int32, C.c_int32]
     L.culbm_debug_inject_cuda_error.restype = None
+    L.culbm_debug_row_wait_extra_bytes.argtypes = [C.c_int32]
+    L.culbm_debug_row_wait_extra_bytes.restype = None
     L.culbm_adj_config_init.argtypes = [C.POINTER(AdjConfig)]
     L.culbm_adj_create.argtypes = [C.POINTER(AdjConfig), C.POINTER(vp)]
     L.culbm_adj_destroy.argtypes = [vp]

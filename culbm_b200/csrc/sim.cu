@@ -4,6 +4,7 @@
 // Replaces the reference's Simulator / Simulator::Data
 // (src/simulator/single_dev_expt/simulator_expt_platform.cu) minus argv
 // parsing, which single_dev_expt_main does on top of this ABI.
+#include <algorithm>
 #include <atomic>
 #include <cerrno>
 #include <cstdio>
@@ -14,6 +15,7 @@
 #include <type_traits>
 #include <vector>
 
+#include "row_kernels.cuh"
 #include "sim_internal.cuh"
 
 namespace culbm {
@@ -22,6 +24,7 @@ namespace {
 thread_local std::string t_last_error;
 std::atomic<int> g_inject_skip{0};
 std::atomic<int> g_inject_code{0};
+std::atomic<int> g_row_extra_tx{0};
 }  // namespace
 
 void set_last_error(const std::string& msg) { t_last_error = msg; }
@@ -221,6 +224,101 @@ culbm_status fill_rest(culbm_sim* s)
     return CULBM_OK;
 }
 
+culbm_status check_device_error(culbm_sim* s)
+{
+    if (s->err_host == nullptr) return CULBM_OK;
+    const int e = *reinterpret_cast<volatile int*>(s->err_host);
+    if (e == 0) return CULBM_OK;
+    *reinterpret_cast<volatile int*>(s->err_host) = 0;
+    return fail(CULBM_ERR_DEVICE_TIMEOUT,
+                "a bounded wait of the row-staged step kernel gave up (its bulk copies did not complete); "
+                "the state of that step is not valid");
+}
+
+// The row-staged kernels (kernel_variant 1 and 2) serve the plain policies
+// with 16-bit storage when rows are 16-byte aligned (nx a multiple of 16),
+// fit one block (nx <= 992) and, in place, the domain has inner rows.
+// Variant 1 stages two rows per block with one output buffer, variant 2
+// with two output buffers.
+bool rows_applicable(const culbm_sim* s)
+{
+    const Domain& D = s->dom;
+    if (is_blocked(s->cfg) || s->esize != 2) return false;
+    if (s->cfg.kernel_variant != 1 && s->cfg.kernel_variant != 2) return false;
+    if (D.nx % 16 != 0 || D.nx < 32 || D.nx > 992) return false;
+    if (s->cfg.stream_policy == CULBM_STREAM_INPLACE && (D.ny < 3 || D.nz < 3)) return false;
+    return true;
+}
+
+// Calls f(stages, output buffers, L2 prefetch rows as integral constants)
+// for the sim's pipeline shape.
+template <class F>
+culbm_status with_row_shape(const culbm_sim* s, F&& f)
+{
+    using std::integral_constant;
+    if (s->cfg.kernel_variant == 2)
+        return f(integral_constant<int, 2>{}, integral_constant<int, 2>{}, integral_constant<int, 0>{});
+    return f(integral_constant<int, 2>{}, integral_constant<int, 1>{}, integral_constant<int, 0>{});
+}
+
+template <typename S, int MODE, int NS, int OB, int PF>
+culbm_status rows_prepare(culbm_sim* s)
+{
+    const RowSmem L = row_smem_layout<S, NS, OB>(s->dom.nx);
+    const int threads = (row_consumer_warps(s->dom.nx) + 1) * 32;
+    auto kern = k_rows16<S, MODE, NS, OB, PF>;
+    CULBM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, L.total));
+    int per_sm = 0, sms = 0;
+    CULBM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, L.total));
+    CULBM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->dev));
+    if (per_sm < 1) return fail(CULBM_ERR_UNSUPPORTED, "row-staged step kernel does not fit an SM");
+    s->row_grid[MODE] = per_sm * sms;
+    return CULBM_OK;
+}
+
+template <typename S>
+culbm_status rows_setup(culbm_sim* s)
+{
+    if constexpr (Is16<S>::value) {
+        CULBM_TRY(with_row_shape(s, [&](auto ns, auto ob, auto pf) -> culbm_status {
+            constexpr int NS = decltype(ns)::value, OB = decltype(ob)::value, PF = decltype(pf)::value;
+            if (s->cfg.stream_policy == CULBM_STREAM_PULL) {
+                CULBM_TRY((rows_prepare<S, ROWS_PULL, NS, OB, PF>(s)));
+            } else {
+                CULBM_TRY((rows_prepare<S, ROWS_AA_ODD, NS, OB, PF>(s)));
+                CULBM_TRY((rows_prepare<S, ROWS_AA_EVEN, NS, OB, PF>(s)));
+            }
+            return CULBM_OK;
+        }));
+        s->rows = true;
+    }
+    return CULBM_OK;
+}
+
+// One row-staged launch over the rows [y0, y0 + ry) x [z0, z0 + rz).
+template <typename S, int MODE>
+culbm_status rows_launch(culbm_sim* s, const StepArgs<S, float>& a, int y0, int z0, int ry, int rz)
+{
+    RowArgs<S> ra{};
+    ra.s = a;
+    ra.y0 = y0;
+    ra.z0 = z0;
+    ra.ry = ry;
+    ra.rz = rz;
+    ra.nrows = ry * rz;
+    ra.err = s->err_dev;
+    ra.debug_extra_tx = g_row_extra_tx.load();
+    const int grid = std::min(ra.nrows, s->row_grid[MODE]);
+    const int threads = (row_consumer_warps(s->dom.nx) + 1) * 32;
+    return with_row_shape(s, [&](auto ns, auto ob, auto pf) -> culbm_status {
+        constexpr int NS = decltype(ns)::value, OB = decltype(ob)::value, PF = decltype(pf)::value;
+        const RowSmem L = row_smem_layout<S, NS, OB>(s->dom.nx);
+        k_rows16<S, MODE, NS, OB, PF><<<grid, threads, L.total, s->stream>>>(ra);
+        CULBM_CUDA(cudaGetLastError());
+        return CULBM_OK;
+    });
+}
+
 template <typename S>
 culbm_status plain_steps(culbm_sim* s, uint32_t nsteps)
 {
@@ -228,6 +326,37 @@ culbm_status plain_steps(culbm_sim* s, uint32_t nsteps)
     const dim3 g = cell_grid(s->dom), b = cell_block();
     for (uint32_t k = 0; k < nsteps; ++k) {
         const uint32_t seed = step_seed(static_cast<uint32_t>(s->step + k));
+        if constexpr (Is16<S>::value) {
+            if (s->rows) {
+                const Domain& D = s->dom;
+                if (s->cfg.stream_policy == CULBM_STREAM_PULL) {
+                    auto a = make_args<S>(s, s->cur, 1 - s->cur);
+                    a.seed = seed;
+                    CULBM_TRY((rows_launch<S, ROWS_PULL>(s, a, 0, 0, D.ny, D.nz)));
+                    s->cur ^= 1;
+                    s->launches += 1;
+                } else {
+                    // face rows with the per-cell kernel (the outer slices of
+                    // split_grid), inner rows row-staged; disjoint locations
+                    auto a = make_args<S>(s, 0, 0);
+                    a.seed = seed;
+                    const dim3 gs = split_grid(D);
+                    const dim3 go(gs.x, gs.y, outer_slices(D));
+                    if (s->aa_phase == 0) {
+                        k_aa_odd<S, R><<<go, b, 0, s->stream>>>(a);
+                        CULBM_CUDA(cudaGetLastError());
+                        CULBM_TRY((rows_launch<S, ROWS_AA_ODD>(s, a, 1, 1, D.ny - 2, D.nz - 2)));
+                    } else {
+                        k_aa_even<S, R><<<go, b, 0, s->stream>>>(a);
+                        CULBM_CUDA(cudaGetLastError());
+                        CULBM_TRY((rows_launch<S, ROWS_AA_EVEN>(s, a, 1, 1, D.ny - 2, D.nz - 2)));
+                    }
+                    s->aa_phase ^= 1;
+                    s->launches += 2;
+                }
+                continue;
+            }
+        }
         if (s->cfg.stream_policy == CULBM_STREAM_PULL) {
             auto a = make_args<S>(s, s->cur, 1 - s->cur);
             a.seed = seed;
@@ -312,6 +441,7 @@ void release(culbm_sim* s)
     if (s->ev0) cudaEventDestroy(s->ev0);
     if (s->ev1) cudaEventDestroy(s->ev1);
     if (s->stream) cudaStreamDestroy(s->stream);
+    if (s->err_host) cudaFreeHost(s->err_host);
     delete s;
 }
 
@@ -453,6 +583,11 @@ culbm_status culbm_create(const culbm_config* cfg, culbm_sim** out)
         CULBM_TRY(dev_alloc(s, reinterpret_cast<void**>(&s->d_red), (4ull * s->red_blocks + 4) * sizeof(double),
                             "reduction scratch"));
         if (blocked) CULBM_TRY(tiles_create(s));
+        CULBM_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&s->err_host), sizeof(int), cudaHostAllocMapped));
+        *s->err_host = 0;
+        CULBM_CUDA(cudaHostGetDevicePointer(reinterpret_cast<void**>(&s->err_dev), s->err_host, 0));
+        if (rows_applicable(s))
+            CULBM_TRY(with_storage(s, [&](auto tag) { return rows_setup<typename decltype(tag)::type>(s); }));
         const float* none[4] = {nullptr, nullptr, nullptr, nullptr};
         CULBM_TRY(upload_state(s, nullptr, none));
         s->loaded = false;   // defaults in place; a load call is still expected
@@ -486,6 +621,7 @@ culbm_status culbm_load_state(culbm_sim* sim, const uint32_t* flag, const float*
     const float* mac[4] = {rho, vx, vy, vz};
     CULBM_TRY(upload_state(sim, flag, mac));
     CULBM_CUDA(cudaStreamSynchronize(sim->stream));
+    CULBM_TRY(check_device_error(sim));
     return CULBM_OK;
 }
 
@@ -542,6 +678,7 @@ culbm_status culbm_step_timed(culbm_sim* sim, uint32_t nsteps, float* elapsed_ms
     CULBM_TRY(culbm_step(sim, nsteps));
     CULBM_CUDA(cudaEventRecord(sim->ev1, sim->stream));
     CULBM_CUDA(cudaEventSynchronize(sim->ev1));
+    CULBM_TRY(check_device_error(sim));
     float ms = 0.0f;
     CULBM_CUDA(cudaEventElapsedTime(&ms, sim->ev0, sim->ev1));
     if (elapsed_ms) *elapsed_ms = ms;
@@ -552,7 +689,7 @@ culbm_status culbm_synchronize(culbm_sim* sim)
 {
     CULBM_TRY(check_sim(sim));
     CULBM_CUDA(cudaStreamSynchronize(sim->stream));
-    return CULBM_OK;
+    return check_device_error(sim);
 }
 
 culbm_status culbm_moments(culbm_sim* sim)
@@ -579,6 +716,7 @@ culbm_status culbm_get_field(culbm_sim* sim, culbm_field field, float* host_out)
     if (field < 0 || field > 3 || host_out == nullptr) return fail(CULBM_ERR_INVALID_ARGUMENT, "bad field or NULL output");
     CULBM_CUDA(cudaMemcpyAsync(host_out, sim->d_mac[field], sim->n * sizeof(float), cudaMemcpyDeviceToHost, sim->stream));
     CULBM_CUDA(cudaStreamSynchronize(sim->stream));
+    CULBM_TRY(check_device_error(sim));
     return CULBM_OK;
 }
 
@@ -638,6 +776,7 @@ culbm_status culbm_get_pulled_ddf(culbm_sim* sim, void* host_out, int32_t out_ty
         CULBM_CUDA(cudaGetLastError());
         CULBM_CUDA(cudaMemcpyAsync(host_out, d_out, bytes, cudaMemcpyDeviceToHost, sim->stream));
         CULBM_CUDA(cudaStreamSynchronize(sim->stream));
+        CULBM_TRY(check_device_error(sim));
         return CULBM_OK;
     });
     cudaFree(d_out);
@@ -676,6 +815,7 @@ culbm_status culbm_set_ddf(culbm_sim* sim, const void* host_in, int32_t in_type)
         else launch(Tag<double>{});
         CULBM_CUDA(cudaGetLastError());
         CULBM_CUDA(cudaStreamSynchronize(sim->stream));
+        CULBM_TRY(check_device_error(sim));
         if (aa) sim->aa_phase = 0;
         return CULBM_OK;
     });
@@ -702,6 +842,7 @@ culbm_status culbm_mass_momentum(culbm_sim* sim, double out[4])
         CULBM_CUDA(cudaGetLastError());
         CULBM_CUDA(cudaMemcpyAsync(out, part + 4 * nb, 4 * sizeof(double), cudaMemcpyDeviceToHost, sim->stream));
         CULBM_CUDA(cudaStreamSynchronize(sim->stream));
+        CULBM_TRY(check_device_error(sim));
         return CULBM_OK;
     });
 }
@@ -724,6 +865,8 @@ const char* culbm_status_string(culbm_status s)
 }
 
 int32_t culbm_abi_version(void) { return CULBM_ABI_VERSION; }
+
+void culbm_debug_row_wait_extra_bytes(int32_t bytes) { g_row_extra_tx.store(bytes > 0 ? bytes : 0); }
 
 void culbm_debug_inject_cuda_error(int32_t skip, int32_t code)
 {

@@ -72,6 +72,12 @@ struct culbm_sim {
     bool loaded = false;
 
     culbm::TileState* tiles = nullptr;
+
+    // Row-staged 16-bit step kernels (row_kernels.cuh), when the domain suits them.
+    bool rows = false;
+    int row_grid[3] = {0, 0, 0};    // resident blocks per launch, by RowMode
+    int* err_host = nullptr;        // mapped host word a bounded device-side wait writes on expiry
+    int* err_dev = nullptr;         // its device address
 };
 
 namespace culbm {
@@ -103,6 +109,9 @@ culbm_status with_storage(const culbm_sim* s, F&& f)
         default: return fail(CULBM_ERR_INVALID_ARGUMENT, "unknown storage format");
     }
 }
+
+// Reports and clears an expired bounded device-side wait (after a synchronisation).
+culbm_status check_device_error(culbm_sim* s);
 
 // Device allocation counted in sim->device_bytes (sim.cu).
 culbm_status dev_alloc(culbm_sim* s, void** p, size_t bytes, const char* what);

@@ -70,11 +70,16 @@ template <> struct Cvt<__nv_bfloat16, float> {
 
 // 16-bit storage with stochastic rounding: the same bit layouts as __half
 // (scaled by 2^15) and __nv_bfloat16, but every store rounds up or down with
-// probability given by the discarded fraction, driven by a counter-based hash
-// of (cell, direction, time step).  The hash inputs name the value, not the
-// address it is written to, so every copy of a population (streaming target,
-// clamp slots, tile buffers) gets the same bits and all streaming policies
-// stay bitwise equal to each other.  Deterministic for a given run.
+// probability given by the discarded fraction.  The rounding is sm_100a's
+// cvt.rs conversion (PTX ISA, "cvt" with the .rs rounding modifier): a
+// random integer R is added to the discarded part of the value's magnitude,
+// measured in units of 2^-13 (f16) or 2^-16 (bf16) of the destination's
+// last place, and the magnitude rounds up when the sum carries.  Its random
+// bits come from a counter-based hash of (cell, direction, time step).  The
+// hash inputs name the value, not the address it is written to, so every
+// copy of a population (streaming target, clamp slots, tile buffers) gets
+// the same bits and all streaming policies stay bitwise equal to each other.
+// Deterministic for a given run.
 struct Half16SR {
     unsigned short bits;
 };
@@ -86,9 +91,8 @@ template <typename S> struct IsSR { static constexpr bool value = false; };
 template <> struct IsSR<Half16SR> { static constexpr bool value = true; };
 template <> struct IsSR<BF16SR> { static constexpr bool value = true; };
 
-// Per-step seed, per-cell hash (one per cell and step) and per-direction
-// random bits.  Integer mixing in the style of the murmur3 finaliser; the
-// per-direction bits are a multiplicative hash whose high bits are used.
+// Per-step seed and per-cell hash (one per cell and step): integer mixing
+// in the style of the murmur3 finaliser.
 __host__ __device__ __forceinline__ uint32_t step_seed(uint32_t t)
 {
     uint32_t h = t * 0x9E3779B1u + 0x7F4A7C15u;
@@ -111,16 +115,81 @@ __device__ __forceinline__ uint32_t cell_hash(uint32_t cell, uint32_t seed)
     return h;
 }
 
-// Random bits of direction d: the cell hash times an odd multiplier of its
-// own per direction (one multiply; the high bits are used).
-__host__ __device__ constexpr uint32_t dir_multiplier(uint32_t d)
+// Random integer of direction d: bits 16-31 of the cell hash times an odd
+// multiplier of the direction (mod 2^32); f16 uses its low 13 bits, bf16 all
+// 16.  Directions are converted in pairs, pair k < 13 holding direction k in
+// the low 16 bits and direction 26 - k in the high 16 bits (pair 13: the
+// centre, low bits), so a pair's rbits word carries the integer of its low
+// direction in bits 0-15 and that of its high direction in bits 16-31.
+__host__ __device__ constexpr int sr_pair(int d) { return d <= 13 ? d : 26 - d; }
+__host__ __device__ constexpr bool sr_high(int d) { return d > 13; }
+__host__ __device__ constexpr uint32_t dir_multiplier(int d)
 {
-    return (0x2C1B3C6Du ^ (d * 0x9E3779B9u)) | 1u;
+    return (0x2C1B3C6Du ^ (static_cast<uint32_t>(d) * 0x9E3779B9u)) | 1u;
 }
 
-__device__ __forceinline__ uint32_t dir_bits(uint32_t hcell, uint32_t d)
+// rbits word of direction d alone (its integer in the half that d occupies).
+__device__ __forceinline__ uint32_t sr_word_dir(uint32_t hcell, int d)
 {
-    return hcell * dir_multiplier(d);
+    const uint32_t w = hcell * dir_multiplier(d);
+    return sr_high(d) ? w : w >> 16;
+}
+
+// rbits word of pair k < 13 (directions k and 26 - k).
+__device__ __forceinline__ uint32_t sr_word_pair(uint32_t hcell, int k)
+{
+    return __byte_perm(hcell * dir_multiplier(k), hcell * dir_multiplier(26 - k), 0x7632);
+}
+
+// Two FP32 values converted to one word of two 16-bit storage values, `hi`
+// in bits 16-31 and `lo` in bits 0-15, in the format's raw domain (the half
+// formats' 2^15 scale already applied).  Nearest-even for __half and
+// __nv_bfloat16.  For the stochastic formats, `rbits` bits 0-12 (f16) or
+// 0-15 (bf16) are the random integer of `lo`, bits 16-28 or 16-31 that of
+// `hi`.  Each half is converted on its own: packing a value with any other
+// value gives it the same bits.
+template <typename S> struct Pack2;
+template <> struct Pack2<__half> {
+    static __device__ __forceinline__ uint32_t cvt(float hi, float lo, uint32_t)
+    {
+        uint32_t d;
+        asm("cvt.rn.f16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(hi), "f"(lo));
+        return d;
+    }
+};
+template <> struct Pack2<__nv_bfloat16> {
+    static __device__ __forceinline__ uint32_t cvt(float hi, float lo, uint32_t)
+    {
+        uint32_t d;
+        asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(hi), "f"(lo));
+        return d;
+    }
+};
+template <> struct Pack2<Half16SR> {
+    static __device__ __forceinline__ uint32_t cvt(float hi, float lo, uint32_t rbits)
+    {
+        uint32_t d;
+        asm("cvt.rs.f16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(hi), "f"(lo), "r"(rbits));
+        return d;
+    }
+};
+template <> struct Pack2<BF16SR> {
+    static __device__ __forceinline__ uint32_t cvt(float hi, float lo, uint32_t rbits)
+    {
+        uint32_t d;
+        asm("cvt.rs.bf16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(hi), "f"(lo), "r"(rbits));
+        return d;
+    }
+};
+
+// The 16-bit pattern of direction d of a cell whose cell_hash for this step
+// is hcell, from its raw value v (2^15 f for the half formats, f for bf16).
+template <typename S>
+__device__ __forceinline__ unsigned short enc16_raw(float v, uint32_t hcell, int d)
+{
+    const uint32_t r = IsSR<S>::value ? sr_word_dir(hcell, d) : 0u;
+    if (sr_high(d)) return static_cast<unsigned short>(Pack2<S>::cvt(v, 0.0f, r) >> 16);
+    return static_cast<unsigned short>(Pack2<S>::cvt(0.0f, v, r));
 }
 
 template <> struct Cvt<Half16SR, float> {
@@ -137,15 +206,6 @@ template <> struct Cvt<Half16SR, float> {
     {
         p->bits = __half_as_ushort(__float2half_rn(__fmul_rn(v, kHalfScale)));
     }
-    // stochastic: add 13 random bits (the high bits of rnd) below the half's
-    // last mantissa bit, truncate
-    static __device__ __forceinline__ unsigned short enc(float v, uint32_t rnd)
-    {
-        const uint32_t u = __float_as_uint(__fmul_rn(v, kHalfScale)) + (rnd >> 19);
-        return __half_as_ushort(__float2half_rz(__uint_as_float(u)));
-    }
-    static __device__ __forceinline__ void st_sr(Half16SR* p, float v, uint32_t rnd) { p->bits = enc(v, rnd); }
-    static __device__ __forceinline__ void st_sr_cs(Half16SR* p, float v, uint32_t rnd) { __stcs(&p->bits, enc(v, rnd)); }
 };
 
 template <> struct Cvt<BF16SR, float> {
@@ -158,12 +218,6 @@ template <> struct Cvt<BF16SR, float> {
     {
         p->bits = __bfloat16_as_ushort(__float2bfloat16_rn(v));
     }
-    static __device__ __forceinline__ unsigned short enc(float v, uint32_t rnd)
-    {
-        return static_cast<unsigned short>((__float_as_uint(v) + (rnd >> 16)) >> 16);
-    }
-    static __device__ __forceinline__ void st_sr(BF16SR* p, float v, uint32_t rnd) { p->bits = enc(v, rnd); }
-    static __device__ __forceinline__ void st_sr_cs(BF16SR* p, float v, uint32_t rnd) { __stcs(&p->bits, enc(v, rnd)); }
 };
 
 // Raw load for consumers that are linear in the populations: the stored
@@ -183,16 +237,16 @@ __device__ __forceinline__ R ld_raw(const S* p)
         return Cvt<S, R>::ld(p);
 }
 
-// Store of population d of the cell whose cell_hash for this step is hcell:
-// stochastic rounding for the SR formats, the format's plain conversion
-// otherwise (hcell then goes unused and its computation is dropped).
-template <typename S, typename R>
-__device__ __forceinline__ void put(S* p, R v, uint32_t hcell, int d)
+// Raw 16-bit store (the pattern enc16_raw gives).
+template <typename S>
+__device__ __forceinline__ void st16(S* p, unsigned short bits)
 {
-    if constexpr (IsSR<S>::value)
-        Cvt<S, R>::st_sr(p, v, dir_bits(hcell, d));
-    else
-        Cvt<S, R>::st(p, v);
+    *reinterpret_cast<unsigned short*>(p) = bits;
+}
+template <typename S>
+__device__ __forceinline__ void st16_cs(S* p, unsigned short bits)
+{
+    __stcs(reinterpret_cast<unsigned short*>(p), bits);
 }
 
 // The 16-bit population formats.
@@ -204,28 +258,58 @@ template <typename S> struct ScaleExp { static constexpr int value = 0; };
 template <> struct ScaleExp<__half> { static constexpr int value = 15; };
 template <> struct ScaleExp<Half16SR> { static constexpr int value = 15; };
 
+// Store of population d (value v) of the cell whose cell_hash for this step
+// is hcell: the format's rounding (stochastic for the SR formats; hcell then
+// feeds the random bits, otherwise it goes unused and its computation is
+// dropped).
+template <typename S, typename R>
+__device__ __forceinline__ void put(S* p, R v, uint32_t hcell, int d)
+{
+    if constexpr (Is16<S>::value)
+        st16(p, enc16_raw<S>(ScaleExp<S>::value ? __fmul_rn(v, kHalfScale) : v, hcell, d));
+    else
+        Cvt<S, R>::st(p, v);
+}
+
 // put() of a raw value v = 2^E * f: the same bits as put(p, f, ...), without
 // the scaling multiply.
 template <typename S, typename R>
 __device__ __forceinline__ void put_raw(S* p, R v, uint32_t hcell, int d)
 {
-    if constexpr (std::is_same<S, __half>::value) {
-        *p = __float2half_rn(v);
-    } else if constexpr (std::is_same<S, Half16SR>::value) {
-        const uint32_t u = __float_as_uint(v) + (dir_bits(hcell, d) >> 19);
-        p->bits = __half_as_ushort(__float2half_rz(__uint_as_float(u)));
-    } else {
-        put(p, v, hcell, d);
-    }
+    if constexpr (Is16<S>::value)
+        st16(p, enc16_raw<S>(v, hcell, d));
+    else
+        Cvt<S, R>::st(p, v);
 }
 
+// put() with the evict-first hint.
 template <typename S, typename R>
 __device__ __forceinline__ void put_cs(S* p, R v, uint32_t hcell, int d)
 {
-    if constexpr (IsSR<S>::value)
-        Cvt<S, R>::st_sr_cs(p, v, dir_bits(hcell, d));
+    if constexpr (Is16<S>::value)
+        st16_cs(p, enc16_raw<S>(ScaleExp<S>::value ? __fmul_rn(v, kHalfScale) : v, hcell, d));
     else
         Cvt<S, R>::st_cs(p, v);
+}
+
+// Stores the 27 raw values f of one cell, direction d at addr(d), with the
+// bits of put_raw.  The 16-bit formats convert the directions in pairs
+// (d, 26 - d) with one packed conversion per pair.
+template <typename S, typename R, class A>
+__device__ __forceinline__ void put27_raw(const R* f, uint32_t hcell, A&& addr)
+{
+    if constexpr (Is16<S>::value) {
+#pragma unroll
+        for (int k = 0; k < 13; ++k) {
+            const uint32_t w = Pack2<S>::cvt(f[26 - k], f[k], IsSR<S>::value ? sr_word_pair(hcell, k) : 0u);
+            st16(addr(k), static_cast<unsigned short>(w));
+            st16(addr(26 - k), static_cast<unsigned short>(w >> 16));
+        }
+        st16(addr(13), enc16_raw<S>(f[13], hcell, 13));
+    } else {
+#pragma unroll
+        for (int d = 0; d < 27; ++d) put_raw(addr(d), f[d], hcell, d);
+    }
 }
 
 // Arithmetic type used with each storage type.

@@ -258,11 +258,8 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 5 : 1) k_pull_step(const
         for (int d = 0; d < 27; ++d) f[d] = R(0);
     }
     cell_update_for<S, true>(op, a.inv_tau, a.rho, a.vx, a.vy, a.vz, c.i, f);
-    if (op & OP_STORE) {
-#pragma unroll
-        for (int d = 0; d < 27; ++d)
-            put_raw(a.dst.p[d] + c.i, f[d], cell_hash(static_cast<uint32_t>(c.i), a.seed), d);
-    }
+    if (op & OP_STORE)
+        put27_raw<S>(f, cell_hash(static_cast<uint32_t>(c.i), a.seed), [&](int d) { return a.dst.p[d] + c.i; });
 }
 
 // In-place odd step (layout A -> B): each cell pulls f_d from the reversed
@@ -384,8 +381,7 @@ __device__ __forceinline__ void aa_odd_cell(const StepArgs<S, R>& a, const CellC
     cell_update_for<S, true>(op, a.inv_tau, a.rho, a.vx, a.vy, a.vz, c.i, f);
     if (!(op & OP_STORE)) return;
     if (ROWS == ROWS_INNER && !xface) {
-#pragma unroll
-        for (int d = 0; d < 27; ++d) put_raw(a.dst.p[d] + (c.i + nb_off(D, d)), f[d], hc, d);
+        put27_raw<S>(f, hc, [&](int d) { return a.dst.p[d] + (c.i + nb_off(D, d)); });
     } else if (ROWS == ROWS_INNER) {
 #pragma unroll
         for (int d = 0; d < 27; ++d) {
@@ -427,8 +423,7 @@ __device__ __forceinline__ void aa_even_cell(const StepArgs<S, R>& a, const Cell
     }
     cell_update_for<S, true>(op, a.inv_tau, a.rho, a.vx, a.vy, a.vz, c.i, f);
     if (!(op & OP_STORE)) return;
-#pragma unroll
-    for (int d = 0; d < 27; ++d) put_raw(a.dst.p[26 - d] + c.i, f[d], hc, d);
+    put27_raw<S>(f, hc, [&](int d) { return a.dst.p[26 - d] + c.i; });
     if (ROWS == ROWS_INNER) {
         if (c.x != 0 && c.x != D.nx - 1) return;
 #pragma unroll

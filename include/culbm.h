@@ -105,7 +105,12 @@ typedef struct culbm_config {
     int32_t cache_hints;       /* 1 (default): evict-first/evict-last hints on global/tile traffic
                                   (reference build switch CULBM_EXPT_CACHE_HINT_POLICY) */
     int32_t use_graphs;        /* 1 (default): tile launch sequences replayed as CUDA graphs */
-    int32_t kernel_variant;    /* reserved for alternative kernel schedules; 0 = default */
+    int32_t kernel_variant;    /* step kernels of the plain policies with 16-bit storage: 0 (default)
+                                  one thread per cell with direct global loads and stores; 1 and 2
+                                  row-staged (whole x-rows of the 27 planes staged in shared memory
+                                  by bulk asynchronous copies, one block per row; 1: one output
+                                  buffer, 2: two), used where nx is a multiple of 16 and at most
+                                  992.  Same bits either way */
     uint32_t reserved[7];
 } culbm_config;
 
@@ -401,6 +406,16 @@ int32_t culbm_abi_version(void);
  * made).  code == 0 disables injection.  No device fault is involved.
  */
 void culbm_debug_inject_cuda_error(int32_t skip, int32_t code);
+
+/*
+ * Test hook for the bounded waits of the row-staged step kernels: with
+ * bytes > 0 every staged row announces `bytes` more than its copies deliver,
+ * so its mbarrier phase never completes; the wait gives up after about a
+ * second, the kernel stops and the next synchronising call returns
+ * CULBM_ERR_DEVICE_TIMEOUT.  bytes <= 0 restores normal operation.  Touches
+ * nothing but the announced byte count; every copy still lands.
+ */
+void culbm_debug_row_wait_extra_bytes(int32_t bytes);
 
 #ifdef __cplusplus
 }

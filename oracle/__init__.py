@@ -72,6 +72,9 @@ def lib():
         L.orc_cell_fast_f32.argtypes = [C.c_uint32, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float, _f32p]
         L.orc_encode_s16.argtypes = [C.c_int, _i64, _f32p, u16p, C.c_uint32]
         L.orc_step_seed.argtypes = [C.c_uint32]
+        L.orc_round16_sr_n.argtypes = [C.c_int, _i64, _f32p, _u32p, u16p]
+        L.orc_sr_bits.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32]
+        L.orc_sr_bits.restype = C.c_uint32
         L.orc_step_seed.restype = C.c_uint32
         L.orc_valid_blk_axis.argtypes = [C.c_uint32] * 3
         L.orc_valid_blk_axis.restype = C.c_int
@@ -226,4 +229,15 @@ def run_s16(scene: Scene, storage: str, inv_tau, nsteps, state=None):
         a, b = b, a
     out = np.empty(27 * scene.n, np.float32)
     L.orc_decode_s16(kind, 27 * scene.n, a, out)
+    return out
+
+
+def round16_sr(kind: str, values, rbits):
+    """Stochastic rounding of FP32 values to IEEE half ("f16") or bfloat16
+    ("bf16") with one random integer each (the restatement of sm_100a's
+    cvt.rs rule); returns the uint16 patterns."""
+    v = np.ascontiguousarray(values, dtype=np.float32)
+    r = np.ascontiguousarray(rbits, dtype=np.uint32)
+    out = np.empty(v.size, np.uint16)
+    lib().orc_round16_sr_n({"f16": 0, "bf16": 1}[kind], v.size, v, r, out)
     return out

@@ -94,14 +94,68 @@ uint32_t orc_step_seed(uint32_t t)
     return h;
 }
 
-/* random bits of population d of `cell` at the step seeded by `seed`: a
- * per-cell finaliser hash times an odd multiplier of direction d (the high
- * bits are used) */
-uint32_t orc_sr_bits(uint32_t cell, uint32_t d, uint32_t seed)
+/* Per-cell hash of the step seeded by `seed` (murmur3-style finaliser). */
+static uint32_t orc_cell_hash(uint32_t cell, uint32_t seed)
 {
     uint32_t h = cell * 0x27D4EB2Fu ^ seed;
     h ^= h >> 16; h *= 0x85EBCA6Bu; h ^= h >> 13; h *= 0xC2B2AE35u; h ^= h >> 16;
-    return h * ((0x2C1B3C6Du ^ (d * 0x9E3779B9u)) | 1u);
+    return h;
+}
+
+/* The random integer of population d of `cell` at the step seeded by `seed`:
+ * bits 16-31 of the cell hash times an odd multiplier of d (mod 2^32); f16
+ * uses its low 13 bits, bf16 all 16. */
+uint32_t orc_sr_bits(uint32_t cell, uint32_t d, uint32_t seed)
+{
+    const uint32_t m = (0x2C1B3C6Du ^ (d * 0x9E3779B9u)) | 1u;
+    return (orc_cell_hash(cell, seed) * m) >> 16;
+}
+
+/* Stochastic rounding of an FP32 value to IEEE half (PTX cvt.rs.f16x2.f32,
+ * one half; no saturation): with q = |v| / ulp, ulp the half's last place at
+ * |v| (2^-24 below the normal range), the magnitude is floor(q), plus one when
+ * floor(frac(q) * 2^13) + r13 >= 2^13.  NaN gives 0x7FFF; a result at or above
+ * 2^16 is infinite. */
+uint16_t orc_round_f16_sr(float v, uint32_t r13)
+{
+    const uint32_t u = f2u(v);
+    const uint16_t sign = (uint16_t)((u >> 16) & 0x8000u);
+    const uint32_t mag = u & 0x7FFFFFFFu;
+    r13 &= 0x1FFFu;
+    if (mag > 0x7F800000u) return 0x7FFF;
+    if (mag == 0x7F800000u) return sign | 0x7C00;
+    const int E = (int)(mag >> 23);
+    if (E == 0) return sign;                       /* below 2^-126: frac(q) * 2^13 < 1 */
+    const uint32_t sig = (mag & 0x7FFFFFu) | 0x800000u;
+    const int e = E - 127;
+    uint32_t m, frac;
+    if (e >= -14) {                                /* normal half: 13 discarded bits */
+        m = sig >> 13;
+        frac = sig & 0x1FFFu;
+    } else {                                       /* subnormal half: units of 2^-24 */
+        const int sh = 126 - E;
+        m = sh < 32 ? sig >> sh : 0u;
+        frac = (sh - 13) < 32 ? (sig >> (sh - 13)) & 0x1FFFu : 0u;
+    }
+    if (frac + r13 >= 0x2000u) m += 1;
+    if (e < -14) return sign | (uint16_t)m;        /* m = 1024 is the smallest normal */
+    if (e > 15) return sign | 0x7C00;
+    uint32_t h = ((uint32_t)(e + 15) << 10) + (m - 1024u);
+    if (h > 0x7C00u) h = 0x7C00u;
+    return sign | (uint16_t)h;
+}
+
+/* Stochastic rounding of an FP32 value to bfloat16 (PTX cvt.rs.bf16x2.f32, one
+ * half; no saturation): r16 added to the 16 discarded bits of the magnitude,
+ * then truncated.  NaN gives 0x7FFF. */
+uint16_t orc_round_bf16_sr(float v, uint32_t r16)
+{
+    const uint32_t u = f2u(v);
+    const uint32_t mag = u & 0x7FFFFFFFu;
+    const uint16_t sign = (uint16_t)((u >> 16) & 0x8000u);
+    if (mag > 0x7F800000u) return 0x7FFF;
+    if (mag == 0x7F800000u) return sign | 0x7F80;
+    return sign | (uint16_t)((mag + (r16 & 0xFFFFu)) >> 16);
 }
 
 static float h16_decode(uint16_t h)
@@ -119,22 +173,6 @@ static uint16_t h16_encode_rn(float v)
     return b;
 }
 
-/* add 13 random bits (the high bits of rnd) below the half's last mantissa
- * bit, then truncate */
-static uint16_t h16_encode_sr(float v, uint32_t rnd)
-{
-    const float t = u2f(f2u(v * 32768.0f) + (rnd >> 19));
-    float z;
-    if (fabsf(t) >= 6.103515625e-05f)          /* normal half range: keep 10 mantissa bits */
-        z = u2f(f2u(t) & ~0x1FFFu);
-    else                                        /* subnormal half: multiples of 2^-24 */
-        z = truncf(t * 16777216.0f) / 16777216.0f;
-    _Float16 h = (_Float16)z;                   /* exact */
-    uint16_t b;
-    memcpy(&b, &h, 2);
-    return b;
-}
-
 static float b16_decode(uint16_t b) { return u2f((uint32_t)b << 16); }
 
 static uint16_t b16_encode_rn(float v)
@@ -143,8 +181,6 @@ static uint16_t b16_encode_rn(float v)
     return (uint16_t)((u + 0x7FFFu + ((u >> 16) & 1u)) >> 16);
 }
 
-static uint16_t b16_encode_sr(float v, uint32_t rnd) { return (uint16_t)((f2u(v) + (rnd >> 16)) >> 16); }
-
 static float s16_decode(int kind, uint16_t b) { return (kind & 1) ? b16_decode(b) : h16_decode(b); }
 
 static uint16_t s16_encode(int kind, float v, uint32_t cell, uint32_t d, uint32_t seed)
@@ -152,8 +188,8 @@ static uint16_t s16_encode(int kind, float v, uint32_t cell, uint32_t d, uint32_
     switch (kind) {
         case 0: return h16_encode_rn(v);
         case 1: return b16_encode_rn(v);
-        case 2: return h16_encode_sr(v, orc_sr_bits(cell, d, seed));
-        default: return b16_encode_sr(v, orc_sr_bits(cell, d, seed));
+        case 2: return orc_round_f16_sr(v * 32768.0f, orc_sr_bits(cell, d, seed));
+        default: return orc_round_bf16_sr(v, orc_sr_bits(cell, d, seed));
     }
 }
 
@@ -291,4 +327,13 @@ void orc_encode_s16(int kind, int64_t n, const float *src, uint16_t *out, uint32
     for (int64_t d = 0; d < 27; ++d)
         for (int64_t i = 0; i < n; ++i)
             out[d * n + i] = s16_encode(kind, src[d * n + i], (uint32_t)i, (uint32_t)d, seed);
+}
+
+/* Element-wise stochastic rounding of n FP32 values with their random
+ * integers r[k]: IEEE half (kind 0, orc_round_f16_sr) or bfloat16 (kind 1,
+ * orc_round_bf16_sr). */
+void orc_round16_sr_n(int kind, int64_t n, const float *v, const uint32_t *r, uint16_t *out)
+{
+    for (int64_t k = 0; k < n; ++k)
+        out[k] = kind ? orc_round_bf16_sr(v[k], r[k]) : orc_round_f16_sr(v[k], r[k]);
 }

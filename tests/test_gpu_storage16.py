@@ -72,3 +72,98 @@ def test_stochastic_rounding_is_unbiased(culbm):
     ulp = 2.0 ** 5 * 2.0 ** -10 / 32768.0    # ulp of v*2^15 = 40.45 (exponent 2^5), back in f units
     assert abs(interior.mean() - float(v)) < 0.02 * ulp
     assert len(np.unique(interior)) == 2
+
+
+def test_hardware_stochastic_rounding_matches_oracle_rule(orc, tmp_path):
+    """sm_100a's cvt.rs.f16x2.f32 / cvt.rs.bf16x2.f32, run now on this GPU
+    over 2^20 seeded (a, b, rbits) triples (tests/golden/cvt_rs_probe.cu),
+    against the oracle's restatement of the rule the storage kernels use."""
+    import importlib.util
+    import os
+    spec = importlib.util.spec_from_file_location(
+        "make_cvt_rs_golden", os.path.join(os.path.dirname(__file__), "golden", "make_cvt_rs_golden.py"))
+    gen = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(gen)
+    a, b, r, f16, _, bf16, _ = gen.run_probe(str(tmp_path))
+    for kind, mask, packed in (("f16", 0x1FFF, f16), ("bf16", 0xFFFF, bf16)):
+        lo = orc.round16_sr(kind, b, r & mask)
+        hi = orc.round16_sr(kind, a, (r >> 16) & mask)
+        assert np.array_equal(lo, (packed & 0xFFFF).astype(np.uint16)), kind
+        assert np.array_equal(hi, (packed >> 16).astype(np.uint16)), kind
+
+
+ROW_DOMAINS = [(32, 3, 3), (48, 7, 5), (64, 12, 10), (96, 5, 9)]
+
+
+@pytest.mark.parametrize("storage", ["fp16", "bf16", "fp16sr", "bf16sr"])
+@pytest.mark.parametrize("sp", [0, 1])
+@pytest.mark.parametrize("dims", ROW_DOMAINS)
+def test_row_staged_kernels_match_oracle(culbm, orc, storage, sp, dims):
+    """The row-staged 16-bit kernels (nx a multiple of 16): pull over every
+    row, in place over the inner rows with the face rows on the per-cell
+    kernels.  Fluid x faces (clamped pulls of inner rows from the edge
+    buffer), solid cells without STORE, EQU inlet/outlet rows; odd and even
+    step counts."""
+    sc = S.reference_channel(*dims, 0.05)
+    sc.flag[:, :, 0] = S.FLUID
+    sc.flag[:, :, -1] = S.FLUID
+    rng = np.random.default_rng(sum(dims) + sp)
+    solid = rng.random(sc.flag.shape) < 0.06
+    sc.flag[solid] = 0
+    for nsteps in (6, 7):
+        want = oracle_pulled16(orc, sc, storage, 0.6, nsteps)
+        with culbm.Simulation(sc.shape, stream_policy=sp, inv_tau=0.6, storage=storage, kernel_variant=1) as sim:
+            sim.load_state(*sc.arrays())
+            sim.step(nsteps)
+            got = sim.pulled_ddf()
+            launches = sim.info()["launches_per_step"]
+        assert launches == (2.0 if sp == 1 else 1.0)   # the row path ran (in place: face rows + inner rows)
+        assert np.array_equal(bits(got), bits(want)), (storage, sp, dims, nsteps)
+
+
+@pytest.mark.parametrize("storage", ["fp16sr", "bf16"])
+@pytest.mark.parametrize("sp", [0, 1])
+def test_row_staged_kernels_equal_per_cell_kernels(culbm, storage, sp):
+    """kernel_variant 0 (per-cell) and 1, 2 (row-staged, one or two output
+    buffers) give the same bits on a larger domain with random flags, over
+    many rows per block."""
+    dims = (160, 40, 36)
+    sc = S.default_scene(*dims)
+    rng = np.random.default_rng(17)
+    pick = rng.random(sc.flag.shape)
+    sc.flag[pick < 0.05] = S.WALL
+    sc.flag[(pick >= 0.05) & (pick < 0.07)] = S.EQUILIBRIUM
+    sc.flag[(pick >= 0.07) & (pick < 0.08)] = 0
+    sc.rho[:] = (1 + 0.01 * rng.standard_normal(sc.flag.shape)).astype(np.float32)
+    sc.vx[:] = (0.02 * rng.standard_normal(sc.flag.shape)).astype(np.float32)
+    out = []
+    for variant in (0, 1, 2):
+        with culbm.Simulation(dims, stream_policy=sp, inv_tau=0.55, storage=storage, kernel_variant=variant) as sim:
+            sim.load_state(*sc.arrays())
+            sim.step(9)
+            out.append(sim.pulled_ddf())
+    assert np.array_equal(bits(out[0]), bits(out[1]))
+    assert np.array_equal(bits(out[0]), bits(out[2]))
+
+
+def test_row_staged_wait_gives_up_and_reports(culbm):
+    """A staged row whose mbarrier phase cannot complete (announced bytes that
+    never arrive): the bounded wait gives up after about a second, the next
+    synchronising call reports CULBM_ERR_DEVICE_TIMEOUT, and the device stays
+    usable for the next run."""
+    from culbm_b200 import _capi
+    lib = _capi.lib()
+    dims = (64, 8, 6)
+    lib.culbm_debug_row_wait_extra_bytes(16)
+    try:
+        with culbm.Simulation(dims, stream_policy=0, storage="fp16", kernel_variant=1) as sim:
+            sim.step(1)
+            rc = lib.culbm_synchronize(sim._h)
+            assert rc == 7, lib.culbm_last_error().decode()    # CULBM_ERR_DEVICE_TIMEOUT
+            assert "bounded wait" in lib.culbm_last_error().decode()
+    finally:
+        lib.culbm_debug_row_wait_extra_bytes(0)
+    with culbm.Simulation(dims, stream_policy=0, storage="fp16", kernel_variant=1) as sim:
+        sim.step(2)
+        sim.synchronize()
+        assert np.isfinite(sim.pulled_ddf()).all()

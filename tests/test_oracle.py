@@ -152,3 +152,19 @@ def test_compact_update_of_16bit_formats_is_the_same_bgk(orc):
             assert e_fast < 1e-6 and e_exact < 1e-4, (flag, e_fast, e_exact)
             worst = max(worst, e_fast)
     assert worst > 0   # the two forms do differ in rounding
+
+
+def test_stochastic_rounding_rule_matches_sm100a_known_answers(orc):
+    """The oracle's restatement of cvt.rs (f16 and bf16, no saturation) against
+    outputs of sm_100a's cvt.rs.f16x2.f32 / cvt.rs.bf16x2.f32 recorded on a
+    B200 (tests/golden/make_cvt_rs_golden.py): rbits bits 0-12 / 0-15 round the
+    low half, bits 16-28 / 16-31 the high half.  Structured cases (carry from
+    an all-ones fraction per random bit, zeros, infinities, NaN, overflow,
+    half subnormals) and seeded random values over the whole FP32 range."""
+    g = np.load(os.path.join(GOLDEN, "cvt_rs_sm100a.npz"))
+    a, b, r = g["a"], g["b"], g["rbits"]
+    for kind, mask, packed in (("f16", 0x1FFF, g["f16x2"]), ("bf16", 0xFFFF, g["bf16x2"])):
+        lo = orc.round16_sr(kind, b, r & mask)
+        hi = orc.round16_sr(kind, a, (r >> 16) & mask)
+        assert np.array_equal(lo, (packed & 0xFFFF).astype(np.uint16)), kind
+        assert np.array_equal(hi, (packed >> 16).astype(np.uint16)), kind
