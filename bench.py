@@ -48,8 +48,9 @@ def peaks():
 
 
 class ClockSampler:
-    """SM clock and throttle-reason sampling (NVML, every 10 ms) during the
-    timed region; falls back to nvidia-smi when NVML is unavailable."""
+    """SM clock and throttle-reason sampling (NVML, every 10 ms) for the whole
+    run, with per-window summaries; falls back to nvidia-smi when NVML is
+    unavailable."""
 
     # NVML clocks-event-reason bits (nvml.h)
     REASONS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown",
@@ -57,7 +58,7 @@ class ClockSampler:
 
     def __init__(self, index=0):
         self.index = index
-        self.samples = []
+        self.samples = []          # (perf_counter time, SM MHz, reason bits)
         self.max_mhz = None
         self._stop = threading.Event()
         self._t = None
@@ -71,7 +72,7 @@ class ClockSampler:
                 r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
             except AttributeError:
                 r = nv.nvmlDeviceGetCurrentClocksThrottleReasons(h)
-            self.samples.append((float(sm), int(r)))
+            self.samples.append((time.perf_counter(), float(sm), int(r)))
             self._stop.wait(0.01)
 
     def _run_smi(self):
@@ -82,7 +83,7 @@ class ClockSampler:
                                       "--format=csv,noheader,nounits"], capture_output=True, text=True,
                                      timeout=10).stdout.strip().split(",")
                 self.max_mhz = float(out[1])
-                self.samples.append((float(out[0]), int(out[2].strip(), 16)))
+                self.samples.append((time.perf_counter(), float(out[0]), int(out[2].strip(), 16)))
             except Exception:
                 pass
             self._stop.wait(0.05)
@@ -98,23 +99,37 @@ class ClockSampler:
         except Exception:
             self._run_smi()
 
-    def __enter__(self):
+    def start(self):
         self._t = threading.Thread(target=self._run, daemon=True)
         self._t.start()
         time.sleep(0.05)
         return self
 
-    def __exit__(self, *exc):
+    def stop(self):
         self._stop.set()
-        self._t.join(timeout=15)
+        if self._t is not None:
+            self._t.join(timeout=15)
 
-    def summary(self):
-        if not self.samples:
+    def __enter__(self):
+        return self.start()
+
+    def __exit__(self, *exc):
+        self.stop()
+
+    def summary(self, t0=None, t1=None):
+        """Median SM clock, max clock and the throttle reasons seen between
+        perf_counter times t0 and t1 (the whole run when both are None); a
+        window shorter than the sampling period takes the nearest sample."""
+        sel = [s for s in self.samples if (t0 is None or s[0] >= t0) and (t1 is None or s[0] <= t1)]
+        if not sel and self.samples and t0 is not None:
+            mid = 0.5 * (t0 + (t1 if t1 is not None else t0))
+            sel = [min(self.samples, key=lambda s: abs(s[0] - mid))]
+        if not sel:
             return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["no samples"], "samples": 0}
-        sm = [s[0] for s in self.samples]
-        reasons = sorted({name for _, r in self.samples for bit, name in self.REASONS.items() if r & bit})
+        sm = [s[1] for s in sel]
+        reasons = sorted({name for _, _, r in sel for bit, name in self.REASONS.items() if r & bit})
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": self.max_mhz, "reasons": reasons,
-                "samples": len(self.samples)}
+                "samples": len(sel)}
 
 
 def dist():
@@ -175,7 +190,7 @@ def traffic_from_profiles(kernel_key):
 
 # ------------------------------------------------------------------- ours ---
 
-def measure(culbm, scene, sp, op, storage, steps, warmup, tile=None, inner=5, ring=False):
+def measure(culbm, scene, sp, op, storage, steps, warmup, tile=None, inner=5, ring=False, clocks=None):
     arrs = scene.arrays()
     kw = {"dev_id": int(os.environ.get("LOCAL_RANK", "0"))}
     if op:
@@ -183,8 +198,13 @@ def measure(culbm, scene, sp, op, storage, steps, warmup, tile=None, inner=5, ri
     with culbm.Simulation(scene.shape, stream_policy=sp, opt_policy=op, storage=storage, inv_tau=0.5, **kw) as sim:
         sim.load_state(*arrs)
         sim.step(warmup)
+        sim.synchronize()
+        t0 = time.perf_counter()
         ms = sim.step_timed(steps)
+        t1 = time.perf_counter()
         info = sim.info()
+    if clocks is not None:
+        info["clocks"] = clocks.summary(t0, t1)
     return scene.n * steps / (ms * 1e-3) / 1e6, ms / steps, info
 
 
@@ -319,6 +339,91 @@ def e2e_run(culbm, scene, steps, sp=1):
     return scene.n * steps / dt / 1e6, h2d, d2h
 
 
+# The reference's own parser of its speed lines (analysis/blocking_experiments.py:40).
+SPEED_RE = __import__("re").compile(r"speed = ([0-9]+(?:\.[0-9]+)?) \(MLUPS\)")
+REF_BIN_DIR = os.path.join(ROOT, "oracle", "_ref")
+
+# Launch shapes of the reference's CUDA binary on the 288x272x280 workload:
+# README.md:41-61 ((0,0) [32,16,2]x[9,17,140]; (1,3) [32,16,2]x[2,6,38],
+# innerLoop 5), the best (0,0) block shape of a B200 retune, and the two build
+# variants of src/simulator/single_dev_expt/CMakeLists.txt:28-41 on the (1,3)
+# README shape.
+REF_BINARY_LEGS = {
+    "readme_00": ("single_dev_expt_main", (32, 16, 2), (9, 17, 140), 0, 0),
+    "retuned_00": ("single_dev_expt_main", (32, 8, 1), (9, 34, 280), 0, 0),
+    "readme_13": ("single_dev_expt_main", (32, 16, 2), (2, 6, 38), 1, 3),
+    "variant_no_persist_no_hint_13": ("single_dev_expt_no_persist_no_hint_main", (32, 16, 2), (2, 6, 38), 1, 3),
+    "variant_no_persist_hint_only_13": ("single_dev_expt_no_persist_hint_only_main", (32, 16, 2), (2, 6, 38), 1, 3),
+}
+
+
+def parse_speeds(stdout):
+    """MLUPS of a reference-style run: the median of its `speed = X (MLUPS)`
+    lines with the first skipped, as analysis/blocking_experiments.py:115 does."""
+    speeds = [float(v) for v in SPEED_RE.findall(stdout)][1:]
+    return statistics.median(speeds) if speeds else None
+
+
+def reference_binary_legs(scene, peak, nstep=600, dstep=100, clocks=None):
+    """The reference's single_dev_expt_main, compiled from its own sources for
+    sm_100a (oracle/_ref, make -C oracle ref-gpu), on the same init-state
+    folder, timed by its own CUDA events (simulator_expt_platform.cu:971-984)."""
+    import shutil
+    import tempfile
+
+    from culbm_b200 import scenes
+    if not os.path.exists(os.path.join(REF_BIN_DIR, "single_dev_expt_main")):
+        return {"unavailable": "oracle/_ref/single_dev_expt_main not built (make -C oracle ref-gpu needs the "
+                               "reference tree)"}
+    tmp = tempfile.mkdtemp(prefix="culbm_refbin_")
+    out = {"workload": WORKLOAD, "steps": nstep, "dstep": dstep,
+           "how": "median of the binary's speed lines, first skipped (analysis/blocking_experiments.py:115)",
+           "legs": {}}
+    try:
+        folder = os.path.join(tmp, "init")
+        scenes.write_folder(scene, folder)
+        nx, ny, nz = scene.shape
+        vec = lambda v: "[" + ",".join(str(int(a)) for a in v) + "]"
+        for name, (binary, block, grid, sp, op) in REF_BINARY_LEGS.items():
+            path = os.path.join(REF_BIN_DIR, binary)
+            if not os.path.exists(path):
+                out["legs"][name] = {"error": f"{binary} not built"}
+                continue
+            cmd = [path, "--domainDim", vec((nx, ny, nz)), "--blockDim", vec(block), "--gridDim", vec(grid),
+                   "--streamPolicy", str(sp), "--optPolicy", str(op), "--innerLoop", "5", "--invTau", "0.5",
+                   "--nstep", str(nstep), "--dstep", str(dstep), "--initStateFolder", folder,
+                   "--dumpFolder", os.path.join(tmp, "dump")]
+            t0 = time.perf_counter()
+            try:
+                r = subprocess.run(cmd, capture_output=True, text=True, timeout=300)
+            except subprocess.TimeoutExpired:
+                out["legs"][name] = {"error": "timed out"}
+                continue
+            t1 = time.perf_counter()
+            mlups = parse_speeds(r.stdout)
+            leg = {"binary": binary, "blockDim": list(block), "gridDim": list(grid),
+                   "policy": f"streamPolicy {sp}, optPolicy {op}" + (", innerLoop 5" if op else ""),
+                   "exit_code": r.returncode}
+            if mlups is None:
+                leg["error"] = (r.stderr or r.stdout)[-300:]
+            else:
+                leg["mlups"] = round(mlups, 1)
+                leg["hbm_frac_of_measured"] = round(mlups * 1e6 * BYTES_PER_LUP["fp32"] / 1e9 / peak, 4)
+            if clocks is not None:
+                leg["clocks"] = clocks.summary(t0, t1)
+            out["legs"][name] = leg
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+    return out
+
+
+def workload_config(sc, ws):
+    """The `config` of both arms' JSON lines (same keys and values)."""
+    return {"workload": WORKLOAD, "cells": sc.n, "solid_fraction": round(sc.solid_fraction(), 4),
+            "storage": "fp32", "l2": "no flush: 2.37 GB of populations per step, 19x the 126 MB L2",
+            "parallelism": f"{ws} independent replica(s), one per GPU"}
+
+
 def cpu_baseline(scene, budget_s=12.0):
     import oracle
     if not oracle.ref_available():
@@ -355,6 +460,7 @@ def run_ours(args):
     peak, peak_kind = peaks()
 
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    clocks = ClockSampler(local).start()
     # headline: FP32 in-place, whole domain
     with culbm_b200.Simulation(sc.shape, stream_policy=1, opt_policy=0, storage="fp32", inv_tau=0.5,
                                dev_id=local) as sim:
@@ -362,9 +468,11 @@ def run_ours(args):
         sim.step(args.warmup)
         sim.synchronize()
         barrier(tdist)
-        with ClockSampler(local) as clocks:
-            ms = sim.step_timed(args.steps)
+        t0 = time.perf_counter()
+        ms = sim.step_timed(args.steps)
+        t1 = time.perf_counter()
         info = sim.info()
+    headline_clocks = clocks.summary(t0, t1)
     barrier(tdist)
     ms_max = max_over_ranks(tdist, ms)
     value = aggregate_mlups(ws, sc.n, args.steps, ms_max)
@@ -372,6 +480,7 @@ def run_ours(args):
     launches = int(round(info["launches_per_step"] * args.steps))
 
     if rank != 0:
+        clocks.stop()
         if tdist is not None:
             tdist.destroy_process_group()
         return
@@ -391,15 +500,23 @@ def run_ours(args):
         # the reference README's (1,3) launch shape: tile [32,16,2] x [2,6,38]
         "blocked_inplace_fp32_readme_tile": (1, 3, "fp32", (64, 96, 76), 5),
         "blocked_inplace_fp32_selected_tile": (1, 3, "fp32", tuple(sel["tile"]), sel["inner_loop"]),
+        # (0,3): pull L2 tiles, the same two tiles
+        "blocked_pull_fp32_readme_tile": (0, 3, "fp32", (64, 96, 76), 5),
+        "blocked_pull_fp32_selected_tile": (0, 3, "fp32", tuple(sel["tile"]), sel["inner_loop"]),
     }.items():
         try:
-            mlups, mps, inf = measure(culbm_b200, sc, sp, op, st, k2, 3, tile=tile, inner=inner)
+            mlups, mps, inf = measure(culbm_b200, sc, sp, op, st, k2, 3, tile=tile, inner=inner, clocks=clocks)
             extra[name] = {"mlups": round(mlups, 1), "ms_per_step": round(mps, 4),
                            "hbm_frac_of_measured": round(mlups * 1e6 * BYTES_PER_LUP[st] / 1e9 / peak, 4),
                            "policy": f"streamPolicy {sp}, optPolicy {op}" +
-                                     (f", tile {tile}, innerLoop {inner}" if op else "")}
+                                     (f", tile {tile}, innerLoop {inner}" if op else ""),
+                           "clocks": inf.get("clocks")}
         except Exception as e:   # report, do not hide
             extra[name] = {"error": str(e)}
+    try:
+        ref_bin = reference_binary_legs(sc, peak, clocks=clocks)
+    except Exception as e:
+        ref_bin = {"error": str(e)}
     try:
         errs = fp64_errors(culbm_b200, steps=args.err_steps)
     except Exception as e:
@@ -414,6 +531,7 @@ def run_ours(args):
         adjoint = {"error": str(e)}
     e2e_mlups, h2d, d2h = e2e_run(culbm_b200, sc, args.steps)
     cpu = cpu_baseline(sc) if ws == 1 else None
+    clocks.stop()
 
     line = {
         "metric": METRIC,
@@ -428,10 +546,8 @@ def run_ours(args):
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic (seeded sphere channel in the reference's flag.dat format)",
-        "config": {"workload": WORKLOAD, "cells": sc.n, "solid_fraction": round(sc.solid_fraction(), 4),
-                   "policy": "streamPolicy 1 (in-place AA), optPolicy 0", "storage": "fp32",
-                   "l2": "no flush: 2.37 GB of populations per step, 19x the 126 MB L2",
-                   "parallelism": f"{ws} independent replica(s), one per GPU"},
+        "config": workload_config(sc, ws),
+        "policy": "streamPolicy 1 (in-place AA), optPolicy 0",
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "peak_kind": f"{peak_kind} copy bandwidth",
                      "algorithmic_bytes_per_lup": BYTES_PER_LUP["fp32"],
@@ -443,9 +559,11 @@ def run_ours(args):
                 "what": f"culbm_load_state from pinned host + {args.steps} steps + culbm_moments + "
                         f"4x culbm_get_field to pinned host, host wall clock"},
         "gpu_launches": launches,
-        "clocks": clocks.summary(),
+        "clocks": headline_clocks,
+        "clocks_whole_run": clocks.summary(),
         "cpu_baseline": cpu,
         "variants": extra,
+        "reference_binary": ref_bin,
         "fp64_error": errs,
         "mixed_precision_512x512x256": mixed,
         "adjoint": adjoint,
@@ -496,7 +614,9 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": round(mlups, 2), "unit": "MLUPS", "n_gpus": ws,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt / args.steps * 1e3, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic (seeded sphere channel)", "config": {"workload": WORKLOAD, "cells": sc.n},
+        "data": "synthetic (seeded sphere channel in the reference's flag.dat format)",
+        "config": workload_config(sc, ws),
+        "policy": "the reference's lbm_core pull step (StaticD3Q27PullKernel order) on the host cores",
         "cpu_baseline": {"value": round(mlups, 2), "unit": "MLUPS", "cores": threads, "kind": "reference",
                          "sample": sample},
         "e2e": {"value": round(mlups, 2), "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},

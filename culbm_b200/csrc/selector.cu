@@ -16,7 +16,8 @@
 // partial sector relative to a full one in a streaming store.  The search
 // keeps tiles with Bx a multiple of 32 up to 160, By >= Bz, 2 (I-1) < Bz,
 // V within the persisting-L2 limit, 2 <= I <= 20, and (added here) only
-// geometries the blocking engine accepts for the given domain.
+// geometries the blocking engine accepts for the given domain, plus
+// whole-row tiles (Bx = nx, no x halo between tiles) on domains wider than 160.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -87,7 +88,9 @@ culbm_status median_ms(cudaStream_t s, cudaEvent_t e0, cudaEvent_t e1, int sampl
 
 // (beta_sec, beta_edge) of the valid x-rows of a tile of width bx advanced
 // i steps: warps of 32 cells cover x in [r, bx - r), r = i - 1; a row start
-// takes the alignments (mod 8 floats) that rows of its length reach.
+// takes the alignments (mod 8 floats) that rows of its length reach.  The
+// reference counts the warps of x < 160, its widest tile; wider tiles (the
+// whole-row tiles below) count all of theirs, which changes nothing up to 160.
 void beta(int bx, int i, double* sec, double* edge)
 {
     const int r = i - 1, len = bx - 2 * r;
@@ -104,7 +107,7 @@ void beta(int bx, int i, double* sec, double* edge)
     long long n_sec = 0, n_edge = 0;
     for (int ph = 0; ph < 8; ++ph) {
         if (ph % g) continue;
-        for (int w = 0; w < 160; w += 32) {
+        for (int w = 0; w < std::max(160, bx); w += 32) {
             const int lo = std::max(r, w), hi = std::min(bx - r, w + 32);
             if (hi > lo) n_sec += (ph + hi - 1) / 8 + 1 - (ph + lo) / 8;
         }
@@ -230,8 +233,12 @@ culbm_status culbm_select_tile(const uint32_t domain_dim[3], int32_t storage, do
     const double cell_bytes = cell_bytes_of(storage);
     const double l2 = static_cast<double>(l2_bytes);
     double best = -1;
+    // tile widths: the reference's multiples of 32 up to 160, and whole rows
+    // (Bx = nx) when the domain is wider
+    std::vector<int> widths = {32, 64, 96, 128, 160};
+    if (domain_dim[0] > 160) widths.push_back(static_cast<int>(domain_dim[0]));
     for (int i = 2; i <= 20; ++i)
-        for (int bx = 32; bx <= 160; bx += 32) {
+        for (int bx : widths) {
             if (bx <= 2 * (i - 1)) continue;
             for (int bz = 2 * (i - 1) + 1; bz <= 160; ++bz)
                 for (int by = bz; by <= 160; ++by) {

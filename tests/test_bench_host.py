@@ -35,6 +35,8 @@ def test_reference_arm_prints_one_contract_line(orc):
     assert line["n_gpus"] == 1 and line["steps"] == 3 and line["warmup"] == 3
     assert line["value"] > 0 and line["ms_per_step"] > 0
     assert line["config"]["workload"] == bench.WORKLOAD and line["config"]["cells"] == 288 * 272 * 280
+    from culbm_b200 import scenes
+    assert line["config"] == bench.workload_config(scenes.spheres_288(), 1)
     cb = line["cpu_baseline"]
     assert cb["kind"] == "reference" and cb["value"] == line["value"] and cb["cores"] >= 1 and cb["sample"]
     assert line["e2e"] == {"value": line["value"], "unit": "MLUPS", "h2d_bytes_per_step": 0,
@@ -58,10 +60,36 @@ def test_clock_summary_names_throttle_reasons():
     c = bench.ClockSampler()
     assert c.summary()["reasons"] == ["no samples"]
     c.max_mhz = 1965
-    c.samples = [(1965.0, 0), (1800.0, 0x4), (1700.0, 0x4 | 0x8), (1965.0, 0x40)]
+    c.samples = [(0.0, 1965.0, 0), (1.0, 1800.0, 0x4), (2.0, 1700.0, 0x4 | 0x8), (3.0, 1965.0, 0x40)]
     s = c.summary()
     assert s["sm_mhz"] == 1882.5 and s["sm_max_mhz"] == 1965 and s["samples"] == 4
     assert s["reasons"] == ["hw_slowdown", "hw_thermal_slowdown", "sw_power_cap"]
+    # a window: only its samples; a window between samples takes the nearest one
+    w = c.summary(0.5, 2.5)
+    assert w["samples"] == 2 and w["sm_mhz"] == 1750.0 and w["reasons"] == ["hw_slowdown", "sw_power_cap"]
+    n = c.summary(2.9, 2.95)
+    assert n["samples"] == 1 and n["sm_mhz"] == 1965.0 and n["reasons"] == ["hw_thermal_slowdown"]
+
+
+def test_speed_lines_parse_like_the_reference_sweep():
+    """Median of the `speed = X (MLUPS)` lines with the first skipped
+    (analysis/blocking_experiments.py:40,115), from both drivers' output."""
+    sys.path.insert(0, ROOT)
+    import bench
+    out = ("Init flag successfully\nspeed = 100.0000 (MLUPS)\nspeed = 25000.5000 (MLUPS)\n"
+           "speed = 26000.0000 (MLUPS)\nspeed = 27000.2500 (MLUPS)\n")
+    assert bench.parse_speeds(out) == 26000.0
+    assert bench.parse_speeds("no speed here") is None
+    assert set(bench.REF_BINARY_LEGS) >= {"readme_00", "retuned_00", "readme_13"}
+
+
+def test_both_arms_share_the_config():
+    sys.path.insert(0, ROOT)
+    import bench
+    from culbm_b200 import scenes
+    sc = scenes.sphere_64()
+    a, b = bench.workload_config(sc, 1), bench.workload_config(sc, 1)
+    assert a == b and set(a) == {"workload", "cells", "solid_fraction", "storage", "l2", "parallelism"}
 
 
 def test_roofline_traffic_is_the_committed_profile():

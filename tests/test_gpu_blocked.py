@@ -146,3 +146,20 @@ def test_blocked_random_geometries(culbm, orc, seed):
     for sp in (1, 0):
         got, info = run_blocked(culbm, sc, sp, 3, tile, inner, nsteps, graphs=bool(seed % 2))
         assert np.array_equal(bits(got), bits(want)), (dims, tile, inner, sp)
+
+
+@pytest.mark.parametrize("sp,op,ring", [(1, 3, False), (1, 3, True), (0, 3, False), (1, 1, False)])
+def test_blocked_without_cache_hints_equals_pull(culbm, orc, sp, op, ring):
+    """cache_hints = 0 (no evict-first / evict-last hints, the reference build
+    switch CULBM_EXPT_CACHE_HINT_POLICY=0 of src/simulator/single_dev_expt/
+    CMakeLists.txt:28-41): the same bits as the plain pull."""
+    sc = S.reference_channel_cube(37, 29, 23, 0.05)
+    nsteps = 13
+    want = oracle_pulled(orc, sc, 0.6, nsteps)
+    with culbm.Simulation(sc.shape, stream_policy=sp, opt_policy=op, inv_tau=0.6, inner_loop=3, tile=(16, 12, 10),
+                          use_ring=ring, cache_hints=False) as sim:
+        sim.load_state(*sc.arrays())
+        sim.step(nsteps)
+        got = sim.pulled_ddf()
+    assert np.array_equal(bits(got), bits(want))
+
