@@ -271,8 +271,9 @@ def mixed_precision_512(culbm, steps):
 def adjoint_runs():
     """Gradient of the pressure drop on the soft-obstacle channels: the
     128x64x64 case (FP32, window 300-500, checkpoints every 50) and the
-    288x272x280 case (48 bumps, 2000 steps, FP16-SR states, plan chosen for
-    a 120 GB budget) with its gradient error against FP32 states."""
+    288x272x280 case (48 bumps, 2000 steps, plan chosen for a 120 GB budget)
+    with FP32 states, FP16-SR states, and an FP32 forward pass with FP16-SR
+    checkpoints, the last two with their gradient error against FP32 states."""
     from culbm_b200 import scenes
     from culbm_b200.adjoint import AdjointProblem
 
@@ -284,7 +285,8 @@ def adjoint_runs():
             inf = p.info()
         n, T = sc.n, window[1]
         total = inf["forward_ms"] + inf["recompute_ms"] + inf["adjoint_ms"]
-        summary = {"storage": storage, "J": J, "dJ_dinv_tau": gt,
+        summary = {"storage": storage, "checkpoint_storage": kw.get("checkpoint_storage") or storage, "J": J,
+                   "dJ_dinv_tau": gt,
                    "checkpoint_every": inf["checkpoint_every"], "checkpoint_inner": inf["checkpoint_inner"],
                    "device_gb": round(inf["device_bytes"] / 1e9, 2),
                    "forward_ms": round(inf["forward_ms"], 2), "recompute_ms": round(inf["recompute_ms"], 2),
@@ -299,17 +301,22 @@ def adjoint_runs():
     out["channel_128x64x64"], _ = run((128, 64, 64), 16, (300, 500), "fp32", checkpoint_every=50)
     budget = 120e9
     big = {}
-    for st in ("fp16sr", "fp32"):
-        big[st] = run((288, 272, 280), 48, (1500, 2000), st, checkpoint_every=0, hbm_budget_bytes=int(budget))
-    g16, g32 = big["fp16sr"][1], big["fp32"][1]
+    for name, st, ck in (("fp16sr", "fp16sr", None), ("fp32", "fp32", None), ("fp32_ck_fp16sr", "fp32", "fp16sr")):
+        big[name] = run((288, 272, 280), 48, (1500, 2000), st, checkpoint_every=0, hbm_budget_bytes=int(budget),
+                        checkpoint_storage=ck)
+    g32 = big["fp32"][1]
 
     def rel(a, b):
         return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / max(np.linalg.norm(np.asarray(b)), 1e-300))
 
+    def versus(g):
+        return {"J_rel": rel(g[0], g32[0]), "dJ_dinv_tau_rel": rel(g[1], g32[1]),
+                "dJ_dsoft_rel_l2": rel(g[2], g32[2]), "dJ_dvx_in_rel_l2": rel(g[3][1], g32[3][1])}
+
     out["channel_288x272x280"] = {
         "hbm_budget_gb": budget / 1e9, "fp16sr": big["fp16sr"][0], "fp32": big["fp32"][0],
-        "fp16sr_vs_fp32": {"J_rel": rel(g16[0], g32[0]), "dJ_dinv_tau_rel": rel(g16[1], g32[1]),
-                           "dJ_dsoft_rel_l2": rel(g16[2], g32[2]), "dJ_dvx_in_rel_l2": rel(g16[3][1], g32[3][1])}}
+        "fp32_ck_fp16sr": big["fp32_ck_fp16sr"][0],
+        "fp16sr_vs_fp32": versus(big["fp16sr"][1]), "fp32_ck_fp16sr_vs_fp32": versus(big["fp32_ck_fp16sr"][1])}
     return out
 
 

@@ -90,7 +90,8 @@ class AdjConfig(C.Structure):
         ("storage", C.c_int32),
         ("hbm_budget_bytes", C.c_uint64),
         ("checkpoint_inner", C.c_int32),
-        ("reserved", C.c_uint32 * 7),
+        ("checkpoint_storage", C.c_int32),
+        ("reserved", C.c_uint32 * 6),
     ]
 
 

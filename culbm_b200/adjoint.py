@@ -29,7 +29,11 @@ class AdjointProblem:
 
     def __init__(self, domain: Sequence[int], window=(300, 500), planes=(1, None), inv_tau=0.5,
                  checkpoint_every: int = 50, precision: str = "fp32", storage: Optional[str] = None,
-                 hbm_budget_bytes: int = 0, dev_id: int = 0, checkpoint_inner: int = 0):
+                 hbm_budget_bytes: int = 0, dev_id: int = 0, checkpoint_inner: int = 0,
+                 checkpoint_storage: Optional[str] = None):
+        """checkpoint_storage ("fp16sr" or "fp16" with storage "fp32"): the
+        forward pass and J in FP32, its checkpoints and the recomputed states
+        of the reverse sweep in that 16-bit format."""
         cfg = _capi.AdjConfig()
         check(lib().culbm_adj_config_init(C.byref(cfg)))
         cfg.dev_id = dev_id
@@ -46,6 +50,7 @@ class AdjointProblem:
         cfg.storage = _capi.STORAGE[storage]
         cfg.hbm_budget_bytes = int(hbm_budget_bytes)
         cfg.checkpoint_inner = int(checkpoint_inner)
+        cfg.checkpoint_storage = 0 if checkpoint_storage is None else _capi.STORAGE[checkpoint_storage]
         self.domain = tuple(int(v) for v in domain)
         self.n = self.domain[0] * self.domain[1] * self.domain[2]
         self._h = C.c_void_p()

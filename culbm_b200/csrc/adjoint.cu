@@ -634,6 +634,16 @@ __global__ void k_fill_rest(S* base, long long count)
         Cvt<S, R>::st(base + j, R(0));
 }
 
+// An FP32 state narrowed to the 16-bit format S, population d of cell i
+// rounded as a step seeded by `seed` stores it (grid y = direction).
+template <typename S>
+__global__ void __launch_bounds__(256) k_narrow_state(const float* src, S* dst, long long n, uint32_t seed)
+{
+    const int d = blockIdx.y;
+    for (long long i = blockIdx.x * 256ll + threadIdx.x; i < n; i += 256ll * gridDim.x)
+        put(dst + d * n + i, src[d * n + i], cell_hash(static_cast<uint32_t>(i), seed), d);
+}
+
 }  // namespace adj
 }  // namespace culbm
 
@@ -657,6 +667,9 @@ struct culbm_adj {
     void* d_ckpt = nullptr;     // nckpt states: F^t for t = 0, K, 2K, ...
     void* d_inner = nullptr;    // ninner states inside one outer segment (two levels only)
     void* d_seg = nullptr;      // nseg states (at least 2)
+    bool mixed = false;         // FP32 forward pass, 16-bit checkpoints (checkpoint_storage)
+    int state_storage = 0;      // storage of the checkpoint, inner and segment states
+    void* d_fwd[2] = {nullptr, nullptr};   // FP32 ping-pong states of the mixed forward pass
     void* d_nu = nullptr;       // 2 x 27 N of the arithmetic type
     double* d_gsoft = nullptr;
     double* d_gtau = nullptr;
@@ -701,6 +714,8 @@ void adj_release(culbm_adj* a)
     cudaFree(a->d_ckpt);
     cudaFree(a->d_inner);
     cudaFree(a->d_seg);
+    cudaFree(a->d_fwd[0]);
+    cudaFree(a->d_fwd[1]);
     cudaFree(a->d_nu);
     cudaFree(a->d_gsoft);
     cudaFree(a->d_gtau);
@@ -717,7 +732,7 @@ void adj_release(culbm_adj* a)
 template <class F>
 culbm_status adj_with_storage(const culbm_adj* a, F&& f)
 {
-    switch (a->cfg.storage) {
+    switch (a->state_storage) {
         case CULBM_STORAGE_F32: return f(Tag<float>{});
         case CULBM_STORAGE_F16: return f(Tag<__half>{});
         case CULBM_STORAGE_F16_SR: return f(Tag<Half16SR>{});
@@ -843,6 +858,35 @@ culbm_status run_forward(culbm_adj* a, bool checkpoints)
     return forward_run<S>(a, 0, T, s0, slot_of, true);
 }
 
+// The forward pass of the mixed mode: FP32 states (ping-pong), the objective
+// recorded from them, and every K-th state narrowed into its 16-bit
+// checkpoint slot (format S).
+template <typename S>
+culbm_status run_forward_mixed(culbm_adj* a, bool checkpoints)
+{
+    if constexpr (!Is16<S>::value) {
+        return fail(CULBM_ERR_UNSUPPORTED, "16-bit checkpoint storage only");
+    } else {
+    const int T = a->cfg.window[1], K = a->K;
+    float* b[2] = {static_cast<float*>(a->d_fwd[0]), static_cast<float*>(a->d_fwd[1])};
+    CULBM_TRY(fill_rest<float>(a, b[0]));
+    const dim3 ng(592, 27);
+    auto narrow = [&](int t) -> culbm_status {
+        adj::k_narrow_state<S><<<ng, 256, 0, a->stream>>>(b[t & 1], state_ptr<S>(a, CKPT, t / K), a->n,
+                                                         step_seed(static_cast<uint32_t>(t > 0 ? t - 1 : 0)));
+        CULBM_CUDA(cudaGetLastError());
+        return CULBM_OK;
+    };
+    if (checkpoints) CULBM_TRY(narrow(0));
+    for (int tb = 0; tb < T; tb += K) {
+        const int te = std::min(T, tb + K);
+        CULBM_TRY(forward_run<float>(a, tb, te, b[tb & 1], [&](int t) -> float* { return b[t & 1]; }, true));
+        if (checkpoints && te % K == 0) CULBM_TRY(narrow(te));
+    }
+    return CULBM_OK;
+    }
+}
+
 // Reverse sweep over the steps t in [tb, te) (te - tb <= nseg + 1) starting
 // from the state F^tb: recompute F^{tb+1} .. F^{te-1} into the segment
 // slots (unless they are already there), then run the adjoint steps
@@ -891,7 +935,11 @@ culbm_status run_gradient(culbm_adj* a)
     const dim3 grid = cell_grid(a->dom), block = cell_block();
 
     CULBM_CUDA(cudaEventRecord(a->ev[0], a->stream));
-    CULBM_TRY(run_forward<S>(a, true));
+    if (a->mixed) {
+        CULBM_TRY(run_forward_mixed<S>(a, true));
+    } else {
+        CULBM_TRY(run_forward<S>(a, true));
+    }
     a->t_fwd = elapsed(a);
 
     CULBM_CUDA(cudaMemsetAsync(a->d_gsoft, 0, a->n * sizeof(double), a->stream));
@@ -917,7 +965,8 @@ culbm_status run_gradient(culbm_adj* a)
         S* ck = state_ptr<S>(a, CKPT, k);
         if (K2 == 0) {
             // the forward pass left the last segment's states in place
-            const bool last = k == (T - 1) / K;
+            // (not in the mixed mode, whose forward states are FP32)
+            const bool last = !a->mixed && k == (T - 1) / K;
             CULBM_TRY(adjoint_segment<S>(a, tb, te, ck, g, nu, cur, rec, adjms, last));
             continue;
         }
@@ -1041,7 +1090,17 @@ culbm_status culbm_adj_create(const culbm_adj_config* cfg, culbm_adj** out)
     a->n = static_cast<long long>(n);
     a->dom.n = static_cast<int>(n);
     a->inv_tau = c.inv_tau;
-    a->esize = c.storage == CULBM_STORAGE_F64 ? 8 : c.storage == CULBM_STORAGE_F32 ? 4 : 2;
+    a->state_storage = c.storage;
+    if (c.checkpoint_storage != 0 && c.checkpoint_storage != c.storage) {
+        if (c.storage != CULBM_STORAGE_F32 ||
+            (c.checkpoint_storage != CULBM_STORAGE_F16 && c.checkpoint_storage != CULBM_STORAGE_F16_SR)) {
+            delete a;
+            return fail(CULBM_ERR_UNSUPPORTED, "checkpoint_storage F16 or F16_SR goes with storage F32");
+        }
+        a->mixed = true;
+        a->state_storage = c.checkpoint_storage;
+    }
+    a->esize = a->state_storage == CULBM_STORAGE_F64 ? 8 : a->state_storage == CULBM_STORAGE_F32 ? 4 : 2;
     a->rsize = f64 ? 8 : 4;
     const int T = c.window[1];
     const double state_bytes = 27.0 * n * a->esize;
@@ -1058,7 +1117,8 @@ culbm_status culbm_adj_create(const culbm_adj_config* cfg, culbm_adj** out)
         // per-cell inputs and gradients, EQU list and block slots, objective
         // planes and sums
         const double fixed = 2.0 * 27 * n * a->rsize + 5.0 * 8 * n + 27.0 * n +
-                             16.0 * (c.window[1] - c.window[0] + 1) * (1.0 + c.domain_dim[1] * c.domain_dim[2]);
+                             16.0 * (c.window[1] - c.window[0] + 1) * (1.0 + c.domain_dim[1] * c.domain_dim[2]) +
+                             (a->mixed ? 2.0 * 27 * n * sizeof(float) : 0.0);
         double budget = static_cast<double>(c.hbm_budget_bytes);
         if (budget == 0) {
             size_t free_b = 0, total_b = 0;
@@ -1099,6 +1159,9 @@ culbm_status culbm_adj_create(const culbm_adj_config* cfg, culbm_adj** out)
         if (a->ninner)
             CULBM_TRY(adj_alloc(a, &a->d_inner, static_cast<size_t>(a->ninner * state_bytes), "inner checkpoints"));
         CULBM_TRY(adj_alloc(a, &a->d_seg, static_cast<size_t>(a->nseg * state_bytes), "recompute segment"));
+        if (a->mixed)
+            for (int k = 0; k < 2; ++k)
+                CULBM_TRY(adj_alloc(a, &a->d_fwd[k], 27ull * n * sizeof(float), "FP32 forward states"));
         CULBM_TRY(adj_alloc(a, &a->d_nu, 2ull * 27 * n * a->rsize, "adjoint populations"));
         CULBM_TRY(adj_alloc(a, &p, n * sizeof(double), "soft gradient"));
         a->d_gsoft = static_cast<double*>(p);
@@ -1237,7 +1300,10 @@ culbm_status culbm_adj_forward(culbm_adj* a, double* J)
     if (!a || !J) return fail(CULBM_ERR_INVALID_ARGUMENT, "NULL argument");
     CULBM_CUDA(cudaSetDevice(a->dev));
     CULBM_CUDA(cudaEventRecord(a->ev[0], a->stream));
-    CULBM_TRY(adj_with_storage(a, [&](auto tag) { return run_forward<typename decltype(tag)::type>(a, false); }));
+    CULBM_TRY(adj_with_storage(a, [&](auto tag) {
+        using S = typename decltype(tag)::type;
+        return a->mixed ? run_forward_mixed<S>(a, false) : run_forward<S>(a, false);
+    }));
     a->t_fwd = elapsed(a);
     return objective(a, J);
 }

@@ -346,7 +346,12 @@ typedef struct culbm_adj_config {
     int32_t checkpoint_inner;      /* K2 with K > 0: two levels.  Each K segment is recomputed once, keeping
                                       states every K2 steps, then swept K2 steps at a time; 1 <= K2 < K.
                                       0 = one level (default) */
-    uint32_t reserved[7];
+    int32_t checkpoint_storage;    /* states kept for the reverse sweep.  0 (default): as `storage`.  With
+                                      storage CULBM_STORAGE_F32: CULBM_STORAGE_F16 or _F16_SR runs the forward
+                                      pass (and J) in FP32 and keeps its checkpoints in that 16-bit format; the
+                                      recomputation between checkpoints and the reverse sweep then use 16-bit
+                                      states, so a one-level plan needs about half the memory */
+    uint32_t reserved[6];
 } culbm_adj_config;
 
 typedef struct culbm_adj culbm_adj;

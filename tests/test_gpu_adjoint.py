@@ -173,6 +173,31 @@ def test_fp32_adjoint_close_to_fp64():
     assert abs(res["fp32"][1] - res["fp64"][1]) <= 1e-3 * abs(res["fp64"][1])
 
 
+@pytest.mark.parametrize("ck,tol", [("fp16sr", 1e-3), ("fp16", 1e-2)])
+def test_fp32_forward_with_16bit_checkpoints(ck, tol):
+    """checkpoint_storage: the forward pass runs in FP32 (J bit for bit that
+    of the FP32 mode), checkpoints and the reverse sweep's states are 16-bit.
+    The gradients stay within `tol` (relative L2) of the FP32 mode's, closer
+    than those of the all-16-bit mode, whose forward trajectory itself is
+    rounded every step (nearest-even checkpoints drift more than stochastic
+    ones)."""
+    dims = (48, 24, 24)
+    sc, f, r, ux, uy, uz, soft = case(*dims, bumps=8)
+    res, info = {}, {}
+    for name, kw in (("fp32", {}), ("mixed", {"checkpoint_storage": ck}), ("all16", {"storage": ck})):
+        with AdjointProblem(dims, window=(60, 120), checkpoint_every=12, **kw) as p:
+            p.set_state(f, r, ux, uy, uz, soft)
+            res[name] = p.gradient()
+            info[name] = p.info()
+            assert p.forward() == res[name][0]
+    assert res["mixed"][0] == res["fp32"][0]
+    e_mixed, e_all16 = rel(res["mixed"][2], res["fp32"][2]), rel(res["all16"][2], res["fp32"][2])
+    assert e_mixed < tol and e_mixed < e_all16, (e_mixed, e_all16)
+    assert abs(res["mixed"][1] - res["fp32"][1]) <= tol * abs(res["fp32"][1])
+    assert rel(res["mixed"][3][1], res["fp32"][3][1]) < tol
+    assert info["mixed"]["checkpoint_every"] == 12
+
+
 def test_torch_shim_backward():
     dims = (16, 8, 8)
     sc, f, r, ux, uy, uz, soft = case(*dims, bumps=3)
