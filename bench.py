@@ -493,6 +493,12 @@ def run_ours(args):
         return
 
     achieved = BYTES_PER_LUP["fp32"] * sc.n / (ms / args.steps * 1e-3) / 1e9
+    if args.headline_only:
+        clocks.stop()
+        print(json.dumps({"metric": METRIC, "value": round(value, 1), "unit": "MLUPS", "n_gpus": ws,
+                          "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4),
+                          "headline_only": True, "gpu_launches": launches, "clocks": headline_clocks}), flush=True)
+        return
     extra = {}
     k2 = max(20, args.steps // 4)
     from culbm_b200 import selector
@@ -638,6 +644,8 @@ def main():
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--err-steps", type=int, default=1000)
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint runs (about 30 s)")
+    ap.add_argument("--headline-only", action="store_true",
+                    help="time the headline and print its line without the other legs (for profiler launch lists)")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be at least 3")

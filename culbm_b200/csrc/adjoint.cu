@@ -68,7 +68,7 @@ struct Args {
 // Pull of the 27 populations of cell (x, y, z) from the state a.src with the
 // per-axis clamp (the same rule as the plain pull step).
 // With ROWS == ROWS_INNER the cell is known to lie off the y and z faces;
-// RAW loads the stored values without the format's scale (ld_raw).
+// RAW loads the stored values without the format's scale (ld_stream_raw).
 template <int ROWS = ROWS_OUTER, bool RAW = false, typename S, typename R>
 __device__ __forceinline__ void pull_state(const Args<S, R>& a, int x, int y, int z, int i, R* f)
 {
@@ -83,7 +83,7 @@ __device__ __forceinline__ void pull_state(const Args<S, R>& a, int x, int y, in
         const int oy = cy_of(d) == 1 ? ndy : cy_of(d) == -1 ? pdy : 0;
         const int oz = cz_of(d) == 1 ? ndz : cz_of(d) == -1 ? pdz : 0;
         const S* p = a.src.p[d] + (i + ox + oy + oz);
-        f[d] = RAW ? ld_raw<S, R>(p) : Cvt<S, R>::ld(p);
+        f[d] = RAW ? ld_stream_raw<S, R>(p) : Cvt<S, R>::ld(p);
     }
 }
 
@@ -487,7 +487,7 @@ __device__ __forceinline__ void adj_cell(const Args<S, R>& a, const CellCoord c,
         });
         for_dirs([&](auto dd) {
             constexpr int d = decltype(dd)::value;
-            const R v = ld_raw<S, R>(a.src.p[d] + (c.i - nb_off(D, d)));
+            const R v = ld_stream_raw<S, R>(a.src.p[d] + (c.i - nb_off(D, d)));
             m.template add<d>(v);
             dots.template add<d>(l, v);
         });
@@ -505,7 +505,7 @@ __device__ __forceinline__ void adj_cell(const Args<S, R>& a, const CellCoord c,
             const int ox = cx_of(d) == 1 ? ndx : cx_of(d) == -1 ? pdx : 0;
             const int oy = cy_of(d) == 1 ? ndy : cy_of(d) == -1 ? pdy : 0;
             const int oz = cz_of(d) == 1 ? ndz : cz_of(d) == -1 ? pdz : 0;
-            const R v = ld_raw<S, R>(a.src.p[d] + (c.i + ox + oy + oz));
+            const R v = ld_stream_raw<S, R>(a.src.p[d] + (c.i + ox + oy + oz));
             m.template add<d>(v);
             dots.template add<d>(l, v);
         });

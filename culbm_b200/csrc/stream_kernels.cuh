@@ -161,14 +161,14 @@ __device__ __forceinline__ void cell_update_for(uint8_t op, R inv_tau, const flo
         cell_update<R, E>(op, inv_tau, rho, vx, vy, vz, i, f);
 }
 
-// Load of a stored population: the value f, or with RAW its raw form
-// 2^E * f (ld_raw, E = ScaleExp<S>) for kernels that fold the scale into the
-// cell update.
+// Load of a stored population from global memory: the value f, or with RAW
+// its raw form 2^E * f (E = ScaleExp<S>) for the step kernels, which fold the
+// scale into the cell update and stream the planes (ld_stream_raw).
 template <bool RAW, typename S, typename R>
 __device__ __forceinline__ R ld_as(const S* p)
 {
     if constexpr (RAW)
-        return ld_raw<S, R>(p);
+        return ld_stream_raw<S, R>(p);
     else
         return Cvt<S, R>::ld(p);
 }
@@ -362,14 +362,14 @@ __device__ __forceinline__ void aa_odd_cell(const StepArgs<S, R>& a, const CellC
     if (op & OP_LOAD) {
         if (ROWS == ROWS_INNER && !xface) {
 #pragma unroll
-            for (int d = 0; d < 27; ++d) f[d] = ld_raw<S, R>(a.src.p[26 - d] + (c.i - nb_off(D, d)));
+            for (int d = 0; d < 27; ++d) f[d] = ld_stream_raw<S, R>(a.src.p[26 - d] + (c.i - nb_off(D, d)));
         } else if (ROWS == ROWS_INNER) {
 #pragma unroll
             for (int d = 0; d < 27; ++d) {
                 const S* p = a.src.p[26 - d] + (c.i - nb_off(D, d));
                 if (cx_of(d) == 1 && c.x == 0) p = xface_edge_ptr(a.edge, D, a.el, 0, d, c.y, c.z);
                 if (cx_of(d) == -1 && c.x == D.nx - 1) p = xface_edge_ptr(a.edge, D, a.el, 1, d, c.y, c.z);
-                f[d] = ld_raw<S, R>(p);
+                f[d] = ld_stream_raw<S, R>(p);
             }
         } else {
             load_pulled<LAYOUT_AA_A, true>(a, c.x, c.y, c.z, c.i, true, f);
