@@ -11,6 +11,7 @@
 //                         the alignments a row start can take;
 //              p = 1 - exp(-V / (L2 - V)), V = tile bytes (0 once V >= L2)
 //   S(B, I)  = h / ((1 + alpha h) / (2 I) + lambda (1 - 1/I))
+//              (with a compute floor for issue-bound storage formats, below)
 // lambda = DRAM bandwidth / L2 bandwidth (copy kernels; 16-byte accesses,
 // which B200 needs to reach its HBM bandwidth), gamma = cost of a
 // partial sector relative to a full one in a streaming store.  The search
@@ -117,8 +118,14 @@ void beta(int bx, int i, double* sec, double* edge)
     *edge = 4.0 * n_edge / (static_cast<double>(period) * len);
 }
 
+// S of the model, with a compute floor added here: `compute` is the plain
+// step's time per update over its DRAM streaming time (0: memory-bound, the
+// reference's model unchanged).  A round's time per valid update is then the
+// larger of its memory time D / h and its compute time compute / h (the
+// halo cells are computed too), against max(1, compute) for plain streaming:
+//   S = h max(1, compute) / max(D, compute),  D = (1 + alpha h) / (2 I) + lambda (1 - 1/I).
 double speedup(int bx, int by, int bz, int i, double lambda, double gamma, double l2, double cell_bytes,
-               bool with_alpha)
+               bool with_alpha, double compute)
 {
     const double r = i - 1;
     const double h = (1 - 2 * r / bx) * (1 - 2 * r / by) * (1 - 2 * r / bz);
@@ -130,7 +137,18 @@ double speedup(int bx, int by, int bz, int i, double lambda, double gamma, doubl
         const double p = v < l2 ? 1.0 - std::exp(-v / (l2 - v)) : 0.0;
         alpha = 1 + lambda * (bs - 1) + p * (2 * gamma - (1 + lambda)) * be;
     }
-    return h / ((1 + alpha * h) / (2.0 * i) + lambda * (1 - 1.0 / i));
+    const double D = (1 + alpha * h) / (2.0 * i) + lambda * (1 - 1.0 / i);
+    return h * std::max(1.0, compute) / std::max(D, compute);
+}
+
+// The compute floor of a storage format on B200: 16-bit steps are bound by
+// instruction issue (CULBM_B200_COMPUTE_16), FP32 and FP64 by memory.
+double compute_of(int32_t storage)
+{
+    return (storage == CULBM_STORAGE_F16 || storage == CULBM_STORAGE_BF16 || storage == CULBM_STORAGE_F16_SR ||
+            storage == CULBM_STORAGE_BF16_SR)
+               ? CULBM_B200_COMPUTE_16
+               : 0.0;
 }
 
 culbm_status resolve_constants(double& lambda, double& gamma)
@@ -231,6 +249,7 @@ culbm_status culbm_select_tile(const uint32_t domain_dim[3], int32_t storage, do
     CULBM_TRY(resolve_constants(lambda, gamma));
     CULBM_TRY(resolve_l2(l2_bytes, &persist_bytes));
     const double cell_bytes = cell_bytes_of(storage);
+    const double compute = compute_of(storage);
     const double l2 = static_cast<double>(l2_bytes);
     double best = -1;
     // tile widths: the reference's multiples of 32 up to 160, and whole rows
@@ -248,14 +267,14 @@ culbm_status culbm_select_tile(const uint32_t domain_dim[3], int32_t storage, do
                     bool ok = true;
                     for (int k = 0; k < 3 && ok; ++k) ok = valid_blk_axis(domain_dim[k], b[k], static_cast<uint32_t>(i));
                     if (!ok) continue;
-                    const double sp = speedup(bx, by, bz, i, lambda, gamma, l2, cell_bytes, true);
+                    const double sp = speedup(bx, by, bz, i, lambda, gamma, l2, cell_bytes, true, compute);
                     if (sp > best) {
                         best = sp;
                         for (int k = 0; k < 3; ++k) out->tile[k] = b[k];
                         out->inner_loop = i;
                         out->predicted_speedup = sp;
                         out->predicted_speedup_no_alignment =
-                            speedup(bx, by, bz, i, lambda, gamma, l2, cell_bytes, false);
+                            speedup(bx, by, bz, i, lambda, gamma, l2, cell_bytes, false, compute);
                     }
                 }
         }
@@ -272,9 +291,9 @@ culbm_status culbm_blocking_speedup(const uint32_t tile[3], int32_t inner_loop, 
     CULBM_TRY(resolve_constants(lambda, gamma));
     CULBM_TRY(resolve_l2(l2_bytes, nullptr));
     const int bx = static_cast<int>(tile[0]), by = static_cast<int>(tile[1]), bz = static_cast<int>(tile[2]);
-    const double cb = cell_bytes_of(storage), l2 = static_cast<double>(l2_bytes);
-    *speedup_out = speedup(bx, by, bz, inner_loop, lambda, gamma, l2, cb, true);
-    if (speedup_no_alignment) *speedup_no_alignment = speedup(bx, by, bz, inner_loop, lambda, gamma, l2, cb, false);
+    const double cb = cell_bytes_of(storage), l2 = static_cast<double>(l2_bytes), c = compute_of(storage);
+    *speedup_out = speedup(bx, by, bz, inner_loop, lambda, gamma, l2, cb, true, c);
+    if (speedup_no_alignment) *speedup_no_alignment = speedup(bx, by, bz, inner_loop, lambda, gamma, l2, cb, false, c);
     return CULBM_OK;
 }
 

@@ -271,11 +271,20 @@ typedef struct culbm_tile_choice {
  * (DRAM copy 6.48 TB/s, L2 copy 13.4 TB/s; a partial sector costs 8.8 full ones). */
 #define CULBM_B200_LAMBDA 0.4841
 #define CULBM_B200_GAMMA 8.772
+/* The 16-bit formats' plain step is bound by instruction issue, not DRAM: its
+ * time per update over the DRAM time of its 108 bytes at the copy bandwidth
+ * (FP16-SR pull: 36.2k MLUPS against 60.6k) on a B200.  The model takes the
+ * larger of memory and compute time per update, so for these formats every
+ * blocked tile predicts S < 1 (the halo cells cost compute and save only
+ * bandwidth) and the tile of largest S is the one with the least halo. */
+#define CULBM_B200_COMPUTE_16 1.67
 
 /* The tile and innerLoop of the largest model speed-up for `domain_dim` and
- * population storage `storage` (CULBM_STORAGE_*).  lambda, gamma <= 0: the
- * B200 values above; l2_bytes, persist_bytes == 0: the current device's L2
- * size and persisting-L2 limit. */
+ * population storage `storage` (CULBM_STORAGE_*), with the compute floor of
+ * the 16-bit formats (CULBM_B200_COMPUTE_16).  lambda, gamma <= 0: the B200
+ * values above; l2_bytes, persist_bytes == 0: the current device's L2 size and
+ * persisting-L2 limit.  A predicted speed-up below 1 means plain streaming
+ * is faster. */
 culbm_status culbm_select_tile(const uint32_t domain_dim[3], int32_t storage, double lambda, double gamma,
                                uint64_t l2_bytes, uint64_t persist_bytes, culbm_tile_choice* out);
 
