@@ -52,6 +52,7 @@
 #pragma once
 
 #include <cstdint>
+#include <type_traits>
 
 #include "culbm.h"
 #include "stream_kernels.cuh"
@@ -107,6 +108,22 @@ __host__ __device__ constexpr int row_consumer_warps(int nx) { return (nx + 31) 
 __device__ __forceinline__ uint32_t smem_addr(const void* p)
 {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// 16-bit shared-memory store at a 32-bit shared address.
+__device__ __forceinline__ void sts16(uint32_t addr, unsigned short v)
+{
+    asm volatile("st.shared.u16 [%0], %1;" ::"r"(addr), "h"(v));
+}
+
+// Raw value 2^E f of a stored 16-bit pattern (the ld_raw of storage.cuh).
+template <typename S>
+__device__ __forceinline__ float raw16_to_float(unsigned short b)
+{
+    if constexpr (std::is_same<S, __half>::value || std::is_same<S, Half16SR>::value)
+        return __half2float(__ushort_as_half(b));
+    else
+        return __uint_as_float(static_cast<uint32_t>(b) << 16);
 }
 
 __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)

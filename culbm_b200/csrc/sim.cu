@@ -16,6 +16,7 @@
 #include <vector>
 
 #include "row_kernels.cuh"
+#include "warp_kernels.cuh"
 #include "sim_internal.cuh"
 
 namespace culbm {
@@ -319,6 +320,76 @@ culbm_status rows_launch(culbm_sim* s, const StepArgs<S, float>& a, int y0, int 
     });
 }
 
+// The warp-staged 16-bit pull (warp_kernels.cuh, kernel_variant 3 with two
+// window buffers per warp, 4 with three): plain pull with 16-bit storage and
+// nx a multiple of 8.
+bool warp_pull_applicable(const culbm_sim* s)
+{
+    return !is_blocked(s->cfg) && s->esize == 2 && (s->cfg.kernel_variant == 3 || s->cfg.kernel_variant == 4) &&
+           s->cfg.stream_policy == CULBM_STREAM_PULL && s->dom.nx % 8 == 0;
+}
+
+using PfnEncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                    const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                    CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+// The population buffer `base` as the 4-D tensor (x, y, z, d) of 16-bit
+// values with the given box.
+culbm_status encode_pop_map(const culbm_sim* s, void* base, const cuuint32_t box[4], CUtensorMap* out)
+{
+    static PfnEncodeTiled encode = nullptr;
+    if (encode == nullptr) {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        CULBM_CUDA(cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &fn, 12000, cudaEnableDefault, &q));
+        if (q != cudaDriverEntryPointSuccess || fn == nullptr)
+            return fail(CULBM_ERR_CUDA, "driver lacks cuTensorMapEncodeTiled");
+        encode = reinterpret_cast<PfnEncodeTiled>(fn);
+    }
+    const Domain& D = s->dom;
+    const cuuint64_t dims[4] = {static_cast<cuuint64_t>(D.nx), static_cast<cuuint64_t>(D.ny),
+                                static_cast<cuuint64_t>(D.nz), 27};
+    const cuuint64_t strides[3] = {2ull * D.nx, 2ull * D.nxy, 2ull * s->n};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    const CUresult r = encode(out, CU_TENSOR_MAP_DATA_TYPE_UINT16, 4, base, dims, strides, box, estr,
+                              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(CULBM_ERR_CUDA, "cuTensorMapEncodeTiled failed: " + std::to_string(r));
+    return CULBM_OK;
+}
+
+template <typename S, int NB>
+culbm_status warp_pull_prepare(culbm_sim* s)
+{
+    const int smem = kWarpWarps * warp_smem_per_warp(NB);
+    CULBM_CUDA(cudaFuncSetAttribute(k_pull16_warp<S, NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    int per_sm = 0, sms = 0;
+    CULBM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pull16_warp<S, NB>, kWarpWarps * 32, smem));
+    CULBM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->dev));
+    if (per_sm < 1) return fail(CULBM_ERR_UNSUPPORTED, "warp-staged pull kernel does not fit an SM");
+    s->row_grid[ROWS_PULL] = per_sm * sms;
+    return CULBM_OK;
+}
+
+template <typename S>
+culbm_status warp_pull_setup(culbm_sim* s)
+{
+    if constexpr (Is16<S>::value) {
+        if (s->cfg.kernel_variant == 4) {
+            CULBM_TRY((warp_pull_prepare<S, 3>(s)));
+        } else {
+            CULBM_TRY((warp_pull_prepare<S, 2>(s)));
+        }
+        const cuuint32_t load_box[4] = {kWarpWin, 1, 1, 3}, store_box[4] = {32, 1, 1, 27};
+        for (int k = 0; k < 2; ++k) {
+            CULBM_TRY(encode_pop_map(s, s->d_pop[k], load_box, &s->map_load[k]));
+            CULBM_TRY(encode_pop_map(s, s->d_pop[k], store_box, &s->map_store[k]));
+        }
+        s->warp_pull = true;
+    }
+    return CULBM_OK;
+}
+
 template <typename S>
 culbm_status plain_steps(culbm_sim* s, uint32_t nsteps)
 {
@@ -327,6 +398,30 @@ culbm_status plain_steps(culbm_sim* s, uint32_t nsteps)
     for (uint32_t k = 0; k < nsteps; ++k) {
         const uint32_t seed = step_seed(static_cast<uint32_t>(s->step + k));
         if constexpr (Is16<S>::value) {
+            if (s->warp_pull) {
+                auto a = make_args<S>(s, s->cur, 1 - s->cur);
+                a.seed = seed;
+                WarpArgs16 w{};
+                w.nseg_row = (s->dom.nx + 31) / 32;
+                w.nseg = w.nseg_row * s->dom.ny * s->dom.nz;
+                w.err = s->err_dev;
+                w.debug_extra_tx = g_row_extra_tx.load();
+                WarpMaps maps;
+                maps.src = s->map_load[s->cur];
+                maps.dst = s->map_store[1 - s->cur];
+                const int blocks = (w.nseg + kWarpWarps - 1) / kWarpWarps;
+                const int grid = std::min(blocks, s->row_grid[ROWS_PULL]);
+                if (s->cfg.kernel_variant == 4)
+                    k_pull16_warp<S, 3><<<grid, kWarpWarps * 32, kWarpWarps * warp_smem_per_warp(3), s->stream>>>(
+                        a, maps, w);
+                else
+                    k_pull16_warp<S, 2><<<grid, kWarpWarps * 32, kWarpWarps * warp_smem_per_warp(2), s->stream>>>(
+                        a, maps, w);
+                CULBM_CUDA(cudaGetLastError());
+                s->cur ^= 1;
+                s->launches += 1;
+                continue;
+            }
             if (s->rows) {
                 const Domain& D = s->dom;
                 if (s->cfg.stream_policy == CULBM_STREAM_PULL) {
@@ -588,6 +683,8 @@ culbm_status culbm_create(const culbm_config* cfg, culbm_sim** out)
         CULBM_CUDA(cudaHostGetDevicePointer(reinterpret_cast<void**>(&s->err_dev), s->err_host, 0));
         if (rows_applicable(s))
             CULBM_TRY(with_storage(s, [&](auto tag) { return rows_setup<typename decltype(tag)::type>(s); }));
+        if (warp_pull_applicable(s))
+            CULBM_TRY(with_storage(s, [&](auto tag) { return warp_pull_setup<typename decltype(tag)::type>(s); }));
         const float* none[4] = {nullptr, nullptr, nullptr, nullptr};
         CULBM_TRY(upload_state(s, nullptr, none));
         s->loaded = false;   // defaults in place; a load call is still expected

@@ -2,6 +2,7 @@
 // translation units (error reporting with fault injection, launch shapes).
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -75,6 +76,9 @@ struct culbm_sim {
 
     // Row-staged 16-bit step kernels (row_kernels.cuh), when the domain suits them.
     bool rows = false;
+    bool warp_pull = false;         // warp-staged 16-bit pull (warp_kernels.cuh)
+    CUtensorMap map_load[2];        // its tensor maps of population buffer 0 and 1: window loads
+    CUtensorMap map_store[2];       // and output stores
     int row_grid[3] = {0, 0, 0};    // resident blocks per launch, by RowMode
     int* err_host = nullptr;        // mapped host word a bounded device-side wait writes on expiry
     int* err_dev = nullptr;         // its device address

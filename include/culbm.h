@@ -110,7 +110,9 @@ typedef struct culbm_config {
                                   row-staged (whole x-rows of the 27 planes staged in shared memory
                                   by bulk asynchronous copies, one block per row; 1: one output
                                   buffer, 2: two), used where nx is a multiple of 16 and at most
-                                  992.  Same bits either way */
+                                  992; 3 and 4 (pull only) warp-staged (32-cell row segments
+                                  through TMA tensor copies, two or three window buffers per
+                                  warp), used where nx is a multiple of 8.  Same bits either way */
     uint32_t reserved[7];
 } culbm_config;
 

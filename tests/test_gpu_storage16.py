@@ -167,3 +167,74 @@ def test_row_staged_wait_gives_up_and_reports(culbm):
         sim.step(2)
         sim.synchronize()
         assert np.isfinite(sim.pulled_ddf()).all()
+
+
+WARP_DOMAINS = [(40, 5, 4), (56, 6, 5), (96, 7, 6), (8, 4, 3)]
+
+
+@pytest.mark.parametrize("variant", [3, 4])
+@pytest.mark.parametrize("storage", ["fp16", "bf16", "fp16sr", "bf16sr"])
+@pytest.mark.parametrize("dims", WARP_DOMAINS)
+def test_warp_staged_pull_matches_oracle(culbm, orc, storage, dims, variant):
+    """The warp-staged 16-bit pull (kernel_variant 3 and 4, nx a multiple of 8):
+    one and several 32-cell segments per row, a partial last segment, rows
+    narrower than the 48-value window, fluid x faces (clamped pulls), solid
+    cells without STORE, EQU rows."""
+    sc = S.reference_channel(*dims, 0.05)
+    sc.flag[:, :, 0] = S.FLUID
+    sc.flag[:, :, -1] = S.FLUID
+    rng = np.random.default_rng(sum(dims) + 3)
+    solid = rng.random(sc.flag.shape) < 0.06
+    sc.flag[solid] = 0
+    for nsteps in (5, 6):
+        want = oracle_pulled16(orc, sc, storage, 0.6, nsteps)
+        with culbm.Simulation(sc.shape, stream_policy=0, inv_tau=0.6, storage=storage,
+                              kernel_variant=variant) as sim:
+            sim.load_state(*sc.arrays())
+            sim.step(nsteps)
+            got = sim.pulled_ddf()
+        assert np.array_equal(bits(got), bits(want)), (storage, dims, nsteps)
+
+
+@pytest.mark.parametrize("storage", ["fp16sr", "bf16"])
+def test_warp_staged_pull_equals_per_cell_pull(culbm, storage):
+    """kernel_variant 3, 4 and 0 give the same bits with random flags over
+    many segments per warp."""
+    dims = (168, 40, 36)
+    sc = S.default_scene(*dims)
+    rng = np.random.default_rng(23)
+    pick = rng.random(sc.flag.shape)
+    sc.flag[pick < 0.05] = S.WALL
+    sc.flag[(pick >= 0.05) & (pick < 0.07)] = S.EQUILIBRIUM
+    sc.flag[(pick >= 0.07) & (pick < 0.08)] = 0
+    sc.rho[:] = (1 + 0.01 * rng.standard_normal(sc.flag.shape)).astype(np.float32)
+    sc.vx[:] = (0.02 * rng.standard_normal(sc.flag.shape)).astype(np.float32)
+    out = []
+    for variant in (0, 3, 4):
+        with culbm.Simulation(dims, stream_policy=0, inv_tau=0.55, storage=storage, kernel_variant=variant) as sim:
+            sim.load_state(*sc.arrays())
+            sim.step(9)
+            out.append(sim.pulled_ddf())
+    assert np.array_equal(bits(out[0]), bits(out[1]))
+    assert np.array_equal(bits(out[0]), bits(out[2]))
+
+
+def test_warp_staged_wait_gives_up_and_reports(culbm):
+    """The warp-staged pull's bounded wait: a phase that cannot complete is
+    reported as CULBM_ERR_DEVICE_TIMEOUT and the device stays usable."""
+    from culbm_b200 import _capi
+    lib = _capi.lib()
+    dims = (64, 8, 6)
+    lib.culbm_debug_row_wait_extra_bytes(16)
+    try:
+        with culbm.Simulation(dims, stream_policy=0, storage="fp16", kernel_variant=3) as sim:
+            sim.step(1)
+            rc = lib.culbm_synchronize(sim._h)
+            assert rc == 7, lib.culbm_last_error().decode()
+    finally:
+        lib.culbm_debug_row_wait_extra_bytes(0)
+    with culbm.Simulation(dims, stream_policy=0, storage="fp16", kernel_variant=3) as sim:
+        sim.step(2)
+        sim.synchronize()
+        assert np.isfinite(sim.pulled_ddf()).all()
+
