@@ -31,7 +31,7 @@ FIELD = {"rho": 0, "vx": 1, "vy": 2, "vz": 3}
 # Every symbol include/culbm.h declares.
 EXPORTED = (
     "culbm_config_init", "culbm_create", "culbm_destroy", "culbm_load_state", "culbm_load_state_folder",
-    "culbm_step", "culbm_step_timed", "culbm_synchronize", "culbm_moments", "culbm_get_field", "culbm_dump",
+    "culbm_step", "culbm_step_timed", "culbm_synchronize", "culbm_moments", "culbm_get_field", "culbm_run_host", "culbm_dump",
     "culbm_get_step", "culbm_get_pulled_ddf", "culbm_set_ddf", "culbm_mass_momentum", "culbm_mass_momentum_noalloc", "culbm_measure_memory",
     "culbm_select_tile", "culbm_blocking_speedup", "culbm_blocking_axis", "culbm_get_info",
     "culbm_last_error", "culbm_status_string", "culbm_abi_version", "culbm_debug_inject_cuda_error",
@@ -58,7 +58,8 @@ class Config(C.Structure):
         ("cache_hints", C.c_int32),
         ("use_graphs", C.c_int32),
         ("kernel_variant", C.c_int32),
-        ("reserved", C.c_uint32 * 7),
+        ("run_slabs", C.c_int32),
+        ("reserved", C.c_uint32 * 6),
     ]
 
 
@@ -162,6 +163,7 @@ def lib():
     L.culbm_synchronize.argtypes = [vp]
     L.culbm_moments.argtypes = [vp]
     L.culbm_get_field.argtypes = [vp, C.c_int, vp]
+    L.culbm_run_host.argtypes = [vp, vp, vp, vp, vp, vp, C.c_uint32, vp, vp, vp, vp]
     L.culbm_dump.argtypes = [vp, C.c_char_p, C.c_uint32]
     L.culbm_get_step.argtypes = [vp, C.POINTER(C.c_uint64)]
     L.culbm_get_pulled_ddf.argtypes = [vp, vp, C.c_int32]

@@ -133,9 +133,9 @@ culbm_status dev_alloc(culbm_sim* s, void** p, size_t bytes, const char* what)
 
 // Builds the compact op bytes from the flag words: step bits plus OP_EDGE on
 // the domain boundary.
-__global__ void k_build_ops(Domain D, const uint32_t* flag, uint8_t* ops)
+__global__ void k_build_ops(Domain D, const uint32_t* flag, uint8_t* ops, int z0)
 {
-    const CellCoord c = cell_of_thread(D);
+    const CellCoord c = cell_of_thread(D, z0);
     if (!c.valid) return;
     const uint32_t fl = flag[c.i];
     uint8_t op = static_cast<uint8_t>(fl & 0x1Fu);
@@ -455,7 +455,7 @@ culbm_status plain_steps(culbm_sim* s, uint32_t nsteps)
         if (s->cfg.stream_policy == CULBM_STREAM_PULL) {
             auto a = make_args<S>(s, s->cur, 1 - s->cur);
             a.seed = seed;
-            k_pull_step<S, R><<<g, b, 0, s->stream>>>(a);
+            k_pull_step<S, R><<<g, b, 0, s->stream>>>(a, 0);
             CULBM_CUDA(cudaGetLastError());
             s->cur ^= 1;
         } else {
@@ -505,6 +505,7 @@ culbm_status validate_config(const culbm_config& c)
         return fail(CULBM_ERR_INVALID_ARGUMENT, "streamPolicy must be 0 or 1");
     if (c.opt_policy < 0 || c.opt_policy > 3) return fail(CULBM_ERR_INVALID_ARGUMENT, "optPolicy must be 0..3");
     if (c.storage < 0 || c.storage > 5) return fail(CULBM_ERR_INVALID_ARGUMENT, "storage must be 0..5");
+    if (c.run_slabs < 0) return fail(CULBM_ERR_INVALID_ARGUMENT, "run_slabs must be 0 (automatic) or positive");
     if (!(c.inv_tau > 0.0f && c.inv_tau < 2.0f))
         return fail(CULBM_ERR_INVALID_ARGUMENT, "invTau must lie in (0, 2)");
     // The reference rejects the ring buffer outside in-place dynamic L2
@@ -526,6 +527,10 @@ void release(culbm_sim* s)
     if (s == nullptr) return;
     cudaSetDevice(s->dev);
     if (s->stream) cudaStreamSynchronize(s->stream);
+    for (auto& st : s->slab_st)
+        if (st) cudaStreamSynchronize(st);
+    for (auto& st : s->copy_st)
+        if (st) cudaStreamSynchronize(st);
     tiles_destroy(s);
     cudaFree(s->d_flag);
     cudaFree(s->d_ops);
@@ -533,6 +538,14 @@ void release(culbm_sim* s)
     for (auto& p : s->d_pop) cudaFree(p);
     cudaFree(s->d_edge);
     cudaFree(s->d_red);
+    for (auto& e : s->slab_ev)
+        if (e) cudaEventDestroy(e);
+    for (auto& e : s->run_ev)
+        if (e) cudaEventDestroy(e);
+    for (auto& st : s->slab_st)
+        if (st) cudaStreamDestroy(st);
+    for (auto& st : s->copy_st)
+        if (st) cudaStreamDestroy(st);
     if (s->ev0) cudaEventDestroy(s->ev0);
     if (s->ev1) cudaEventDestroy(s->ev1);
     if (s->stream) cudaStreamDestroy(s->stream);
@@ -559,7 +572,7 @@ culbm_status upload_state(culbm_sim* s, const uint32_t* flag, const float* const
             CULBM_CUDA(cudaGetLastError());
         }
     }
-    k_build_ops<<<cell_grid(s->dom), cell_block(), 0, s->stream>>>(s->dom, s->d_flag, s->d_ops);
+    k_build_ops<<<cell_grid(s->dom), cell_block(), 0, s->stream>>>(s->dom, s->d_flag, s->d_ops, 0);
     CULBM_CUDA(cudaGetLastError());
     if (is_blocked(s->cfg)) {
         std::vector<uint32_t> host;
@@ -574,6 +587,269 @@ culbm_status upload_state(culbm_sim* s, const uint32_t* flag, const float* const
     s->step = 0;
     s->loaded = true;
     return CULBM_OK;
+}
+
+// ------------------------------------------------- overlapped host run ---
+//
+// culbm_run_host cuts the domain into slabs of z-planes a_0 = 0 < a_1 < ...
+// < a_m = nz, at least two planes each, and skews them in time: step t of
+// slab j updates the planes [a_j - t', a_{j+1} - t') (clamped to the domain;
+// t' counts the steps of the skewed phase; slab 0 starts at 0 and the last
+// ends at nz).  A cell of a plain step reads and writes only locations
+// within one plane of itself, so
+//   step t of slab j reads what step t-1 wrote on its own region and on
+//   slab j-1's (which holds the two planes below it): it waits for nothing
+//   above, so slab 0 can take all its steps as soon as its inputs are in;
+//   steps of one t on different slabs touch disjoint locations (each
+//   location belongs to one cell per step), and so do step t on slab j and
+//   step t-1 on slab j+1: in pull mode the write sets of t and the read sets
+//   of t-1 above a_{j+1} - t' are disjoint, and in place one of the two
+//   steps touches only its own planes;
+//   the dump of slab j, on the region of the step after the last, waits for
+//   the last step on slabs j and j-1.
+// Events carry the dependencies.  One copy stream brings the slabs in, in
+// slab order; the other takes each dump region out as it finishes, so the
+// fields of low slabs leave while high slabs still step.  Only the first and
+// the last steps of a long run go slab by slab; the steps in between are
+// whole-domain launches.  The population start does not depend on the
+// inputs (rest equilibrium, as culbm_load_state), so it runs on the
+// simulation's stream while the first slab arrives.
+//
+// Order of submission.  A device runs the streams of a process on a few
+// hardware queues (8 by default), and work that shares a queue starts in the
+// order it was submitted.  The slabs' work is therefore spread over
+// kRunStreams streams (slab j on stream j mod kRunStreams) and submitted by
+// anti-diagonal d = j + t', then t': everything a task waits for has a
+// smaller d.  Each slab's four step events are a ring: step t's event is
+// waited on by step t+1 of slab j+1 (d + 2) before step t+4 records it again
+// (d + 4).
+
+constexpr int kSlabEvents = 6;   // per slab: a ring of 4 step events, inputs copied in, dump done
+constexpr int kSlabIn = 4, kSlabDump = 5;
+constexpr int kMaxSlabs = 32;
+constexpr long long kMinSlabCells = 1ll << 19;
+constexpr int kRunStreams = 4;
+
+// Slab count: culbm_config.run_slabs, or slabs of at least kMinSlabCells
+// cells (enough blocks to fill the device) and at most kMaxSlabs; at most
+// nz / 2 either way.
+int run_slabs(const culbm_sim* s)
+{
+    const Domain& D = s->dom;
+    const long long want = s->cfg.run_slabs > 0 ? s->cfg.run_slabs
+                                                : std::min<long long>(kMaxSlabs, D.n / kMinSlabCells);
+    return static_cast<int>(std::max<long long>(1, std::min<long long>(want, D.nz / 2)));
+}
+
+// First plane of slab j of nslab balanced slabs (slab_z0(nslab) = nz).
+int slab_z0(const Domain& D, int nslab, int j)
+{
+    return static_cast<int>(static_cast<long long>(j) * D.nz / nslab);
+}
+
+// First plane of slab j's region `shift` steps into a skewed phase.
+int slab_lo(const Domain& D, int nslab, int j, int shift)
+{
+    if (j <= 0) return 0;
+    if (j >= nslab) return D.nz;
+    return std::max(0, slab_z0(D, nslab, j) - shift);
+}
+
+culbm_status ensure_run_streams(culbm_sim* s, int nstream, int nslab)
+{
+    for (auto& st : s->copy_st)
+        if (!st) CULBM_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    for (auto& e : s->run_ev)
+        if (!e) CULBM_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    while (static_cast<int>(s->slab_st.size()) < nstream) {
+        cudaStream_t st = nullptr;
+        CULBM_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        s->slab_st.push_back(st);
+    }
+    while (static_cast<int>(s->slab_ev.size()) < nslab * kSlabEvents) {
+        cudaEvent_t e = nullptr;
+        CULBM_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        s->slab_ev.push_back(e);
+    }
+    return CULBM_OK;
+}
+
+// Submits the skewed steps t0 .. t1-1 slab by slab, with the op bytes of
+// each slab's planes first when `build` and the dump of each slab's region
+// after step t1 - 1 last when `dump`.  The first step waits for nothing from
+// the neighbours: it follows the population start or a join of all slabs.
+template <typename S>
+culbm_status run_slab_steps(culbm_sim* s, int nslab, int nstream, int t0, int t1, bool build, bool dump)
+{
+    using R = typename ArithOf<S>::type;
+    const Domain& D = s->dom;
+    auto ev = [&](int j, int k) { return s->slab_ev[static_cast<size_t>(j) * kSlabEvents + k]; };
+    auto planes = [&](int za, int zb) { return dim3((D.nx + 31) / 32, (D.ny + 7) / 8, zb - za); };
+    const dim3 b = cell_block();
+    const bool pull = s->cfg.stream_policy == CULBM_STREAM_PULL;
+
+    struct Task {
+        int d, t, j;   // t = t0 - 1: op bytes; t1: dump
+    };
+    std::vector<Task> tasks;
+    tasks.reserve(static_cast<size_t>(nslab) * (t1 - t0 + 2));
+    for (int j = 0; j < nslab; ++j)
+        for (int t = build ? t0 - 1 : t0; t <= (dump ? t1 : t1 - 1); ++t) tasks.push_back({j + std::max(t - t0, 0), t, j});
+    std::sort(tasks.begin(), tasks.end(), [](const Task& x, const Task& y) { return x.d != y.d ? x.d < y.d : x.t < y.t; });
+
+    for (const Task& k : tasks) {
+        const int j = k.j, t = k.t;
+        cudaStream_t st = s->slab_st[j % nstream];
+        if (t < t0) {
+            const int za = slab_z0(D, nslab, j), zb = slab_z0(D, nslab, j + 1);
+            CULBM_CUDA(cudaStreamWaitEvent(st, ev(j, kSlabIn), 0));
+            k_build_ops<<<planes(za, zb), b, 0, st>>>(D, s->d_flag, s->d_ops, za);
+            CULBM_CUDA(cudaGetLastError());
+            continue;
+        }
+        // Step t - 1 on slab j - 1 (on slab j it is earlier on the same stream).
+        if (t > t0 && j > 0 && (j - 1) % nstream != j % nstream)
+            CULBM_CUDA(cudaStreamWaitEvent(st, ev(j - 1, (t - 1) & 3), 0));
+        const int za = slab_lo(D, nslab, j, t - t0), zb = slab_lo(D, nslab, j + 1, t - t0);
+        if (t == t1) {
+            // Dump of the state after step t1 - 1, as culbm_moments.
+            if (zb > za) {
+                const int cur = pull ? t1 & 1 : 0;
+                const int layout = pull ? LAYOUT_PULL : ((t1 & 1) == 0 ? LAYOUT_AA_A : LAYOUT_AA_B);
+                auto a = make_args<S>(s, cur, cur);
+                float* const* m = s->d_mac;
+                with_layout(layout, [&](auto L) {
+                    k_moments<decltype(L)::value, S, R><<<planes(za, zb), b, 0, st>>>(a, s->d_flag, m[0], m[1], m[2],
+                                                                                    m[3], za);
+                });
+                CULBM_CUDA(cudaGetLastError());
+            }
+            CULBM_CUDA(cudaEventRecord(ev(j, kSlabDump), st));
+            continue;
+        }
+        if (zb > za) {
+            if (pull) {
+                auto a = make_args<S>(s, t & 1, 1 - (t & 1));
+                a.seed = step_seed(static_cast<uint32_t>(t));
+                k_pull_step<S, R><<<planes(za, zb), b, 0, st>>>(a, za);
+            } else {
+                auto a = make_args<S>(s, 0, 0);
+                a.seed = step_seed(static_cast<uint32_t>(t));
+                const SlabSplit q = slab_split(D, za, zb);
+                if ((t & 1) == 0)
+                    k_aa_odd_slab<S, R><<<slab_split_grid(D, q), b, 0, st>>>(a, q);
+                else
+                    k_aa_even_slab<S, R><<<slab_split_grid(D, q), b, 0, st>>>(a, q);
+            }
+            CULBM_CUDA(cudaGetLastError());
+            s->launches += 1;
+        }
+        CULBM_CUDA(cudaEventRecord(ev(j, t & 3), st));
+    }
+    return CULBM_OK;
+}
+
+// The simulation's stream waits for every slab stream (join), or every slab
+// stream for the simulation's stream (fork).
+culbm_status join_slabs(culbm_sim* s, int nstream)
+{
+    for (int k = 0; k < nstream; ++k) {
+        CULBM_CUDA(cudaEventRecord(s->slab_ev[k * kSlabEvents + kSlabDump], s->slab_st[k]));
+        CULBM_CUDA(cudaStreamWaitEvent(s->stream, s->slab_ev[k * kSlabEvents + kSlabDump], 0));
+    }
+    return CULBM_OK;
+}
+
+culbm_status fork_slabs(culbm_sim* s, int nstream, cudaEvent_t e)
+{
+    CULBM_CUDA(cudaEventRecord(e, s->stream));
+    for (int k = 0; k < nstream; ++k) CULBM_CUDA(cudaStreamWaitEvent(s->slab_st[k], e, 0));
+    return CULBM_OK;
+}
+
+template <typename S>
+culbm_status run_host_overlapped(culbm_sim* s, const uint32_t* flag, const float* const mac[4], uint32_t nsteps,
+                                 float* const out[4])
+{
+    const Domain& D = s->dom;
+    const int nslab = run_slabs(s);
+    const int nstream = std::min(nslab, kRunStreams);
+    CULBM_TRY(ensure_run_streams(s, nstream, nslab));
+    auto ev = [&](int j, int k) { return s->slab_ev[static_cast<size_t>(j) * kSlabEvents + k]; };
+    cudaStream_t h2d = s->copy_st[0], d2h = s->copy_st[1];
+    const int T = static_cast<int>(nsteps);
+
+    // Everything follows the simulation's earlier work.
+    CULBM_CUDA(cudaEventRecord(s->run_ev[0], s->stream));
+    CULBM_CUDA(cudaStreamWaitEvent(h2d, s->run_ev[0], 0));
+    CULBM_CUDA(cudaStreamWaitEvent(d2h, s->run_ev[0], 0));
+    // Defaults of NULL inputs and the population start, on the simulation's stream.
+    const dim3 g1(1184), b1(256);
+    if (flag == nullptr) k_fill_u32<<<g1, b1, 0, s->stream>>>(s->d_flag, s->n, kDefaultFlag);
+    const float dflt[4] = {1.0f, 0.0f, 0.0f, 0.0f};
+    for (int k = 0; k < 4; ++k)
+        if (mac[k] == nullptr) k_fill_f32<<<g1, b1, 0, s->stream>>>(s->d_mac[k], s->n, dflt[k]);
+    CULBM_CUDA(cudaGetLastError());
+    CULBM_TRY(fill_rest<S>(s));
+    CULBM_TRY(fork_slabs(s, nstream, s->run_ev[1]));
+
+    // Slabs in, in slab order.
+    auto span = [&](int j, long long* off, long long* cnt) {
+        const int z0 = slab_z0(D, nslab, j), z1 = slab_z0(D, nslab, j + 1);
+        *off = static_cast<long long>(z0) * D.nxy;
+        *cnt = static_cast<long long>(z1 - z0) * D.nxy;
+    };
+    for (int j = 0; j < nslab; ++j) {
+        long long off, cnt;
+        span(j, &off, &cnt);
+        if (flag != nullptr)
+            CULBM_CUDA(cudaMemcpyAsync(s->d_flag + off, flag + off, cnt * sizeof(uint32_t), cudaMemcpyHostToDevice, h2d));
+        for (int k = 0; k < 4; ++k)
+            if (mac[k] != nullptr)
+                CULBM_CUDA(cudaMemcpyAsync(s->d_mac[k] + off, mac[k] + off, cnt * sizeof(float), cudaMemcpyHostToDevice,
+                                           h2d));
+        CULBM_CUDA(cudaEventRecord(ev(j, kSlabIn), h2d));
+    }
+
+    // Slab by slab for the first and the last nslab steps, which the copies
+    // overlap; whole-domain launches in between.  fill_rest left cur = 0 and
+    // aa_phase = 0.
+    const bool pull = s->cfg.stream_policy == CULBM_STREAM_PULL;
+    int shift_end = T;   // steps into the skewed phase that ends with the dumps
+    if (T <= 2 * nslab) {
+        CULBM_TRY(run_slab_steps<S>(s, nslab, nstream, 0, T, true, true));
+    } else {
+        const int ta = nslab, tb = T - nslab;
+        shift_end = T - tb;
+        CULBM_TRY(run_slab_steps<S>(s, nslab, nstream, 0, ta, true, false));
+        CULBM_TRY(join_slabs(s, nstream));
+        s->step = static_cast<uint64_t>(ta);
+        s->cur = pull ? ta & 1 : 0;
+        s->aa_phase = pull ? 0 : ta & 1;
+        CULBM_TRY(plain_steps<S>(s, static_cast<uint32_t>(tb - ta)));
+        CULBM_TRY(fork_slabs(s, nstream, s->run_ev[1]));
+        CULBM_TRY(run_slab_steps<S>(s, nslab, nstream, tb, T, false, true));
+    }
+    s->step = nsteps;
+    s->launched_steps += nsteps;
+    s->cur = pull ? T & 1 : 0;
+    s->aa_phase = pull ? 0 : T & 1;
+    s->loaded = true;
+
+    // The fields out as each slab's dump finishes.
+    for (int j = 0; j < nslab; ++j) {
+        const int za = slab_lo(D, nslab, j, shift_end), zb = slab_lo(D, nslab, j + 1, shift_end);
+        if (zb <= za) continue;
+        const long long off = static_cast<long long>(za) * D.nxy, cnt = static_cast<long long>(zb - za) * D.nxy;
+        CULBM_CUDA(cudaStreamWaitEvent(d2h, ev(j, kSlabDump), 0));
+        for (int k = 0; k < 4; ++k)
+            CULBM_CUDA(cudaMemcpyAsync(out[k] + off, s->d_mac[k] + off, cnt * sizeof(float), cudaMemcpyDeviceToHost, d2h));
+    }
+    // Every slab stream ends with dumps, which the copy-out stream waited for.
+    CULBM_CUDA(cudaEventRecord(s->run_ev[2], d2h));
+    CULBM_CUDA(cudaStreamWaitEvent(s->stream, s->run_ev[2], 0));
+    CULBM_CUDA(cudaStreamSynchronize(s->stream));
+    return check_device_error(s);
 }
 
 bool read_exact(const std::string& path, void* dst, size_t bytes, bool* present, std::string* err)
@@ -800,7 +1076,7 @@ culbm_status culbm_moments(culbm_sim* sim)
         const dim3 g = cell_grid(sim->dom), b = cell_block();
         float* const* m = sim->d_mac;
         with_layout(layout, [&](auto L) {
-            k_moments<decltype(L)::value, S, R><<<g, b, 0, sim->stream>>>(a, sim->d_flag, m[0], m[1], m[2], m[3]);
+            k_moments<decltype(L)::value, S, R><<<g, b, 0, sim->stream>>>(a, sim->d_flag, m[0], m[1], m[2], m[3], 0);
         });
         CULBM_CUDA(cudaGetLastError());
         return CULBM_OK;
@@ -815,6 +1091,31 @@ culbm_status culbm_get_field(culbm_sim* sim, culbm_field field, float* host_out)
     CULBM_CUDA(cudaStreamSynchronize(sim->stream));
     CULBM_TRY(check_device_error(sim));
     return CULBM_OK;
+}
+
+culbm_status culbm_run_host(culbm_sim* sim, const uint32_t* flag, const float* rho, const float* vx,
+                            const float* vy, const float* vz, uint32_t nsteps, float* out_rho, float* out_vx,
+                            float* out_vy, float* out_vz)
+{
+    CULBM_TRY(check_sim(sim));
+    float* const out[4] = {out_rho, out_vx, out_vy, out_vz};
+    for (float* o : out)
+        if (o == nullptr) return fail(CULBM_ERR_INVALID_ARGUMENT, "culbm_run_host: NULL output buffer");
+    const float* mac[4] = {rho, vx, vy, vz};
+    if (is_blocked(sim->cfg) || sim->rows || sim->warp_pull) {
+        // The tile engine and the staged 16-bit kernels step the whole domain at once.
+        CULBM_TRY(upload_state(sim, flag, mac));
+        CULBM_TRY(culbm_step(sim, nsteps));
+        CULBM_TRY(culbm_moments(sim));
+        for (int k = 0; k < 4; ++k)
+            CULBM_CUDA(cudaMemcpyAsync(out[k], sim->d_mac[k], sim->n * sizeof(float), cudaMemcpyDeviceToHost,
+                                       sim->stream));
+        CULBM_CUDA(cudaStreamSynchronize(sim->stream));
+        return check_device_error(sim);
+    }
+    return with_storage(sim, [&](auto tag) {
+        return run_host_overlapped<typename decltype(tag)::type>(sim, flag, mac, nsteps, out);
+    });
 }
 
 culbm_status culbm_dump(culbm_sim* sim, const char* folder, uint32_t field_mask)

@@ -7,6 +7,7 @@
 
 #include <cstdint>
 #include <string>
+#include <vector>
 
 #include "culbm.h"
 #include "stream_kernels.cuh"
@@ -82,6 +83,12 @@ struct culbm_sim {
     int row_grid[3] = {0, 0, 0};    // resident blocks per launch, by RowMode
     int* err_host = nullptr;        // mapped host word a bounded device-side wait writes on expiry
     int* err_dev = nullptr;         // its device address
+
+    // Overlapped host run (culbm_run_host), created on first use.
+    cudaStream_t copy_st[2] = {nullptr, nullptr};   // host-to-device, device-to-host copies
+    std::vector<cudaStream_t> slab_st;              // one per slab of z-planes
+    std::vector<cudaEvent_t> slab_ev;               // kSlabEvents per slab
+    cudaEvent_t run_ev[3] = {nullptr, nullptr, nullptr};   // start, populations filled, copies out done
 };
 
 namespace culbm {

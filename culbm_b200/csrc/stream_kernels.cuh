@@ -231,23 +231,27 @@ struct CellCoord {
     bool valid;
 };
 
-__device__ __forceinline__ CellCoord cell_of_thread(const Domain& D)
+// Cell of this thread in a cell_grid launch over the planes z0, z0 + 1, ...
+// (grid z = the number of planes).
+__device__ __forceinline__ CellCoord cell_of_thread(const Domain& D, int z0 = 0)
 {
     CellCoord c;
     c.x = blockIdx.x * blockDim.x + threadIdx.x;
     c.y = blockIdx.y * blockDim.y + threadIdx.y;
-    c.z = blockIdx.z;
+    c.z = z0 + static_cast<int>(blockIdx.z);
     c.valid = c.x < D.nx && c.y < D.ny;
     c.i = c.x + D.nx * (c.y + D.ny * c.z);
     return c;
 }
 
-// One pull step src -> dst over the whole domain.
+// One pull step src -> dst over the planes z0 .. z0 + gridDim.z - 1 (the
+// whole domain with z0 = 0 and a cell_grid launch).
 // Replaces StaticD3Q27PullKernel, reference kernel.cu:2489-2632.
 template <typename S, typename R>
-__global__ void __launch_bounds__(256, sizeof(R) == 4 ? 5 : 1) k_pull_step(const __grid_constant__ StepArgs<S, R> a)
+__global__ void __launch_bounds__(256, sizeof(R) == 4 ? 5 : 1)
+    k_pull_step(const __grid_constant__ StepArgs<S, R> a, int z0)
 {
-    const CellCoord c = cell_of_thread(a.dom);
+    const CellCoord c = cell_of_thread(a.dom, z0);
     if (!c.valid) return;
     const uint8_t op = a.ops[c.i];
     R f[27];
@@ -470,14 +474,111 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 5 : 1) k_aa_even(const _
         aa_even_cell<S, R, ROWS_INNER>(a, c);
 }
 
+// Grid-z layout of an in-place launch over the slab of planes za .. zb-1
+// (the overlapped host run): split_grid restricted to the slab.  First the
+// z-face planes the slab holds (z = 0, z = nz-1), then slices of the y-face
+// rows of its interior planes, then one slice per interior plane; so the
+// outer rows, with their longer clamp code, keep blocks of their own.
+struct SlabSplit {
+    int za;    // first plane of the slab
+    int zlo;   // first interior plane (0 < z < nz-1) of the slab
+    int ni;    // interior planes in the slab
+    int nzf;   // z-face planes in the slab
+    int nys;   // slices of y-face rows
+};
+
+__host__ __device__ inline SlabSplit slab_split(const Domain& D, int za, int zb)
+{
+    SlabSplit q;
+    q.za = za;
+    q.zlo = za > 1 ? za : 1;
+    const int zhi = zb < D.nz - 1 ? zb : D.nz - 1;
+    q.ni = zhi > q.zlo ? zhi - q.zlo : 0;
+    q.nzf = (za == 0 ? 1 : 0) + (D.nz > 1 && zb == D.nz ? 1 : 0);
+    const int rows_per_slice = ((D.ny + 7) / 8) * 8;
+    const int nyf = D.ny > 1 ? 2 : 1;
+    q.nys = (nyf * q.ni + rows_per_slice - 1) / rows_per_slice;
+    return q;
+}
+
+inline dim3 slab_split_grid(const Domain& D, const SlabSplit& q)
+{
+    return dim3((D.nx + 31) / 32, (D.ny + 7) / 8, q.nzf + q.nys + q.ni);
+}
+
+// Cell of this thread in a slab_split_grid launch: ROWS_OUTER, ROWS_INNER
+// (uniform over a block), or -1 if the thread has no cell.
+__device__ __forceinline__ int slab_split_cell(const Domain& D, const SlabSplit& q, CellCoord& c)
+{
+    c.x = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c.x >= D.nx) return -1;
+    const int bz = static_cast<int>(blockIdx.z);
+    const int yy = blockIdx.y * blockDim.y + threadIdx.y;
+    int kind;
+    if (bz < q.nzf) {
+        if (yy >= D.ny) return -1;
+        c.y = yy;
+        c.z = (bz == 0 && q.za == 0) ? 0 : D.nz - 1;
+        kind = ROWS_OUTER;
+    } else if (bz < q.nzf + q.nys) {
+        const int r = (bz - q.nzf) * static_cast<int>(gridDim.y * blockDim.y) + yy;
+        if (D.ny > 1) {
+            if (r >= 2 * q.ni) return -1;
+            c.z = q.zlo + (r >> 1);
+            c.y = (r & 1) ? D.ny - 1 : 0;
+        } else {
+            if (r >= q.ni) return -1;
+            c.z = q.zlo + r;
+            c.y = 0;
+        }
+        kind = ROWS_OUTER;
+    } else {
+        c.z = q.zlo + (bz - q.nzf - q.nys);
+        c.y = 1 + yy;
+        if (c.y > D.ny - 2) return -1;
+        kind = ROWS_INNER;
+    }
+    c.i = c.x + D.nx * (c.y + D.ny * c.z);
+    c.valid = true;
+    return kind;
+}
+
+// In-place steps over a slab of planes (the overlapped host run).  A cell
+// of one step touches only locations within one plane of itself, so slabs
+// at least two planes thick can run a step concurrently, and a slab's next
+// step needs only this step done on the slab and its two neighbours.
+template <typename S, typename R>
+__global__ void __launch_bounds__(256, sizeof(R) == 4 ? 5 : 1)
+    k_aa_odd_slab(const __grid_constant__ StepArgs<S, R> a, SlabSplit q)
+{
+    CellCoord c;
+    const int kind = slab_split_cell(a.dom, q, c);
+    if (kind == ROWS_OUTER)
+        aa_odd_cell<S, R, ROWS_OUTER>(a, c);
+    else if (kind == ROWS_INNER)
+        aa_odd_cell<S, R, ROWS_INNER>(a, c);
+}
+
+template <typename S, typename R>
+__global__ void __launch_bounds__(256, sizeof(R) == 4 ? 5 : 1)
+    k_aa_even_slab(const __grid_constant__ StepArgs<S, R> a, SlabSplit q)
+{
+    CellCoord c;
+    const int kind = slab_split_cell(a.dom, q, c);
+    if (kind == ROWS_OUTER)
+        aa_even_cell<S, R, ROWS_OUTER>(a, c);
+    else if (kind == ROWS_INNER)
+        aa_even_cell<S, R, ROWS_INNER>(a, c);
+}
+
 // Moments of the pulled populations, written where the DUMP bits are set.
 // Replaces StaticD3Q27PullDumpKernel, reference kernel.cu:2634-2735 (and the
 // per-tile dump kernels, which compute the same values for CORRECT cells).
 template <int LAYOUT, typename S, typename R>
 __global__ void __launch_bounds__(256) k_moments(const __grid_constant__ StepArgs<S, R> a, const uint32_t* flag,
-                                                 float* rho, float* vx, float* vy, float* vz)
+                                                 float* rho, float* vx, float* vy, float* vz, int z0)
 {
-    const CellCoord c = cell_of_thread(a.dom);
+    const CellCoord c = cell_of_thread(a.dom, z0);
     if (!c.valid) return;
     const uint32_t fl = flag[c.i];
     if ((fl & (FLAG_DUMP_RHO | FLAG_DUMP_VX | FLAG_DUMP_VY | FLAG_DUMP_VZ)) == 0) return;

@@ -34,7 +34,7 @@ class Simulation:
                  block_dim: Optional[Sequence[int]] = None, grid_dim: Optional[Sequence[int]] = None,
                  tile: Optional[Sequence[int]] = None, use_ring: bool = False, dev_id: int = 0,
                  persist_l2: bool = False, cache_hints: bool = True, use_graphs: bool = True,
-                 kernel_variant: int = 0):
+                 kernel_variant: int = 0, run_slabs: int = 0):
         cfg = _capi.default_config()
         cfg.dev_id = dev_id
         for k in range(3):
@@ -59,6 +59,7 @@ class Simulation:
         cfg.cache_hints = int(bool(cache_hints))
         cfg.use_graphs = int(bool(use_graphs))
         cfg.kernel_variant = int(kernel_variant)
+        cfg.run_slabs = int(run_slabs)
         self.cfg = cfg
         self.domain = tuple(int(v) for v in domain)
         self.n = self.domain[0] * self.domain[1] * self.domain[2]
@@ -124,6 +125,30 @@ class Simulation:
         v = C.c_uint64(0)
         check(lib().culbm_get_step(self._h, C.byref(v)))
         return v.value
+
+    def run_host(self, nsteps: int, flag=None, rho=None, vx=None, vy=None, vz=None, out=None):
+        """load_state, ``nsteps`` steps, moments and the four fields in one call
+        (culbm_run_host): the slabs' copies overlap the steps when the arrays
+        are page-locked.  ``out`` is four float32 arrays of N values (new ones
+        when None); returns them as (rho, vx, vy, vz)."""
+        arrs = []
+        for a, dt in ((flag, np.uint32), (rho, np.float32), (vx, np.float32), (vy, np.float32), (vz, np.float32)):
+            if a is None:
+                arrs.append(None)
+                continue
+            if not (isinstance(a, np.ndarray) and a.dtype == dt and a.flags.c_contiguous):
+                a = np.ascontiguousarray(a, dtype=dt)
+            a = a.reshape(-1)
+            if a.size != self.n:
+                raise ValueError(f"expected {self.n} values, got {a.size}")
+            arrs.append(a)
+        if out is None:
+            out = tuple(np.empty(self.n, dtype=np.float32) for _ in range(4))
+        for o in out:
+            if not (isinstance(o, np.ndarray) and o.dtype == np.float32 and o.flags.c_contiguous and o.size == self.n):
+                raise ValueError(f"each output must be a contiguous float32 array of {self.n} values")
+        check(lib().culbm_run_host(self._h, *[_ptr(a) for a in arrs], int(nsteps), *[_ptr(o) for o in out]))
+        return tuple(out)
 
     # -------------------------------------------------------------- outputs
     def moments(self) -> None:

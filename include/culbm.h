@@ -113,7 +113,10 @@ typedef struct culbm_config {
                                   992; 3 and 4 (pull only) warp-staged (32-cell row segments
                                   through TMA tensor copies, two or three window buffers per
                                   warp), used where nx is a multiple of 8.  Same bits either way */
-    uint32_t reserved[7];
+    int32_t run_slabs;         /* culbm_run_host: slabs of z-planes the overlapped run cuts the domain
+                                  into; 0 (default) automatic: slabs of at least 2^19 cells, at most
+                                  32; always at most nz/2, so that every slab has two planes or more */
+    uint32_t reserved[6];
 } culbm_config;
 
 /* Fills cfg with the reference's defaults plus the additions' defaults. */
@@ -177,6 +180,28 @@ culbm_status culbm_moments(culbm_sim* sim);
 /* Copies one device macroscopic buffer (N floats) to host_out; synchronises.
  * Replaces the cudaMemcpy of dumpRes, simulator_expt_platform.cu:572-606. */
 culbm_status culbm_get_field(culbm_sim* sim, culbm_field field, float* host_out);
+
+/*
+ * One whole run from host memory to host memory: the effect of
+ * culbm_load_state(flag, rho, vx, vy, vz), culbm_step(nsteps),
+ * culbm_moments() and culbm_get_field() of the four fields into
+ * out_rho/out_vx/out_vy/out_vz, with the same bits; synchronises.
+ * The copies overlap the steps.  The domain is cut into slabs of z-planes
+ * (at least two planes each).  A slab's host-to-device copy, its steps and
+ * its device-to-host copy run as soon as its data and its neighbours' are
+ * ready, so early slabs step while later ones still arrive and leave while
+ * later ones still step.  Overlap needs page-locked host buffers
+ * (cudaHostAlloc / cudaHostRegister); pageable ones give the same results
+ * with the copies serialised.  The blocked policies (optPolicy > 0) and
+ * kernel_variant != 0 run the four calls one after another.  Inputs may be
+ * NULL as in culbm_load_state; outputs must not be.  The simulation's own
+ * stream waits for earlier work first and holds the run's end when the call
+ * returns.  Replaces one run of the reference's driver from its init state
+ * to its dump, simulator_expt_platform.cu:944-991 with :572-606.
+ */
+culbm_status culbm_run_host(culbm_sim* sim, const uint32_t* flag, const float* rho, const float* vx,
+                            const float* vy, const float* vz, uint32_t nsteps, float* out_rho, float* out_vx,
+                            float* out_vy, float* out_vz);
 
 /*
  * Writes <folder>/<rho|vx|vy|vz>_<step>.dat for every field whose bit is set
