@@ -238,6 +238,18 @@ def fp64_errors(culbm, steps=1000):
                         f"{steps} steps, vs FP64 storage+arithmetic", "errors": out}
 
 
+def selector_summary(sel):
+    """culbm_select_tile's pick: the model's speed-up over plain streaming
+    (the reference's model, with the 16-bit compute floor), the same tile's
+    speed-up with B200's measured step costs, and whether blocking is
+    expected to pay (the latter above 1).  --blockDim auto with a blocked
+    optPolicy prints both."""
+    return {"tile": list(sel["tile"]), "inner_loop": sel["inner_loop"],
+            "predicted_speedup": round(sel["speedup"], 4),
+            "predicted_speedup_b200": round(sel["speedup_b200"], 4),
+            "blocking_pays": bool(sel["speedup_b200"] > 1.0)}
+
+
 def mixed_precision_512(culbm, steps):
     """The 512x512x256 channel with 120 spheres (radii 6-18): in-place
     streaming with FP32, FP16 and BF16 storage, plain and L2-blocked."""
@@ -248,6 +260,7 @@ def mixed_precision_512(culbm, steps):
            "cells": sc.n, "steps": steps, "runs": {}}
     from culbm_b200 import selector
     s32, s16 = selector.select(sc.shape, "fp32"), selector.select(sc.shape, "fp16sr")
+    out["selector"] = {k: selector_summary(v) for k, v in (("fp32", s32), ("fp16sr", s16))}
     for name, (op, st, tile, inner) in {
         "inplace_fp32": (0, "fp32", None, 5),
         "inplace_fp16": (0, "fp16", None, 5),
@@ -593,6 +606,7 @@ def run_ours(args):
         "clocks_whole_run": clocks.summary(),
         "cpu_baseline": cpu,
         "variants": extra,
+        "selector": {"fp32": selector_summary(sel)},
         "reference_binary": ref_bin,
         "fp64_error": errs,
         "mixed_precision_512x512x256": mixed,

@@ -130,7 +130,8 @@ class TileChoice(C.Structure):
         ("inner_loop", C.c_int32),
         ("predicted_speedup", C.c_double),
         ("predicted_speedup_no_alignment", C.c_double),
-        ("reserved", C.c_uint32 * 8),
+        ("predicted_speedup_b200", C.c_double),
+        ("reserved", C.c_uint32 * 6),
     ]
 
 

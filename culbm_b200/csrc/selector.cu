@@ -125,7 +125,7 @@ void beta(int bx, int i, double* sec, double* edge)
 // halo cells are computed too), against max(1, compute) for plain streaming:
 //   S = h max(1, compute) / max(D, compute),  D = (1 + alpha h) / (2 I) + lambda (1 - 1/I).
 double speedup(int bx, int by, int bz, int i, double lambda, double gamma, double l2, double cell_bytes,
-               bool with_alpha, double compute)
+               bool with_alpha, double compute, double tile_cost = -1)
 {
     const double r = i - 1;
     const double h = (1 - 2 * r / bx) * (1 - 2 * r / by) * (1 - 2 * r / bz);
@@ -138,7 +138,19 @@ double speedup(int bx, int by, int bz, int i, double lambda, double gamma, doubl
         alpha = 1 + lambda * (bs - 1) + p * (2 * gamma - (1 + lambda)) * be;
     }
     const double D = (1 + alpha * h) / (2.0 * i) + lambda * (1 - 1.0 / i);
-    return h * std::max(1.0, compute) / std::max(D, compute);
+    // tile_cost >= 0: a tile step's own cost per computed cell, apart from
+    // the plain step's (predicted_speedup_b200)
+    return h * std::max(1.0, compute) / std::max(D, tile_cost >= 0 ? tile_cost : compute);
+}
+
+// The measured plain and tile step costs of a storage format on B200 (FP64:
+// none measured, the model as it is).
+void b200_costs(int32_t storage, double* plain, double* tile)
+{
+    const bool is16 = storage == CULBM_STORAGE_F16 || storage == CULBM_STORAGE_BF16 ||
+                      storage == CULBM_STORAGE_F16_SR || storage == CULBM_STORAGE_BF16_SR;
+    *plain = is16 ? CULBM_B200_COMPUTE_16 : storage == CULBM_STORAGE_F32 ? CULBM_B200_PLAIN_32 : 0.0;
+    *tile = is16 ? CULBM_B200_TILE_16 : storage == CULBM_STORAGE_F32 ? CULBM_B200_TILE_32 : 0.0;
 }
 
 // The compute floor of a storage format on B200: 16-bit steps are bound by
@@ -279,6 +291,11 @@ culbm_status culbm_select_tile(const uint32_t domain_dim[3], int32_t storage, do
                 }
         }
     if (best < 0) return fail(CULBM_ERR_INVALID_ARGUMENT, "no tile of the model's range fits this domain");
+    double plain_cost, tile_cost;
+    b200_costs(storage, &plain_cost, &tile_cost);
+    out->predicted_speedup_b200 = speedup(static_cast<int>(out->tile[0]), static_cast<int>(out->tile[1]),
+                                          static_cast<int>(out->tile[2]), out->inner_loop, lambda, gamma, l2,
+                                          cell_bytes, true, plain_cost, tile_cost);
     return CULBM_OK;
 }
 

@@ -257,7 +257,8 @@ int run(Options o)
             o.cfg.inner_loop = t.inner_loop;
             std::cout << "Auto tile: blockDim [" << t.tile[0] << "," << t.tile[1] << "," << t.tile[2]
                       << "] gridDim [1,1,1] innerLoop " << t.inner_loop << " (modelled speed-up "
-                      << t.predicted_speedup << " over plain streaming)" << std::endl;
+                      << t.predicted_speedup << " over plain streaming, " << t.predicted_speedup_b200
+                      << " with B200's measured step costs)" << std::endl;
         }
     }
     if (o.dstep == 0) throw std::invalid_argument("--dstep must be positive");

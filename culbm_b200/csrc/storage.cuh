@@ -237,6 +237,16 @@ __device__ __forceinline__ R ld_raw(const S* p)
         return Cvt<S, R>::ld(p);
 }
 
+// ld_raw with the evict-first hint (ld.global.cs).
+template <typename S, typename R>
+__device__ __forceinline__ R ld_raw_cs(const S* p)
+{
+    if constexpr (std::is_same<S, __half>::value || std::is_same<S, Half16SR>::value)
+        return __half2float(__ushort_as_half(__ldcs(reinterpret_cast<const unsigned short*>(p))));
+    else
+        return Cvt<S, R>::ld_cs(p);
+}
+
 // ld_raw from global memory with a 256-byte L2 fetch granularity
 // (ld.global.L2::256B): the step kernels read every population plane as a
 // stream, and on B200 the larger L2 fetch made the FP32 in-place and pull
@@ -317,23 +327,41 @@ __device__ __forceinline__ void put_cs(S* p, R v, uint32_t hcell, int d)
         Cvt<S, R>::st_cs(p, v);
 }
 
+// put_raw() with the evict-first hint when CS.
+template <bool CS, typename S, typename R>
+__device__ __forceinline__ void put_raw_h(S* p, R v, uint32_t hcell, int d)
+{
+    if constexpr (!CS)
+        put_raw(p, v, hcell, d);
+    else if constexpr (Is16<S>::value)
+        st16_cs(p, enc16_raw<S>(v, hcell, d));
+    else
+        Cvt<S, R>::st_cs(p, v);
+}
+
 // Stores the 27 raw values f of one cell, direction d at addr(d), with the
-// bits of put_raw.  The 16-bit formats convert the directions in pairs
-// (d, 26 - d) with one packed conversion per pair.
-template <typename S, typename R, class A>
+// bits of put_raw (evict-first stores when CS).  The 16-bit formats convert
+// the directions in pairs (d, 26 - d) with one packed conversion per pair.
+template <typename S, bool CS = false, typename R, class A>
 __device__ __forceinline__ void put27_raw(const R* f, uint32_t hcell, A&& addr)
 {
     if constexpr (Is16<S>::value) {
+        auto st = [](S* p, unsigned short b) {
+            if constexpr (CS)
+                st16_cs(p, b);
+            else
+                st16(p, b);
+        };
 #pragma unroll
         for (int k = 0; k < 13; ++k) {
             const uint32_t w = Pack2<S>::cvt(f[26 - k], f[k], IsSR<S>::value ? sr_word_pair(hcell, k) : 0u);
-            st16(addr(k), static_cast<unsigned short>(w));
-            st16(addr(26 - k), static_cast<unsigned short>(w >> 16));
+            st(addr(k), static_cast<unsigned short>(w));
+            st(addr(26 - k), static_cast<unsigned short>(w >> 16));
         }
-        st16(addr(13), enc16_raw<S>(f[13], hcell, 13));
+        st(addr(13), enc16_raw<S>(f[13], hcell, 13));
     } else {
 #pragma unroll
-        for (int d = 0; d < 27; ++d) put_raw(addr(d), f[d], hcell, d);
+        for (int d = 0; d < 27; ++d) put_raw_h<CS>(addr(d), f[d], hcell, d);
     }
 }
 

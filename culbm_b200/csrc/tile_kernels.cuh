@@ -74,23 +74,17 @@ __device__ __forceinline__ long long gaddr(const GlobalPops<S>& g, const Domain&
     return (long long)pz * D.nxy + (long long)y * D.nx + x;
 }
 
+// The tile steps work on raw values 2^E f (E = ScaleExp<S>; the scale is
+// folded into the cell update, as in the plain steps), loaded with ld_raw
+// and stored with put_raw / put27_raw: the same bits as loading f and
+// storing it with put.
 template <typename S, typename R, bool HINT>
 __device__ __forceinline__ R gload(const S* p)
 {
     if constexpr (HINT) {
-        return Cvt<S, R>::ld_cs(p);
+        return ld_raw_cs<S, R>(p);
     } else {
-        return Cvt<S, R>::ld(p);
-    }
-}
-
-template <typename S, typename R, bool HINT>
-__device__ __forceinline__ void gstore(S* p, R v, uint32_t hcell, int d)
-{
-    if constexpr (HINT) {
-        put_cs(p, v, hcell, d);
-    } else {
-        put(p, v, hcell, d);
+        return ld_raw<S, R>(p);
     }
 }
 
@@ -131,6 +125,13 @@ __device__ __forceinline__ bool in_tile(int px, int py, int pz, int bx, int by, 
     return (unsigned)px < (unsigned)bx && (unsigned)py < (unsigned)by && (unsigned)pz < (unsigned)bz;
 }
 
+// Resident blocks per SM the tile step kernels are compiled for: four
+// blocks of 256 (at most 64 registers; the first-step kernels spill 8-24
+// bytes).  Left free, the first-step kernels took 75-80 registers (three
+// blocks) and the 16-bit steps ran a quarter slower; five blocks (48
+// registers) spill 36-140 bytes.
+constexpr int kTileMinBlocks = 4;
+
 // Programmatic dependent launch: the tile steps of a round are launched
 // with programmatic stream serialisation, so the next step's blocks may start
 // while this grid's last blocks run.  Each step lets its dependents start at
@@ -166,9 +167,7 @@ __device__ __forceinline__ void tile_store_global(const TileArgs<S, R>& a, const
 {
     S* base = a.g.base[sel];
     const long long off = gaddr(a.g, a.dom, offz, c.gx, c.gy, c.gz);
-    const uint32_t hc = tile_hash(a, c.gi);
-#pragma unroll
-    for (int d = 0; d < 27; ++d) gstore<S, R, HINT>(base + d * a.g.stride + off, f[d], hc, d);
+    put27_raw<S, HINT>(f, tile_hash(a, c.gi), [&](int d) { return base + d * a.g.stride + off; });
 }
 
 // Selected buffers of the current round.
@@ -185,7 +184,7 @@ __device__ __forceinline__ void tile_load_aa(const TileArgs<S, R>& a, const Tile
     const Domain& D = a.dom;
     if (LAYOUT == LAYOUT_AA_B) {
 #pragma unroll
-        for (int d = 0; d < 27; ++d) f[d] = Cvt<S, R>::ld(a.t0.p[d] + c.t);
+        for (int d = 0; d < 27; ++d) f[d] = ld_raw<S, R>(a.t0.p[d] + c.t);
         return;
     }
     if (!edge) {
@@ -198,7 +197,7 @@ __device__ __forceinline__ void tile_load_aa(const TileArgs<S, R>& a, const Tile
             const int cx = cx_of(d), cy = cy_of(d), cz = cz_of(d);
             const bool ok = (cx == 1 ? lx : cx == -1 ? hx : true) && (cy == 1 ? ly : cy == -1 ? hy : true) &&
                             (cz == 1 ? lz : cz == -1 ? hz : true);
-            f[d] = ok ? Cvt<S, R>::ld(a.t0.p[26 - d] + (c.t - (cx + cy * a.bx + cz * a.bxy))) : R(0);
+            f[d] = ok ? ld_raw<S, R>(a.t0.p[26 - d] + (c.t - (cx + cy * a.bx + cz * a.bxy))) : R(0);
         }
         return;
     }
@@ -206,9 +205,9 @@ __device__ __forceinline__ void tile_load_aa(const TileArgs<S, R>& a, const Tile
     for (int d = 0; d < 27; ++d) {
         const int cx = cx_of(d), cy = cy_of(d), cz = cz_of(d);
         if (!inside(D, c.gx - cx, c.gy - cy, c.gz - cz))
-            f[d] = Cvt<S, R>::ld(a.edge + edge_slot(D, a.el, c.gx, c.gy, c.gz, d));
+            f[d] = ld_raw<S, R>(a.edge + edge_slot(D, a.el, c.gx, c.gy, c.gz, d));
         else if (in_tile(c.px - cx, c.py - cy, c.pz - cz, a.bx, a.by, a.bz))
-            f[d] = Cvt<S, R>::ld(a.t0.p[26 - d] + (c.t - (cx + cy * a.bx + cz * a.bxy)));
+            f[d] = ld_raw<S, R>(a.t0.p[26 - d] + (c.t - (cx + cy * a.bx + cz * a.bxy)));
         else
             f[d] = R(0);
     }
@@ -225,14 +224,14 @@ __device__ __forceinline__ void tile_file_clamp_sources(const TileArgs<S, R>& a,
     for_dirs([&](auto dd) {
         constexpr int d = decltype(dd)::value;
         for_each_clamp_reader<d>(a.dom, c.gx, c.gy, c.gz, [&](int yx, int yy, int yz) {
-            put(a.edge + edge_slot(a.dom, a.el, yx, yy, yz, d), f[d], hc, d);
+            put_raw(a.edge + edge_slot(a.dom, a.el, yx, yy, yz, d), f[d], hc, d);
         });
     });
 }
 
 // First step: global pull -> tile (layout A), or -> global when I == 1.
 template <typename S, typename R, bool ONE, bool HINT>
-__global__ void __launch_bounds__(256) k_tile_aa_first(const __grid_constant__ TileArgs<S, R> a)
+__global__ void __launch_bounds__(256, kTileMinBlocks) k_tile_aa_first(const __grid_constant__ TileArgs<S, R> a)
 {
     tile_step_enter();
     const TileCell c = tile_cell(a);
@@ -246,20 +245,20 @@ __global__ void __launch_bounds__(256) k_tile_aa_first(const __grid_constant__ T
 #pragma unroll
         for (int d = 0; d < 27; ++d) f[d] = R(0);
     }
-    cell_update_for<S, false>(op, a.inv_tau, a.rho, a.vx, a.vy, a.vz, c.gi, f);
+    cell_update_for<S, true>(op, a.inv_tau, a.rho, a.vx, a.vy, a.vz, c.gi, f);
     if (!(op & OP_STORE)) return;
     if constexpr (ONE) {
         if (c.correct) tile_store_global<S, R, HINT>(a, c, round_dst_sel(a.rs, ring), a.rs->dst_offz, f);
     } else {
 #pragma unroll
-        for (int d = 0; d < 27; ++d) put(a.t0.p[26 - d] + c.t, f[d], tile_hash(a, c.gi), d);
+        put27_raw<S>(f, tile_hash(a, c.gi), [&](int d) { return a.t0.p[26 - d] + c.t; });
         if (op & OP_EDGE) tile_file_clamp_sources(a, c, f);
     }
 }
 
 // Middle odd step inside the tile (layout A -> B).
 template <typename S, typename R>
-__global__ void __launch_bounds__(256) k_tile_aa_odd(const __grid_constant__ TileArgs<S, R> a)
+__global__ void __launch_bounds__(256, kTileMinBlocks) k_tile_aa_odd(const __grid_constant__ TileArgs<S, R> a)
 {
     tile_step_enter();
     const TileCell c = tile_cell(a);
@@ -274,7 +273,7 @@ __global__ void __launch_bounds__(256) k_tile_aa_odd(const __grid_constant__ Til
 #pragma unroll
         for (int d = 0; d < 27; ++d) f[d] = R(0);
     }
-    cell_update_for<S, false>(op, a.inv_tau, a.rho, a.vx, a.vy, a.vz, c.gi, f);
+    cell_update_for<S, true>(op, a.inv_tau, a.rho, a.vx, a.vy, a.vz, c.gi, f);
     if (!(op & OP_STORE)) return;
     if (!edge) {
         // off the domain faces a push only has to stay inside the tile
@@ -287,7 +286,7 @@ __global__ void __launch_bounds__(256) k_tile_aa_odd(const __grid_constant__ Til
             const int cx = cx_of(d), cy = cy_of(d), cz = cz_of(d);
             const bool ok = (cx == 1 ? hx : cx == -1 ? lx : true) && (cy == 1 ? hy : cy == -1 ? ly : true) &&
                             (cz == 1 ? hz : cz == -1 ? lz : true);
-            if (ok) put(a.t0.p[d] + (c.t + cx + cy * a.bx + cz * a.bxy), f[d], hc, d);
+            if (ok) put_raw(a.t0.p[d] + (c.t + cx + cy * a.bx + cz * a.bxy), f[d], hc, d);
         }
         return;
     }
@@ -295,13 +294,13 @@ __global__ void __launch_bounds__(256) k_tile_aa_odd(const __grid_constant__ Til
         constexpr int d = decltype(dd)::value;
         constexpr int cx = cx_of(d), cy = cy_of(d), cz = cz_of(d);
         if (inside(D, c.gx + cx, c.gy + cy, c.gz + cz) && in_tile(c.px + cx, c.py + cy, c.pz + cz, a.bx, a.by, a.bz))
-            put(a.t0.p[d] + (c.t + cx + cy * a.bx + cz * a.bxy), f[d], tile_hash(a, c.gi), d);
+            put_raw(a.t0.p[d] + (c.t + cx + cy * a.bx + cz * a.bxy), f[d], tile_hash(a, c.gi), d);
         if (edge) {
             // slot d of each boundary cell whose clamped pull reads this cell
             for_each_clamp_reader<d>(D, c.gx, c.gy, c.gz, [&](int yx, int yy, int yz) {
                 const int qx = yx - a.ox, qy = yy - a.oy, qz = yz - a.oz;
                 if (in_tile(qx, qy, qz, a.bx, a.by, a.bz))
-                    put(a.t0.p[d] + (qx + a.bx * (qy + a.by * qz)), f[d], tile_hash(a, c.gi), d);
+                    put_raw(a.t0.p[d] + (qx + a.bx * (qy + a.by * qz)), f[d], tile_hash(a, c.gi), d);
             });
         }
     });
@@ -309,7 +308,7 @@ __global__ void __launch_bounds__(256) k_tile_aa_odd(const __grid_constant__ Til
 
 // Middle even step inside the tile (layout B -> A).
 template <typename S, typename R>
-__global__ void __launch_bounds__(256) k_tile_aa_even(const __grid_constant__ TileArgs<S, R> a)
+__global__ void __launch_bounds__(256, kTileMinBlocks) k_tile_aa_even(const __grid_constant__ TileArgs<S, R> a)
 {
     tile_step_enter();
     const TileCell c = tile_cell(a);
@@ -322,16 +321,15 @@ __global__ void __launch_bounds__(256) k_tile_aa_even(const __grid_constant__ Ti
 #pragma unroll
         for (int d = 0; d < 27; ++d) f[d] = R(0);
     }
-    cell_update_for<S, false>(op, a.inv_tau, a.rho, a.vx, a.vy, a.vz, c.gi, f);
+    cell_update_for<S, true>(op, a.inv_tau, a.rho, a.vx, a.vy, a.vz, c.gi, f);
     if (!(op & OP_STORE)) return;
-#pragma unroll
-    for (int d = 0; d < 27; ++d) put(a.t0.p[26 - d] + c.t, f[d], tile_hash(a, c.gi), d);
+    put27_raw<S>(f, tile_hash(a, c.gi), [&](int d) { return a.t0.p[26 - d] + c.t; });
     if (op & OP_EDGE) tile_file_clamp_sources(a, c, f);
 }
 
 // Last step: tile (layout A or B) -> global result, valid cells only.
 template <int LAYOUT, typename S, typename R, bool HINT>
-__global__ void __launch_bounds__(256) k_tile_aa_last(const __grid_constant__ TileArgs<S, R> a)
+__global__ void __launch_bounds__(256, kTileMinBlocks) k_tile_aa_last(const __grid_constant__ TileArgs<S, R> a)
 {
     tile_step_enter();
     const TileCell c = tile_cell(a);
@@ -344,7 +342,7 @@ __global__ void __launch_bounds__(256) k_tile_aa_last(const __grid_constant__ Ti
 #pragma unroll
         for (int d = 0; d < 27; ++d) f[d] = R(0);
     }
-    cell_update_for<S, false>(op, a.inv_tau, a.rho, a.vx, a.vy, a.vz, c.gi, f);
+    cell_update_for<S, true>(op, a.inv_tau, a.rho, a.vx, a.vy, a.vz, c.gi, f);
     if (op & OP_STORE) tile_store_global<S, R, HINT>(a, c, round_dst_sel(a.rs, a.g.ring_nz), a.rs->dst_offz, f);
 }
 
@@ -366,7 +364,7 @@ __device__ __forceinline__ void tile_pull(const TileArgs<S, R>& a, const Pops<S>
             const int cx = cx_of(d), cy = cy_of(d), cz = cz_of(d);
             const bool ok = (cx == 1 ? lx : cx == -1 ? hx : true) && (cy == 1 ? ly : cy == -1 ? hy : true) &&
                             (cz == 1 ? lz : cz == -1 ? hz : true);
-            f[d] = ok ? Cvt<S, R>::ld(src.p[d] + (c.t - (cx + cy * a.bx + cz * a.bxy))) : R(0);
+            f[d] = ok ? ld_raw<S, R>(src.p[d] + (c.t - (cx + cy * a.bx + cz * a.bxy))) : R(0);
         }
         return;
     }
@@ -377,14 +375,14 @@ __device__ __forceinline__ void tile_pull(const TileArgs<S, R>& a, const Pops<S>
         if ((unsigned)(c.gy - cy) >= (unsigned)a.dom.ny) cy = 0;
         if ((unsigned)(c.gz - cz) >= (unsigned)a.dom.nz) cz = 0;
         if (in_tile(c.px - cx, c.py - cy, c.pz - cz, a.bx, a.by, a.bz))
-            f[d] = Cvt<S, R>::ld(src.p[d] + (c.t - (cx + cy * a.bx + cz * a.bxy)));
+            f[d] = ld_raw<S, R>(src.p[d] + (c.t - (cx + cy * a.bx + cz * a.bxy)));
         else
             f[d] = R(0);
     }
 }
 
 template <typename S, typename R, bool ONE, bool HINT>
-__global__ void __launch_bounds__(256) k_tile_pull_first(const __grid_constant__ TileArgs<S, R> a)
+__global__ void __launch_bounds__(256, kTileMinBlocks) k_tile_pull_first(const __grid_constant__ TileArgs<S, R> a)
 {
     tile_step_enter();
     const TileCell c = tile_cell(a);
@@ -398,19 +396,18 @@ __global__ void __launch_bounds__(256) k_tile_pull_first(const __grid_constant__
 #pragma unroll
         for (int d = 0; d < 27; ++d) f[d] = R(0);
     }
-    cell_update_for<S, false>(op, a.inv_tau, a.rho, a.vx, a.vy, a.vz, c.gi, f);
+    cell_update_for<S, true>(op, a.inv_tau, a.rho, a.vx, a.vy, a.vz, c.gi, f);
     if (!(op & OP_STORE)) return;
     if constexpr (ONE) {
         if (c.correct) tile_store_global<S, R, HINT>(a, c, round_dst_sel(a.rs, ring), a.rs->dst_offz, f);
     } else {
-#pragma unroll
-        for (int d = 0; d < 27; ++d) put(a.t0.p[d] + c.t, f[d], tile_hash(a, c.gi), d);
+        put27_raw<S>(f, tile_hash(a, c.gi), [&](int d) { return a.t0.p[d] + c.t; });
     }
 }
 
 // Middle step t0 -> t1 (the host swaps t0/t1 between launches).
 template <typename S, typename R>
-__global__ void __launch_bounds__(256) k_tile_pull_mid(const __grid_constant__ TileArgs<S, R> a)
+__global__ void __launch_bounds__(256, kTileMinBlocks) k_tile_pull_mid(const __grid_constant__ TileArgs<S, R> a)
 {
     tile_step_enter();
     const TileCell c = tile_cell(a);
@@ -423,14 +420,13 @@ __global__ void __launch_bounds__(256) k_tile_pull_mid(const __grid_constant__ T
 #pragma unroll
         for (int d = 0; d < 27; ++d) f[d] = R(0);
     }
-    cell_update_for<S, false>(op, a.inv_tau, a.rho, a.vx, a.vy, a.vz, c.gi, f);
+    cell_update_for<S, true>(op, a.inv_tau, a.rho, a.vx, a.vy, a.vz, c.gi, f);
     if (!(op & OP_STORE)) return;
-#pragma unroll
-    for (int d = 0; d < 27; ++d) put(a.t1.p[d] + c.t, f[d], tile_hash(a, c.gi), d);
+    put27_raw<S>(f, tile_hash(a, c.gi), [&](int d) { return a.t1.p[d] + c.t; });
 }
 
 template <typename S, typename R, bool HINT>
-__global__ void __launch_bounds__(256) k_tile_pull_last(const __grid_constant__ TileArgs<S, R> a)
+__global__ void __launch_bounds__(256, kTileMinBlocks) k_tile_pull_last(const __grid_constant__ TileArgs<S, R> a)
 {
     tile_step_enter();
     const TileCell c = tile_cell(a);
@@ -443,7 +439,7 @@ __global__ void __launch_bounds__(256) k_tile_pull_last(const __grid_constant__ 
 #pragma unroll
         for (int d = 0; d < 27; ++d) f[d] = R(0);
     }
-    cell_update_for<S, false>(op, a.inv_tau, a.rho, a.vx, a.vy, a.vz, c.gi, f);
+    cell_update_for<S, true>(op, a.inv_tau, a.rho, a.vx, a.vy, a.vz, c.gi, f);
     if (op & OP_STORE) tile_store_global<S, R, HINT>(a, c, round_dst_sel(a.rs, a.g.ring_nz), a.rs->dst_offz, f);
 }
 

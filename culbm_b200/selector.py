@@ -35,7 +35,7 @@ def select(domain: Sequence[int], storage: str = "fp32", lam: float = 0.0, gamma
     check(lib().culbm_select_tile(d, _capi.STORAGE[storage], float(lam), float(gamma), int(l2_bytes),
                                   int(persist_bytes), C.byref(t)))
     return {"tile": list(t.tile), "inner_loop": t.inner_loop, "speedup": t.predicted_speedup,
-            "speedup_no_alignment": t.predicted_speedup_no_alignment}
+            "speedup_no_alignment": t.predicted_speedup_no_alignment, "speedup_b200": t.predicted_speedup_b200}
 
 
 def speedup(tile: Sequence[int], inner_loop: int, storage: str = "fp32", lam: float = 0.0, gamma: float = 0.0,

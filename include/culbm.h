@@ -291,7 +291,10 @@ typedef struct culbm_tile_choice {
     int32_t inner_loop;
     double predicted_speedup;      /* model speed-up over plain streaming (S) */
     double predicted_speedup_no_alignment;  /* the same without the sector-alignment term (S0) */
-    uint32_t reserved[8];
+    double predicted_speedup_b200; /* S of the chosen tile with B200's measured step costs
+                                      (CULBM_B200_PLAIN_* and CULBM_B200_TILE_*): above 1 when
+                                      blocking is expected to beat plain streaming on B200 */
+    uint32_t reserved[6];
 } culbm_tile_choice;
 
 /* Constants used when lambda, gamma <= 0: culbm_measure_memory on a B200
@@ -305,6 +308,17 @@ typedef struct culbm_tile_choice {
  * blocked tile predicts S < 1 (the halo cells cost compute and save only
  * bandwidth) and the tile of largest S is the one with the least halo. */
 #define CULBM_B200_COMPUTE_16 1.67
+/* Measured step costs on B200, each as time per update over the DRAM time of
+ * the format's bytes per update at the copy bandwidth.  The model takes the
+ * DRAM traffic of an L2-blocked round as its time; on B200 the tile steps
+ * themselves cost more than that, in L2 or not.  Plain FP32 pull: 29.2k
+ * MLUPS against 30.3k.  An FP32 L2-tile step (pull tiles, per computed cell,
+ * halo included): 28.7k against 30.3k.  A 16-bit tile step: 22.8k against
+ * 60.6k.  The plain 16-bit step is CULBM_B200_COMPUTE_16.
+ * predicted_speedup_b200 = h max(1, plain) / max(D, tile) with these. */
+#define CULBM_B200_PLAIN_32 1.04
+#define CULBM_B200_TILE_32 1.06
+#define CULBM_B200_TILE_16 2.66
 
 /* The tile and innerLoop of the largest model speed-up for `domain_dim` and
  * population storage `storage` (CULBM_STORAGE_*), with the compute floor of
