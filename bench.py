@@ -333,13 +333,15 @@ def adjoint_runs():
     return out
 
 
-def e2e_run(culbm, scene, steps, sp=1, reps=3):
+def e2e_run(culbm, scene, steps, sp=1, reps=3, tdist=None, ws=1, dev_id=0):
     """Through the public API with page-locked host buffers, host wall clock,
-    best of `reps`.  `overlapped`: one culbm_run_host call (the init state in,
-    `steps` steps, the dump kernel and rho/vx/vy/vz out, with the slabs'
-    copies overlapping the steps).  `sequential`: the same run as
-    culbm_load_state + culbm_step + culbm_moments + 4x culbm_get_field, which
-    copy before and after the steps."""
+    best of `reps`; with several ranks each rank runs its own replica between
+    barriers, the time is the slowest rank's and the MLUPS the whole job's.
+    `overlapped`: one culbm_run_host call (the init state in, `steps` steps,
+    the dump kernel and rho/vx/vy/vz out, with the slabs' copies overlapping
+    the steps).  `sequential`: the same run as culbm_load_state + culbm_step +
+    culbm_moments + 4x culbm_get_field, which copy before and after the
+    steps."""
     import ctypes as C
 
     from culbm_b200 import _capi
@@ -349,25 +351,33 @@ def e2e_run(culbm, scene, steps, sp=1, reps=3):
     out_arrays = tuple(o[0] for o in outs)
     best = {"overlapped": float("inf"), "sequential": float("inf")}
     same = True
-    with culbm.Simulation(scene.shape, stream_policy=sp, inv_tau=0.5) as sim:
+
+    def timed(fn):
+        barrier(tdist)
+        t0 = time.perf_counter()
+        fn()
+        return max_over_ranks(tdist, time.perf_counter() - t0)
+
+    with culbm.Simulation(scene.shape, stream_policy=sp, inv_tau=0.5, dev_id=dev_id) as sim:
         lib = _capi.lib()
         sim.run_host(5, *[h[0] for h in host], out=out_arrays)   # creates the run's streams
-        for _ in range(reps):
-            t0 = time.perf_counter()
-            sim.run_host(steps, *[h[0] for h in host], out=out_arrays)
-            best["overlapped"] = min(best["overlapped"], time.perf_counter() - t0)
-            first = [o.copy() for o in out_arrays]
-            t0 = time.perf_counter()
+
+        def sequential():
             _capi.check(lib.culbm_load_state(sim._h, *[h[0].ctypes.data_as(C.c_void_p) for h in host]))
             sim.step(steps)
             sim.moments()
             for k in range(4):
                 _capi.check(lib.culbm_get_field(sim._h, k, out_arrays[k].ctypes.data_as(C.c_void_p)))
-            best["sequential"] = min(best["sequential"], time.perf_counter() - t0)
+
+        for _ in range(reps):
+            best["overlapped"] = min(best["overlapped"],
+                                     timed(lambda: sim.run_host(steps, *[h[0] for h in host], out=out_arrays)))
+            first = [o.copy() for o in out_arrays]
+            best["sequential"] = min(best["sequential"], timed(sequential))
             same = same and all(np.array_equal(a.view(np.uint32), b.view(np.uint32)) for a, b in zip(first, out_arrays))
     h2d = sum(h[0].nbytes for h in host)
     d2h = sum(o[0].nbytes for o in outs)
-    mlups = {k: scene.n * steps / v / 1e6 for k, v in best.items()}
+    mlups = {k: ws * scene.n * steps / v / 1e6 for k, v in best.items()}
     return mlups, h2d, d2h, same
 
 
@@ -511,6 +521,10 @@ def run_ours(args):
     ms_per_step = ms_max / args.steps
     launches = int(round(info["launches_per_step"] * args.steps))
 
+    # End to end on every rank (its own replica), before the single-rank legs.
+    e2e = None
+    if not args.headline_only:
+        e2e = e2e_run(culbm_b200, sc, args.steps, tdist=tdist, ws=ws, dev_id=local)
     if rank != 0:
         clocks.stop()
         if tdist is not None:
@@ -567,7 +581,7 @@ def run_ours(args):
         adjoint = adjoint_runs() if not args.no_adjoint else None
     except Exception as e:
         adjoint = {"error": str(e)}
-    e2e_mlups, h2d, d2h, e2e_same = e2e_run(culbm_b200, sc, args.steps)
+    e2e_mlups, h2d, d2h, e2e_same = e2e
     cpu = cpu_baseline(sc) if ws == 1 else None
     clocks.stop()
 

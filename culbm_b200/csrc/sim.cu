@@ -626,18 +626,19 @@ culbm_status upload_state(culbm_sim* s, const uint32_t* flag, const float* const
 
 constexpr int kSlabEvents = 6;   // per slab: a ring of 4 step events, inputs copied in, dump done
 constexpr int kSlabIn = 4, kSlabDump = 5;
-constexpr int kMaxSlabs = 32;
-constexpr long long kMinSlabCells = 1ll << 19;
 constexpr int kRunStreams = 4;
 
-// Slab count: culbm_config.run_slabs, or slabs of at least kMinSlabCells
-// cells (enough blocks to fill the device) and at most kMaxSlabs; at most
-// nz / 2 either way.
-int run_slabs(const culbm_sim* s)
+// Slab count: culbm_config.run_slabs, or automatic: runs of up to 40 steps
+// (all skewed) take up to 64 slabs of at least 2^18 cells, so that the first
+// slabs arrive early; longer runs up to 32 slabs of at least 2^19 cells,
+// which keeps their two skewed phases short.  At most nz / 2 either way.
+// (288x272x280, in place: 20 steps 19.9 ms with 64 slabs against 20.5 ms
+// with 32; 100 steps 87.1 ms with 32 against 89.0 ms with 64.)
+int run_slabs(const culbm_sim* s, uint32_t nsteps)
 {
     const Domain& D = s->dom;
-    const long long want = s->cfg.run_slabs > 0 ? s->cfg.run_slabs
-                                                : std::min<long long>(kMaxSlabs, D.n / kMinSlabCells);
+    long long want = s->cfg.run_slabs;
+    if (want <= 0) want = nsteps <= 40 ? std::min<long long>(64, D.n >> 18) : std::min<long long>(32, D.n >> 19);
     return static_cast<int>(std::max<long long>(1, std::min<long long>(want, D.nz / 2)));
 }
 
@@ -772,7 +773,7 @@ culbm_status run_host_overlapped(culbm_sim* s, const uint32_t* flag, const float
                                  float* const out[4])
 {
     const Domain& D = s->dom;
-    const int nslab = run_slabs(s);
+    const int nslab = run_slabs(s, nsteps);
     const int nstream = std::min(nslab, kRunStreams);
     CULBM_TRY(ensure_run_streams(s, nstream, nslab));
     auto ev = [&](int j, int k) { return s->slab_ev[static_cast<size_t>(j) * kSlabEvents + k]; };

@@ -114,8 +114,9 @@ typedef struct culbm_config {
                                   through TMA tensor copies, two or three window buffers per
                                   warp), used where nx is a multiple of 8.  Same bits either way */
     int32_t run_slabs;         /* culbm_run_host: slabs of z-planes the overlapped run cuts the domain
-                                  into; 0 (default) automatic: slabs of at least 2^19 cells, at most
-                                  32; always at most nz/2, so that every slab has two planes or more */
+                                  into; 0 (default) automatic: for runs of up to 40 steps at most 64
+                                  slabs of at least 2^18 cells, else at most 32 of at least 2^19;
+                                  always at most nz/2, so that every slab has two planes or more */
     uint32_t reserved[6];
 } culbm_config;
 

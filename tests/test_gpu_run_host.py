@@ -119,14 +119,15 @@ def test_run_host_page_locked_buffers_and_repeat(culbm):
 
 
 @pytest.mark.parametrize("run_slabs", [0, 5, 32])
-def test_run_host_slab_counts(culbm, run_slabs):
-    """The automatic count (slabs of 2^19 cells or more: two here) and explicit ones."""
+@pytest.mark.parametrize("nsteps", [12, 45])
+def test_run_host_slab_counts(culbm, run_slabs, nsteps):
+    """The automatic count (5 slabs for 12 steps, 2 for 45 here) and explicit ones."""
     dims = (128, 64, 160)
     arrs = scene(dims).arrays()
     for sp in (0, 1):
-        want = sequential(culbm, dims, arrs, 12, stream_policy=sp)
-        got = overlapped(culbm, dims, arrs, 12, run_slabs=run_slabs, stream_policy=sp)
-        assert_fields_equal(got, want, f"run_slabs={run_slabs} sp={sp}")
+        want = sequential(culbm, dims, arrs, nsteps, stream_policy=sp)
+        got = overlapped(culbm, dims, arrs, nsteps, run_slabs=run_slabs, stream_policy=sp)
+        assert_fields_equal(got, want, f"run_slabs={run_slabs} sp={sp} steps={nsteps}")
 
 
 def test_run_host_sequential_configurations(culbm):

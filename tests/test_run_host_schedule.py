@@ -29,11 +29,12 @@ next to it):
 """
 import pytest
 
-KMAX_SLABS, KMIN_CELLS, KSTREAMS = 32, 1 << 19, 4
+KSTREAMS = 4
 
 
-def run_slabs(nx, ny, nz, requested=0):
-    want = requested if requested > 0 else min(KMAX_SLABS, nx * ny * nz // KMIN_CELLS)
+def run_slabs(nx, ny, nz, nsteps, requested=0):
+    n = nx * ny * nz
+    want = requested if requested > 0 else (min(64, n >> 18) if nsteps <= 40 else min(32, n >> 19))
     return max(1, min(want, nz // 2))
 
 
@@ -181,17 +182,19 @@ def check(nz, T, pull, ns):
 
 @pytest.mark.parametrize("pull", [True, False])
 @pytest.mark.parametrize("nz,T", [(1, 3), (3, 2), (5, 7), (9, 8), (16, 1), (16, 7), (37, 8), (40, 20),
-                                  (40, 41), (9, 30), (280, 20), (280, 70)])
+                                  (40, 41), (9, 30), (280, 20), (280, 70), (280, 41)])
 def test_schedule_has_no_race_and_no_stale_read(nz, T, pull):
-    ns = run_slabs(288, 272, nz, requested=16 if nz < 280 else 0)
+    ns = run_slabs(288, 272, nz, T, requested=16 if nz < 280 else 0)
     assert ns == 1 or all(slab_z0(nz, ns, j + 1) - slab_z0(nz, ns, j) >= 2 for j in range(ns))
     problems = check(nz, T, pull, ns)
     assert not problems, problems[:5]
 
 
 def test_automatic_slab_count():
-    assert run_slabs(288, 272, 280) == 32           # 21.9 M cells: capped at 32
-    assert run_slabs(128, 64, 160) == 2             # 1.3 M cells: slabs of 2^19 cells or more
-    assert run_slabs(48, 20, 44) == 1
-    assert run_slabs(512, 512, 256) == 32
-    assert run_slabs(288, 272, 3, requested=16) == 1
+    assert run_slabs(288, 272, 280, 20) == 64       # 21.9 M cells, a short run: 64 slabs of 2^18 or more
+    assert run_slabs(288, 272, 280, 100) == 32      # a long run: 32 slabs of 2^19 or more
+    assert run_slabs(128, 64, 160, 12) == 5         # 1.3 M cells
+    assert run_slabs(128, 64, 160, 41) == 2
+    assert run_slabs(48, 20, 44, 20) == 1
+    assert run_slabs(512, 512, 256, 100) == 32
+    assert run_slabs(288, 272, 3, 20, requested=16) == 1
