@@ -365,6 +365,26 @@ __device__ __forceinline__ void put27_raw(const R* f, uint32_t hcell, A&& addr)
     }
 }
 
+// put27_raw for the directions d with keep(d) only (the others are not
+// stored); the 16-bit formats still convert in pairs.
+template <typename S, typename R, class A, class K>
+__device__ __forceinline__ void put27_raw_if(const R* f, uint32_t hcell, A&& addr, K&& keep)
+{
+    if constexpr (Is16<S>::value) {
+#pragma unroll
+        for (int k = 0; k < 13; ++k) {
+            const uint32_t w = Pack2<S>::cvt(f[26 - k], f[k], IsSR<S>::value ? sr_word_pair(hcell, k) : 0u);
+            if (keep(k)) st16(addr(k), static_cast<unsigned short>(w));
+            if (keep(26 - k)) st16(addr(26 - k), static_cast<unsigned short>(w >> 16));
+        }
+        if (keep(13)) st16(addr(13), enc16_raw<S>(f[13], hcell, 13));
+    } else {
+#pragma unroll
+        for (int d = 0; d < 27; ++d)
+            if (keep(d)) put_raw(addr(d), f[d], hcell, d);
+    }
+}
+
 // Arithmetic type used with each storage type.
 template <typename S> struct ArithOf { using type = float; };
 template <> struct ArithOf<double> { using type = double; };

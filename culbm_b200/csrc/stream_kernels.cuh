@@ -368,12 +368,24 @@ __device__ __forceinline__ void aa_odd_cell(const StepArgs<S, R>& a, const CellC
 #pragma unroll
             for (int d = 0; d < 27; ++d) f[d] = ld_stream_raw<S, R>(a.src.p[26 - d] + (c.i - nb_off(D, d)));
         } else if (ROWS == ROWS_INNER) {
+            // A warp with an x-face lane loads like the others, the face lane
+            // from its own column for the directions whose source lies
+            // outside (so every load stays in the domain), and that lane
+            // alone then takes those directions from the edge buffer.
+            const bool lo = c.x == 0, hi = c.x == D.nx - 1;
+            const int ip = c.i + (lo ? 1 : 0), im = c.i - (hi ? 1 : 0);
 #pragma unroll
             for (int d = 0; d < 27; ++d) {
-                const S* p = a.src.p[26 - d] + (c.i - nb_off(D, d));
-                if (cx_of(d) == 1 && c.x == 0) p = xface_edge_ptr(a.edge, D, a.el, 0, d, c.y, c.z);
-                if (cx_of(d) == -1 && c.x == D.nx - 1) p = xface_edge_ptr(a.edge, D, a.el, 1, d, c.y, c.z);
-                f[d] = ld_stream_raw<S, R>(p);
+                const int base = cx_of(d) == 1 ? ip : cx_of(d) == -1 ? im : c.i;
+                f[d] = ld_stream_raw<S, R>(a.src.p[26 - d] + (base - nb_off(D, d)));
+            }
+            if (lo) {
+#pragma unroll
+                for (int d = 2; d < 27; d += 3) f[d] = ld_stream_raw<S, R>(xface_edge_ptr(a.edge, D, a.el, 0, d, c.y, c.z));
+            }
+            if (hi) {
+#pragma unroll
+                for (int d = 0; d < 27; d += 3) f[d] = ld_stream_raw<S, R>(xface_edge_ptr(a.edge, D, a.el, 1, d, c.y, c.z));
             }
         } else {
             load_pulled<LAYOUT_AA_A, true>(a, c.x, c.y, c.z, c.i, true, f);
@@ -387,14 +399,18 @@ __device__ __forceinline__ void aa_odd_cell(const StepArgs<S, R>& a, const CellC
     if (ROWS == ROWS_INNER && !xface) {
         put27_raw<S>(f, hc, [&](int d) { return a.dst.p[d] + (c.i + nb_off(D, d)); });
     } else if (ROWS == ROWS_INNER) {
+        // streaming target x + c_d, unless it leaves the domain in x
+        const bool lo = c.x == 0, hi = c.x == D.nx - 1;
+        put27_raw_if<S>(f, hc, [&](int d) { return a.dst.p[d] + (c.i + nb_off(D, d)); },
+                        [&](int d) { return !((cx_of(d) == 1 && hi) || (cx_of(d) == -1 && lo)); });
+        // an x-face cell is the clamped source of the cell on its own face
+        if (lo) {
 #pragma unroll
-        for (int d = 0; d < 27; ++d) {
-            const int cx = cx_of(d);
-            S* p = a.dst.p[d] + (c.i + nb_off(D, d));
-            // streaming target x + c_d, unless it leaves the domain in x
-            if (cx == 0 || (cx == 1 && c.x < D.nx - 1) || (cx == -1 && c.x > 0)) put_raw(p, f[d], hc, d);
-            // an x-face cell is the clamped source of the cell on its own face
-            if ((cx == 1 && c.x == 0) || (cx == -1 && c.x == D.nx - 1)) put_raw(p - cx, f[d], hc, d);
+            for (int d = 2; d < 27; d += 3) put_raw(a.dst.p[d] + (c.i + nb_off(D, d) - 1), f[d], hc, d);
+        }
+        if (hi) {
+#pragma unroll
+            for (int d = 0; d < 27; d += 3) put_raw(a.dst.p[d] + (c.i + nb_off(D, d) + 1), f[d], hc, d);
         }
     } else {
         for_dirs([&](auto dd) {
