@@ -537,6 +537,8 @@ def run_ours(args):
         print(json.dumps({"metric": METRIC, "value": round(value, 1), "unit": "MLUPS", "n_gpus": ws,
                           "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4),
                           "headline_only": True, "gpu_launches": launches, "clocks": headline_clocks}), flush=True)
+        if tdist is not None:
+            tdist.destroy_process_group()
         return
     extra = {}
     k2 = max(20, args.steps // 4)
@@ -627,6 +629,8 @@ def run_ours(args):
         "adjoint": adjoint,
     }
     print(json.dumps(line), flush=True)
+    if tdist is not None:
+        tdist.destroy_process_group()
 
 
 # -------------------------------------------------------------- reference ---
