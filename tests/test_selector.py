@@ -61,3 +61,38 @@ def test_blocking_axis_bounds(culbm):
     assert selector.blocking_axis(280, 288, 3) == [0, 280]
     with pytest.raises(_capi.CulbmError, match="don't match"):
         selector.blocking_axis(64, 4, 3)
+
+
+def _header_constant(name):
+    import re
+    path = os.path.join(os.path.dirname(os.path.dirname(__file__)), "include", "culbm.h")
+    m = re.search(r"#define\s+" + name + r"\s+([0-9.]+)", open(path).read())
+    return float(m.group(1))
+
+
+@pytest.mark.parametrize("domain", [(288, 272, 280), (512, 512, 256), (1024, 512, 512)])
+def test_b200_speedup_uses_the_measured_step_costs(culbm, domain):
+    """predicted_speedup_b200 = h max(1, plain) / max(D, tile) for the chosen
+    tile, with the header's measured B200 costs; below 1 (plain streaming is
+    faster on B200) for FP32 and the 16-bit formats; FP64 has no measured costs
+    and keeps the model's value."""
+    from culbm_b200 import selector
+    l2, persist = 126 << 20, 80 << 20
+    plain32, tile32 = _header_constant("CULBM_B200_PLAIN_32"), _header_constant("CULBM_B200_TILE_32")
+    plain16, tile16 = _header_constant("CULBM_B200_COMPUTE_16"), _header_constant("CULBM_B200_TILE_16")
+    for storage in ("fp32", "fp16sr", "bf16", "fp64"):
+        s = selector.select(domain, storage, l2_bytes=l2, persist_bytes=persist)
+        r = s["inner_loop"] - 1
+        h = 1.0
+        for b in s["tile"]:
+            h *= 1 - 2 * r / b
+        if storage == "fp64":
+            assert s["speedup_b200"] == pytest.approx(s["speedup"], rel=1e-12)
+            continue
+        if storage == "fp32":
+            d = h / s["speedup"]          # the model's own round time (S = h / D for FP32)
+            want = h * max(1.0, plain32) / max(d, tile32)
+        else:
+            want = h * max(1.0, plain16) / tile16   # D is far below the tile cost here
+        assert s["speedup_b200"] == pytest.approx(want, rel=1e-9)
+        assert s["speedup_b200"] < 1.0
