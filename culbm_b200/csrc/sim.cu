@@ -435,14 +435,14 @@ culbm_status plain_steps(culbm_sim* s, uint32_t nsteps)
                     // split_grid), inner rows row-staged; disjoint locations
                     auto a = make_args<S>(s, 0, 0);
                     a.seed = seed;
-                    const dim3 gs = split_grid(D);
-                    const dim3 go(gs.x, gs.y, outer_slices(D));
+                    const dim3 gs = split_grid(D, kAaRows);
+                    const dim3 go(gs.x, gs.y, outer_slices(D, kAaRows));
                     if (s->aa_phase == 0) {
-                        k_aa_odd<S, R><<<go, b, 0, s->stream>>>(a);
+                        k_aa_odd<S, R><<<go, aa_block(), 0, s->stream>>>(a);
                         CULBM_CUDA(cudaGetLastError());
                         CULBM_TRY((rows_launch<S, ROWS_AA_ODD>(s, a, 1, 1, D.ny - 2, D.nz - 2)));
                     } else {
-                        k_aa_even<S, R><<<go, b, 0, s->stream>>>(a);
+                        k_aa_even<S, R><<<go, aa_block(), 0, s->stream>>>(a);
                         CULBM_CUDA(cudaGetLastError());
                         CULBM_TRY((rows_launch<S, ROWS_AA_EVEN>(s, a, 1, 1, D.ny - 2, D.nz - 2)));
                     }
@@ -461,11 +461,11 @@ culbm_status plain_steps(culbm_sim* s, uint32_t nsteps)
         } else {
             auto a = make_args<S>(s, 0, 0);
             a.seed = seed;
-            const dim3 gs = split_grid(s->dom);
+            const dim3 gs = split_grid(s->dom, kAaRows);
             if (s->aa_phase == 0)
-                k_aa_odd<S, R><<<gs, b, 0, s->stream>>>(a);
+                k_aa_odd<S, R><<<gs, aa_block(), 0, s->stream>>>(a);
             else
-                k_aa_even<S, R><<<gs, b, 0, s->stream>>>(a);
+                k_aa_even<S, R><<<gs, aa_block(), 0, s->stream>>>(a);
             CULBM_CUDA(cudaGetLastError());
             s->aa_phase ^= 1;
         }
@@ -497,7 +497,7 @@ culbm_status validate_config(const culbm_config& c)
         d.nx = static_cast<int>(c.domain_dim[0]);
         d.ny = static_cast<int>(c.domain_dim[1]);
         d.nz = static_cast<int>(c.domain_dim[2]);
-        if (split_grid(d).z > 65535)
+        if (split_grid(d, kAaRows).z > 65535)
             return fail(CULBM_ERR_INVALID_ARGUMENT, "domainDim z too large for in-place streaming (grid z above 65535)");
     }
     if (c.vel_set != 0) return fail(CULBM_ERR_INVALID_ARGUMENT, "Unsupport Velocity Set: " + std::to_string(c.vel_set));
@@ -736,11 +736,11 @@ culbm_status run_slab_steps(culbm_sim* s, int nslab, int nstream, int t0, int t1
             } else {
                 auto a = make_args<S>(s, 0, 0);
                 a.seed = step_seed(static_cast<uint32_t>(t));
-                const SlabSplit q = slab_split(D, za, zb);
+                const SlabSplit q = slab_split(D, za, zb, kAaRows);
                 if ((t & 1) == 0)
-                    k_aa_odd_slab<S, R><<<slab_split_grid(D, q), b, 0, st>>>(a, q);
+                    k_aa_odd_slab<S, R><<<slab_split_grid(D, q, kAaRows), aa_block(), 0, st>>>(a, q);
                 else
-                    k_aa_even_slab<S, R><<<slab_split_grid(D, q), b, 0, st>>>(a, q);
+                    k_aa_even_slab<S, R><<<slab_split_grid(D, q, kAaRows), aa_block(), 0, st>>>(a, q);
             }
             CULBM_CUDA(cudaGetLastError());
             s->launches += 1;

@@ -283,7 +283,7 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 5 : 1)
 //     selects and predicated stores; the code stays straight-line.
 //   ROWS_OUTER: rows on a y or z face, processed with the general per-axis
 //     clamp code (about 2 (ny + nz) of the ny*nz rows).
-// Grid (split_grid): 32 x 8 blocks, one warp per 32 cells of a row.  The
+// Grid (split_grid): 32 x `rows` blocks, one warp per 32 cells of a row.  The
 // first grid-z slices hold the outer rows (the z = 0 and z = nz-1 planes,
 // then the y-face rows of the interior planes), so their longer code runs
 // beside the inner rows rather than as a tail; each further slice is one
@@ -291,17 +291,23 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 5 : 1)
 // accesses stay coalesced, and no thread divides by a runtime value.
 enum RowSet : int { ROWS_INNER = 0, ROWS_OUTER = 1 };
 
-// Grid-z slices of the outer rows.
-__host__ __device__ __forceinline__ int outer_slices(const Domain& D)
+// Rows per block of the in-place step launches (split_grid, slab_split):
+// with four rows of 32 cells (128 threads), at the same 40 warps per SM, the
+// in-place FP32 steps ran 1.3 % faster at 288x272x280 and 0.7 % at
+// 512x512x256 than with eight; the pull is indifferent and keeps eight.
+constexpr int kAaRows = 4;
+
+// Grid-z slices of the outer rows (blocks of `rows` rows).
+__host__ __device__ __forceinline__ int outer_slices(const Domain& D, int rows = 8)
 {
-    const int rows_per_slice = ((D.ny + 7) / 8) * 8;
+    const int rows_per_slice = ((D.ny + rows - 1) / rows) * rows;
     const int nzf = D.nz > 1 ? 2 : 1, nyf = D.ny > 1 ? 2 : 1;
     return nzf + (D.nz > 2 ? (nyf * (D.nz - 2) + rows_per_slice - 1) / rows_per_slice : 0);
 }
 
-inline dim3 split_grid(const Domain& D)
+inline dim3 split_grid(const Domain& D, int rows = 8)
 {
-    return dim3((D.nx + 31) / 32, (D.ny + 7) / 8, outer_slices(D) + (D.nz > 2 ? D.nz - 2 : 0));
+    return dim3((D.nx + 31) / 32, (D.ny + rows - 1) / rows, outer_slices(D, rows) + (D.nz > 2 ? D.nz - 2 : 0));
 }
 
 // Cell of this thread in a split_grid launch whose grid-z slices start at
@@ -314,7 +320,7 @@ __device__ __forceinline__ int split_cell(const Domain& D, int z0, CellCoord& c)
     const int bz = static_cast<int>(blockIdx.z) - z0;
     const int yy = blockIdx.y * blockDim.y + threadIdx.y;
     const int nzf = D.nz > 1 ? 2 : 1;
-    const int oz = outer_slices(D);
+    const int oz = outer_slices(D, static_cast<int>(blockDim.y));
     int kind;
     if (bz < nzf) {
         if (yy >= D.ny) return -1;
@@ -503,7 +509,7 @@ struct SlabSplit {
     int nys;   // slices of y-face rows
 };
 
-__host__ __device__ inline SlabSplit slab_split(const Domain& D, int za, int zb)
+__host__ __device__ inline SlabSplit slab_split(const Domain& D, int za, int zb, int rows = 8)
 {
     SlabSplit q;
     q.za = za;
@@ -511,15 +517,15 @@ __host__ __device__ inline SlabSplit slab_split(const Domain& D, int za, int zb)
     const int zhi = zb < D.nz - 1 ? zb : D.nz - 1;
     q.ni = zhi > q.zlo ? zhi - q.zlo : 0;
     q.nzf = (za == 0 ? 1 : 0) + (D.nz > 1 && zb == D.nz ? 1 : 0);
-    const int rows_per_slice = ((D.ny + 7) / 8) * 8;
+    const int rows_per_slice = ((D.ny + rows - 1) / rows) * rows;
     const int nyf = D.ny > 1 ? 2 : 1;
     q.nys = (nyf * q.ni + rows_per_slice - 1) / rows_per_slice;
     return q;
 }
 
-inline dim3 slab_split_grid(const Domain& D, const SlabSplit& q)
+inline dim3 slab_split_grid(const Domain& D, const SlabSplit& q, int rows = 8)
 {
-    return dim3((D.nx + 31) / 32, (D.ny + 7) / 8, q.nzf + q.nys + q.ni);
+    return dim3((D.nx + 31) / 32, (D.ny + rows - 1) / rows, q.nzf + q.nys + q.ni);
 }
 
 // Cell of this thread in a slab_split_grid launch: ROWS_OUTER, ROWS_INNER
