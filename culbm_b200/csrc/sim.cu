@@ -435,14 +435,14 @@ culbm_status plain_steps(culbm_sim* s, uint32_t nsteps)
                     // split_grid), inner rows row-staged; disjoint locations
                     auto a = make_args<S>(s, 0, 0);
                     a.seed = seed;
-                    const dim3 gs = split_grid(D, kAaRows);
-                    const dim3 go(gs.x, gs.y, outer_slices(D, kAaRows));
+                    const dim3 gs = split_grid(D, AaShape<S>::rows, AaShape<S>::cols);
+                    const dim3 go(gs.x, gs.y, outer_slices(D, AaShape<S>::rows));
                     if (s->aa_phase == 0) {
-                        k_aa_odd<S, R><<<go, aa_block(), 0, s->stream>>>(a);
+                        k_aa_odd<S, R><<<go, aa_block<S>(), 0, s->stream>>>(a);
                         CULBM_CUDA(cudaGetLastError());
                         CULBM_TRY((rows_launch<S, ROWS_AA_ODD>(s, a, 1, 1, D.ny - 2, D.nz - 2)));
                     } else {
-                        k_aa_even<S, R><<<go, aa_block(), 0, s->stream>>>(a);
+                        k_aa_even<S, R><<<go, aa_block<S>(), 0, s->stream>>>(a);
                         CULBM_CUDA(cudaGetLastError());
                         CULBM_TRY((rows_launch<S, ROWS_AA_EVEN>(s, a, 1, 1, D.ny - 2, D.nz - 2)));
                     }
@@ -461,11 +461,11 @@ culbm_status plain_steps(culbm_sim* s, uint32_t nsteps)
         } else {
             auto a = make_args<S>(s, 0, 0);
             a.seed = seed;
-            const dim3 gs = split_grid(s->dom, kAaRows);
+            const dim3 gs = split_grid(s->dom, AaShape<S>::rows, AaShape<S>::cols);
             if (s->aa_phase == 0)
-                k_aa_odd<S, R><<<gs, aa_block(), 0, s->stream>>>(a);
+                k_aa_odd<S, R><<<gs, aa_block<S>(), 0, s->stream>>>(a);
             else
-                k_aa_even<S, R><<<gs, aa_block(), 0, s->stream>>>(a);
+                k_aa_even<S, R><<<gs, aa_block<S>(), 0, s->stream>>>(a);
             CULBM_CUDA(cudaGetLastError());
             s->aa_phase ^= 1;
         }
@@ -497,8 +497,14 @@ culbm_status validate_config(const culbm_config& c)
         d.nx = static_cast<int>(c.domain_dim[0]);
         d.ny = static_cast<int>(c.domain_dim[1]);
         d.nz = static_cast<int>(c.domain_dim[2]);
-        if (split_grid(d, kAaRows).z > 65535)
+        const bool s16 = c.storage == CULBM_STORAGE_F16 || c.storage == CULBM_STORAGE_BF16 ||
+                         c.storage == CULBM_STORAGE_F16_SR || c.storage == CULBM_STORAGE_BF16_SR;
+        const dim3 g = s16 ? split_grid(d, AaShape<__half>::rows, AaShape<__half>::cols)
+                           : split_grid(d, AaShape<float>::rows, AaShape<float>::cols);
+        if (g.z > 65535)
             return fail(CULBM_ERR_INVALID_ARGUMENT, "domainDim z too large for in-place streaming (grid z above 65535)");
+        if (g.y > 65535)
+            return fail(CULBM_ERR_INVALID_ARGUMENT, "domainDim y too large for in-place streaming (grid y above 65535)");
     }
     if (c.vel_set != 0) return fail(CULBM_ERR_INVALID_ARGUMENT, "Unsupport Velocity Set: " + std::to_string(c.vel_set));
     if (c.stream_policy != CULBM_STREAM_PULL && c.stream_policy != CULBM_STREAM_INPLACE)
@@ -736,11 +742,12 @@ culbm_status run_slab_steps(culbm_sim* s, int nslab, int nstream, int t0, int t1
             } else {
                 auto a = make_args<S>(s, 0, 0);
                 a.seed = step_seed(static_cast<uint32_t>(t));
-                const SlabSplit q = slab_split(D, za, zb, kAaRows);
+                constexpr int ar = AaShape<S>::rows, ac = AaShape<S>::cols;
+                const SlabSplit q = slab_split(D, za, zb, ar);
                 if ((t & 1) == 0)
-                    k_aa_odd_slab<S, R><<<slab_split_grid(D, q, kAaRows), aa_block(), 0, st>>>(a, q);
+                    k_aa_odd_slab<S, R><<<slab_split_grid(D, q, ar, ac), aa_block<S>(), 0, st>>>(a, q);
                 else
-                    k_aa_even_slab<S, R><<<slab_split_grid(D, q, kAaRows), aa_block(), 0, st>>>(a, q);
+                    k_aa_even_slab<S, R><<<slab_split_grid(D, q, ar, ac), aa_block<S>(), 0, st>>>(a, q);
             }
             CULBM_CUDA(cudaGetLastError());
             s->launches += 1;

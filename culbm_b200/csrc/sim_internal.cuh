@@ -94,8 +94,9 @@ struct culbm_sim {
 namespace culbm {
 
 inline dim3 cell_block() { return dim3(32, 8, 1); }
-// Blocks of the in-place step launches (kAaRows rows of 32 cells).
-inline dim3 aa_block() { return dim3(32, kAaRows, 1); }
+// Blocks of the in-place step launches of storage format S (AaShape).
+template <typename S>
+inline dim3 aa_block() { return dim3(AaShape<S>::cols, AaShape<S>::rows, 1); }
 inline dim3 cell_grid(const Domain& D)
 {
     return dim3((D.nx + 31) / 32, (D.ny + 7) / 8, D.nz);

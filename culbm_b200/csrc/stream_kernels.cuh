@@ -283,7 +283,8 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 5 : 1)
 //     selects and predicated stores; the code stays straight-line.
 //   ROWS_OUTER: rows on a y or z face, processed with the general per-axis
 //     clamp code (about 2 (ny + nz) of the ny*nz rows).
-// Grid (split_grid): 32 x `rows` blocks, one warp per 32 cells of a row.  The
+// Grid (split_grid): blocks of `cols` x `rows` cells (cols a multiple of 32),
+// one warp per 32 cells of a row.  The
 // first grid-z slices hold the outer rows (the z = 0 and z = nz-1 planes,
 // then the y-face rows of the interior planes), so their longer code runs
 // beside the inner rows rather than as a tail; each further slice is one
@@ -291,11 +292,19 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 5 : 1)
 // accesses stay coalesced, and no thread divides by a runtime value.
 enum RowSet : int { ROWS_INNER = 0, ROWS_OUTER = 1 };
 
-// Rows per block of the in-place step launches (split_grid, slab_split):
-// with four rows of 32 cells (128 threads), at the same 40 warps per SM, the
-// in-place FP32 steps ran 1.3 % faster at 288x272x280 and 0.7 % at
-// 512x512x256 than with eight; the pull is indifferent and keeps eight.
-constexpr int kAaRows = 4;
+// Block shape of the in-place step launches (split_grid, slab_split), by
+// storage format: one row of 96 cells (three warps, one 32-cell segment
+// each) for FP32 and FP64, four rows of 32 for the 16-bit formats.  At the
+// same 40 warps per SM, blocks of 32 x 4 ran the in-place FP32 steps 1.3 %
+// faster at 288x272x280 and 0.7 % at 512x512x256 than 32 x 8, and 96 x 1
+// another 0.7-0.8 %; the 16-bit steps are 0.8 % (288x272x280) and 2.1 %
+// (512x512x256) faster with 32 x 4 than with 96 x 1.  The pull is
+// indifferent and keeps 32 x 8.
+template <typename S>
+struct AaShape {
+    static constexpr int cols = Is16<S>::value ? 32 : 96;
+    static constexpr int rows = Is16<S>::value ? 4 : 1;
+};
 
 // Grid-z slices of the outer rows (blocks of `rows` rows).
 __host__ __device__ __forceinline__ int outer_slices(const Domain& D, int rows = 8)
@@ -305,9 +314,10 @@ __host__ __device__ __forceinline__ int outer_slices(const Domain& D, int rows =
     return nzf + (D.nz > 2 ? (nyf * (D.nz - 2) + rows_per_slice - 1) / rows_per_slice : 0);
 }
 
-inline dim3 split_grid(const Domain& D, int rows = 8)
+inline dim3 split_grid(const Domain& D, int rows = 8, int cols = 32)
 {
-    return dim3((D.nx + 31) / 32, (D.ny + rows - 1) / rows, outer_slices(D, rows) + (D.nz > 2 ? D.nz - 2 : 0));
+    return dim3((D.nx + cols - 1) / cols, (D.ny + rows - 1) / rows,
+                outer_slices(D, rows) + (D.nz > 2 ? D.nz - 2 : 0));
 }
 
 // Cell of this thread in a split_grid launch whose grid-z slices start at
@@ -523,9 +533,9 @@ __host__ __device__ inline SlabSplit slab_split(const Domain& D, int za, int zb,
     return q;
 }
 
-inline dim3 slab_split_grid(const Domain& D, const SlabSplit& q, int rows = 8)
+inline dim3 slab_split_grid(const Domain& D, const SlabSplit& q, int rows = 8, int cols = 32)
 {
-    return dim3((D.nx + 31) / 32, (D.ny + rows - 1) / rows, q.nzf + q.nys + q.ni);
+    return dim3((D.nx + cols - 1) / cols, (D.ny + rows - 1) / rows, q.nzf + q.nys + q.ni);
 }
 
 // Cell of this thread in a slab_split_grid launch: ROWS_OUTER, ROWS_INNER

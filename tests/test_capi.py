@@ -59,6 +59,9 @@ def _create(cfg):
     (lambda c: setattr(c, "stream_policy", 2), "streamPolicy"),
     (lambda c: setattr(c, "inv_tau", 2.5), "invTau"),
     (lambda c: c.domain_dim.__setitem__(2, 0), "domainDim"),
+    # in-place launches use one row of cells per block, so ny is the grid's y extent
+    (lambda c: (setattr(c, "stream_policy", 1), c.domain_dim.__setitem__(0, 32),
+                c.domain_dim.__setitem__(1, 70000), c.domain_dim.__setitem__(2, 4)), "grid y above 65535"),
 ])
 def test_invalid_configs_rejected_before_device(culbm, mutate, needle):
     from culbm_b200 import _capi
