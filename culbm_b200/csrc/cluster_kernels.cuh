@@ -1,0 +1,176 @@
+// optPolicy 2 (L1/L2 mixed blocking) with pull streaming: one thread-block
+// cluster per tile, the populations of every cell held in registers across
+// the innerLoop steps of a round, and streaming between the cells of a tile
+// through shared memory -- the CTA's own and, across CTA faces, the other
+// CTAs' through distributed shared memory (DSMEM).
+//
+// The reference's HaloBlockingL1L2D3Q27PullKernel
+// (src/simulator/single_dev_expt/kernel.cu:138-329, streaming in
+// L1L2StreamCore.cuh:45-690) runs one tile per cooperative launch over the
+// whole GPU: registers per cell, shared memory inside a CTA, warp shuffles
+// for +-x, an L2 swap buffer for CTA faces and a grid-wide barrier per step.
+// Here a tile is small enough for one cluster (at most 16 CTAs), so:
+//   * the CTA-face exchange goes through DSMEM instead of an L2 buffer, and
+//     the per-step barrier is the cluster's hardware barrier instead of a
+//     grid-wide one (no spin-wait of our own);
+//   * every tile of a round runs in ONE launch (a grid of clusters), so no
+//     tile waits for another and the SMs stay busy across tiles;
+//   * the geometry (tile extent, halo innerLoop-1, valid boxes from
+//     calcValidPrev, blocking_alogrithm.hpp:7-41) is the reference's, as in
+//     the L2 tile engine, and the results are the plain pull step's bit for
+//     bit (per-axis domain clamp; pulls from outside the tile read 0 and only
+//     reach cells outside the valid box).
+#pragma once
+
+#include <cooperative_groups.h>
+
+#include "tile_kernels.cuh"
+
+namespace culbm {
+
+namespace cg = cooperative_groups;
+
+// Most CTAs in one cluster (B200 allows 16 with the non-portable attribute).
+constexpr int kClusterMaxCtas = 16;
+
+template <typename S, typename R>
+struct ClusterTileArgs {
+    Domain dom;
+    int B[3];          // tile extent (cells)
+    int nt[3];         // tiles per axis
+    int I;             // innerLoop of the geometry (halo depth I - 1)
+    int k;             // steps of this round (1..I)
+    int cdim[3];       // CTAs per tile per axis (the cluster's shape)
+    const uint8_t* ops;
+    const float* rho;
+    const float* vx;
+    const float* vy;
+    const float* vz;
+    R inv_tau;
+    GlobalPops<S> g;   // double-buffered global state (no ring buffer)
+    const RoundState* rs;
+};
+
+// First valid index of tile `idx` along one axis: calcValidPrev
+// (blocking_alogrithm.hpp:34-41), as valid_prev in tile_runtime.cu.
+__device__ __forceinline__ int cluster_valid_start(int idx, int blk, int num, int it, int dom)
+{
+    if (idx == num) return dom;
+    if (idx == 0) return 0;
+    return (blk + 1 - it) + (idx - 1) * (blk + 2 - 2 * it);
+}
+
+// The round's k steps over one tile per cluster.  Shared memory: two slots
+// of 9 directions x (threads of the CTA) populations in storage format S;
+// groups of 9 directions alternate between the slots, so a slot is rewritten
+// only after the barrier that follows every read of its previous contents.
+template <typename S, typename R, bool HINT>
+__global__ void __launch_bounds__(1024, 1) k_tile_cluster_pull(const __grid_constant__ ClusterTileArgs<S, R> a)
+{
+    extern __shared__ __align__(16) unsigned char cluster_smem[];
+    S* slots = reinterpret_cast<S*>(cluster_smem);
+    cg::cluster_group cl = cg::this_cluster();
+
+    const Domain& D = a.dom;
+    const int nthr = static_cast<int>(blockDim.x * blockDim.y * blockDim.z);
+    const int lt = static_cast<int>(threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z));
+    const int bdim[3] = {static_cast<int>(blockDim.x), static_cast<int>(blockDim.y), static_cast<int>(blockDim.z)};
+    const int bidx[3] = {static_cast<int>(blockIdx.x), static_cast<int>(blockIdx.y), static_cast<int>(blockIdx.z)};
+    const int tidx[3] = {static_cast<int>(threadIdx.x), static_cast<int>(threadIdx.y), static_cast<int>(threadIdx.z)};
+    const int dn[3] = {D.nx, D.ny, D.nz};
+
+    // this thread's cell: tile coordinates p, global coordinates gc
+    int p[3], gc[3];
+    bool active = true, correct = true;
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+        const int kt = bidx[q] / a.cdim[q];
+        p[q] = (bidx[q] - kt * a.cdim[q]) * bdim[q] + tidx[q];
+        const int vlo = cluster_valid_start(kt, a.B[q], a.nt[q], a.I, dn[q]);
+        const int vhi = cluster_valid_start(kt + 1, a.B[q], a.nt[q], a.I, dn[q]);
+        gc[q] = max(vlo - (a.I - 1), 0) + p[q];
+        active = active && p[q] < a.B[q] && gc[q] < dn[q];
+        correct = correct && gc[q] >= vlo && gc[q] < vhi;
+    }
+    const int gi = active ? gc[0] + D.nx * (gc[1] + D.ny * gc[2]) : 0;
+    const uint8_t op = active ? a.ops[gi] : uint8_t(0);
+    const int sel_src = a.rs->sel, sel_dst = 1 - a.rs->sel;
+    const uint32_t step0 = a.rs->step;
+
+    R f[27];
+    if (op & OP_LOAD) {
+        // first step: pull from the global state with the domain clamp
+        const S* base = a.g.base[sel_src];
+        const int xs[3] = {gc[0] == 0 ? gc[0] : gc[0] - 1, gc[0], gc[0] == D.nx - 1 ? gc[0] : gc[0] + 1};
+        const int ys[3] = {(gc[1] == 0 ? gc[1] : gc[1] - 1) * D.nx, gc[1] * D.nx,
+                           (gc[1] == D.ny - 1 ? gc[1] : gc[1] + 1) * D.nx};
+        const long long zs[3] = {(long long)(gc[2] == 0 ? gc[2] : gc[2] - 1) * D.nxy, (long long)gc[2] * D.nxy,
+                                 (long long)(gc[2] == D.nz - 1 ? gc[2] : gc[2] + 1) * D.nxy};
+#pragma unroll
+        for (int d = 0; d < 27; ++d)
+            f[d] = gload<S, R, HINT>(base + d * a.g.stride + zs[1 - cz_of(d)] + (ys[1 - cy_of(d)] + xs[1 - cx_of(d)]));
+    } else {
+#pragma unroll
+        for (int d = 0; d < 27; ++d) f[d] = R(0);
+    }
+    cell_update_for<S, true>(op, a.inv_tau, a.rho, a.vx, a.vy, a.vz, gi, f);
+
+    // CTA of the cluster (linear rank, x fastest) and cell inside it that
+    // hold tile cell s, for the exchange
+    auto rank_of = [&](const int* s) {
+        return (s[0] / bdim[0]) + a.cdim[0] * ((s[1] / bdim[1]) + a.cdim[1] * (s[2] / bdim[2]));
+    };
+    auto local_of = [&](const int* s) {
+        return (s[0] % bdim[0]) + bdim[0] * ((s[1] % bdim[1]) + bdim[1] * (s[2] % bdim[2]));
+    };
+
+    int group = 0;   // running count of exchanged groups (selects the slot)
+    for (int m = 1; m < a.k; ++m) {
+        // post-collision populations of step m - 1 in storage format S
+        // (the same rounding as a stored step, stochastic bits included)
+        S q[27];
+        put27_raw<S>(f, cell_hash(static_cast<uint32_t>(gi), step_seed(step0 + static_cast<uint32_t>(m - 1))),
+                     [&](int d) { return &q[d]; });
+#pragma unroll
+        for (int grp = 0; grp < 3; ++grp, ++group) {
+            S* slot = slots + (group & 1) * 9 * nthr;
+#pragma unroll
+            for (int e = 0; e < 9; ++e) slot[e * nthr + lt] = q[grp * 9 + e];
+            cl.sync();   // barrier.cluster arrive (release) + wait (acquire)
+#pragma unroll
+            for (int e = 0; e < 9; ++e) {
+                const int d = grp * 9 + e;
+                R v = R(0);
+                if (op & OP_LOAD) {
+                    const int c[3] = {cx_of(d), cy_of(d), cz_of(d)};
+                    int s[3];
+                    bool in = true;
+#pragma unroll
+                    for (int ax = 0; ax < 3; ++ax) {
+                        // domain clamp per axis, then the tile bound (halo: 0)
+                        const int cc = (unsigned)(gc[ax] - c[ax]) >= (unsigned)dn[ax] ? 0 : c[ax];
+                        s[ax] = p[ax] - cc;
+                        in = in && (unsigned)s[ax] < (unsigned)a.B[ax];
+                    }
+                    if (in) {
+                        const S* src = cl.map_shared_rank(slot + e * nthr + local_of(s), rank_of(s));
+                        v = ld_raw<S, R>(src);
+                    }
+                }
+                f[d] = v;
+            }
+        }
+        cell_update_for<S, true>(op, a.inv_tau, a.rho, a.vx, a.vy, a.vz, gi, f);
+    }
+
+    if (active && correct && (op & OP_STORE)) {
+        S* base = a.g.base[sel_dst];
+        const long long off = gi;
+        put27_raw<S>(f, cell_hash(static_cast<uint32_t>(gi), step_seed(step0 + static_cast<uint32_t>(a.k - 1))),
+                     [&](int d) { return base + d * a.g.stride + off; });
+    }
+    // no CTA leaves while another may still read its shared memory
+    if (a.k > 1) cl.sync();
+}
+
+}  // namespace culbm

@@ -6,16 +6,21 @@
 // Replaces the reference's haloBlocking*Run lambdas and initBlockingFlag /
 // initRingDDFBuf / mapGlobalMem2PersistL2
 // (src/simulator/single_dev_expt/simulator_expt_platform.cu:120-305, 608-942).
-// optPolicy 1 (static L2) and 2 (L1/L2 mixed) run on the same L2 tile engine
-// as 3 (dynamic L2): all three give the plain step's results bit for bit, so
-// they differ only in speed, and on this GPU the graph-replayed L2 engine is
-// the one kept.
+// optPolicy 1 (static L2) runs on the same L2 tile engine as 3 (dynamic L2).
+// optPolicy 2 (L1/L2 mixed) with pull streaming runs on the cluster engine
+// (cluster_kernels.cuh: one thread-block cluster per tile, populations in
+// registers, streaming through shared memory and DSMEM, one launch per
+// round) whenever the tile fits one cluster; larger tiles, and in-place
+// streaming, run on the L2 tile engine.  Every engine gives the plain step's
+// results bit for bit, so they differ only in speed.
 #include <algorithm>
+#include <climits>
 #include <cstring>
 #include <string>
 #include <vector>
 
 #include "sim_internal.cuh"
+#include "cluster_kernels.cuh"
 #include "tile_kernels.cuh"
 
 namespace culbm {
@@ -89,6 +94,12 @@ struct TileState {
     bool window = false;
     cudaAccessPolicyWindow apw{};
     size_t persist_bytes = 0;
+    // cluster engine (optPolicy 2, pull): CTA shape, CTAs per tile per axis
+    // (the cluster's shape) and dynamic shared memory per CTA
+    bool cluster = false;
+    int cta[3] = {0, 0, 0};
+    int cdim[3] = {0, 0, 0};
+    size_t cluster_smem = 0;
 };
 
 bool is_blocked(const culbm_config& cfg) { return cfg.opt_policy != CULBM_OPT_NONE; }
@@ -167,6 +178,46 @@ struct TileLauncher {
         return CULBM_OK;
     }
 
+    // Every tile of a round of k steps in one launch of the cluster engine.
+    template <bool HINT>
+    culbm_status cluster_round(int k)
+    {
+        ClusterTileArgs<S, R> a{};
+        a.dom = s->dom;
+        for (int q = 0; q < 3; ++q) {
+            a.B[q] = ts->B[q];
+            a.nt[q] = ts->nt[q];
+            a.cdim[q] = ts->cdim[q];
+        }
+        a.I = ts->I;
+        a.k = k;
+        a.ops = s->d_ops;
+        a.rho = s->d_mac[0];
+        a.vx = s->d_mac[1];
+        a.vy = s->d_mac[2];
+        a.vz = s->d_mac[3];
+        a.inv_tau = static_cast<R>(s->cfg.inv_tau);
+        a.g.base[0] = static_cast<S*>(s->d_pop[0]);
+        a.g.base[1] = static_cast<S*>(s->d_pop[1]);
+        a.g.stride = ts->gstride;
+        a.rs = ts->d_rs;
+        cudaLaunchConfig_t lc{};
+        lc.gridDim = dim3(ts->cdim[0] * ts->nt[0], ts->cdim[1] * ts->nt[1], ts->cdim[2] * ts->nt[2]);
+        lc.blockDim = dim3(ts->cta[0], ts->cta[1], ts->cta[2]);
+        lc.dynamicSmemBytes = ts->cluster_smem;
+        lc.stream = s->stream;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = ts->cdim[0];
+        attr[0].val.clusterDim.y = ts->cdim[1];
+        attr[0].val.clusterDim.z = ts->cdim[2];
+        lc.attrs = attr;
+        lc.numAttrs = 1;
+        CULBM_CUDA(cudaLaunchKernelEx(&lc, k_tile_cluster_pull<S, R, HINT>, a));
+        s->launches += 1;
+        return CULBM_OK;
+    }
+
     // All tiles for one round of k <= I steps, then the round-state advance.
     // Step j of a tile (0-based) covers the valid box grown by k - 1 - j.
     // With two lanes, lane 1 forks from and joins the simulation's stream
@@ -175,6 +226,13 @@ struct TileLauncher {
     {
         const bool hint = s->cfg.cache_hints != 0;
         const bool inplace = s->cfg.stream_policy == CULBM_STREAM_INPLACE;
+        if (ts->cluster) {
+            CULBM_TRY(hint ? cluster_round<true>(k) : cluster_round<false>(k));
+            k_tile_advance<<<1, 32, 0, s->stream>>>(ts->d_rs, ts->ring_nz, ts->ring_step, k);
+            CULBM_CUDA(cudaGetLastError());
+            s->launches += 1;
+            return CULBM_OK;
+        }
         const TileArgs<S, R> base = base_args();
         if (ts->lanes > 1) {
             CULBM_CUDA(cudaEventRecord(ts->ev_fork, s->stream));
@@ -322,6 +380,78 @@ __global__ void k_fill_dirs(S* base, long long stride, typename ArithOf<S>::type
         for (int d = 0; d < 27; ++d) Cvt<S, R>::st(base + d * stride + j, f[d]);
 }
 
+// CTA shape and cluster shape for the cluster engine: one thread per tile
+// cell, at most 1024 threads per CTA and kClusterMaxCtas CTAs per tile.
+// Preferred: portable clusters (at most 8 CTAs), then the fewest idle
+// threads, then the fewest CTAs.  False if no shape covers the tile.
+bool cluster_shape(const int B[3], int cta[3], int cdim[3])
+{
+    const long long cells = 1ll * B[0] * B[1] * B[2];
+    long long best = LLONG_MAX;
+    for (int tx = 32; tx <= 1024 && tx - 32 < B[0]; tx += 32)
+        for (int ty = 1; tx * ty <= 1024 && ty <= B[1]; ++ty)
+            for (int tz = 1; tx * ty * tz <= 1024 && tz <= B[2]; ++tz) {
+                const int n[3] = {(B[0] + tx - 1) / tx, (B[1] + ty - 1) / ty, (B[2] + tz - 1) / tz};
+                const long long ctas = 1ll * n[0] * n[1] * n[2];
+                if (ctas > kClusterMaxCtas) continue;
+                const long long idle = ctas * tx * ty * tz - cells;
+                const long long key = (ctas > 8 ? (1ll << 40) : 0) + idle * 64 + ctas;
+                if (key < best) {
+                    best = key;
+                    cta[0] = tx;
+                    cta[1] = ty;
+                    cta[2] = tz;
+                    for (int q = 0; q < 3; ++q) cdim[q] = n[q];
+                }
+            }
+    return best != LLONG_MAX;
+}
+
+// Selects the cluster engine for optPolicy 2 with pull streaming when the
+// tile fits one cluster and the GPU can hold such a cluster; otherwise the
+// tile engine stays in charge (ts->cluster false).
+template <typename S>
+culbm_status cluster_plan(culbm_sim* s, TileState* ts)
+{
+    using R = typename ArithOf<S>::type;
+    int cta[3], cdim[3];
+    if (!cluster_shape(ts->B, cta, cdim)) return CULBM_OK;
+    for (int q = 0; q < 3; ++q)
+        if (1ll * cdim[q] * ts->nt[q] > (q == 0 ? INT_MAX : 65535)) return CULBM_OK;
+    const int nthr = cta[0] * cta[1] * cta[2];
+    const int ctas = cdim[0] * cdim[1] * cdim[2];
+    const size_t smem = 2ull * 9 * nthr * sizeof(S);
+    void (*kernels[2])(ClusterTileArgs<S, R>) = {k_tile_cluster_pull<S, R, true>, k_tile_cluster_pull<S, R, false>};
+    for (auto kern : kernels) {
+        CULBM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+        if (ctas > 8) CULBM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    }
+    cudaLaunchConfig_t lc{};
+    lc.gridDim = dim3(cdim[0] * ts->nt[0], cdim[1] * ts->nt[1], cdim[2] * ts->nt[2]);
+    lc.blockDim = dim3(cta[0], cta[1], cta[2]);
+    lc.dynamicSmemBytes = smem;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = cdim[0];
+    attr[0].val.clusterDim.y = cdim[1];
+    attr[0].val.clusterDim.z = cdim[2];
+    lc.attrs = attr;
+    lc.numAttrs = 1;
+    int resident = 0;
+    if (cudaOccupancyMaxActiveClusters(&resident, kernels[0], &lc) != cudaSuccess) {
+        (void)cudaGetLastError();   // not a sticky error: this shape just cannot run
+        return CULBM_OK;
+    }
+    if (resident < 1) return CULBM_OK;
+    ts->cluster = true;
+    for (int q = 0; q < 3; ++q) {
+        ts->cta[q] = cta[q];
+        ts->cdim[q] = cdim[q];
+    }
+    ts->cluster_smem = smem;
+    return CULBM_OK;
+}
+
 }  // namespace
 
 // One axis of a blocked geometry: tile extent b (blockDim*gridDim) over
@@ -376,6 +506,17 @@ culbm_status tiles_create(culbm_sim* s)
             }
     ts->tile_n = 1ll * ts->B[0] * ts->B[1] * ts->B[2];
     const bool inplace = c.stream_policy == CULBM_STREAM_INPLACE;
+    if (!inplace && c.opt_policy == CULBM_OPT_L1L2) {
+        CULBM_TRY(with_storage(s, [&](auto tag) { return cluster_plan<typename decltype(tag)::type>(s, ts); }));
+        if (ts->cluster) {
+            // no tile buffers: the tile lives in registers and shared memory
+            void* p = nullptr;
+            CULBM_TRY(dev_alloc(s, &p, sizeof(RoundState), "round state"));
+            ts->d_rs = static_cast<RoundState*>(p);
+            ts->gstride = s->n;
+            return CULBM_OK;
+        }
+    }
     ts->lane_bytes = ((inplace ? 1 : 2) * 27ull * ts->tile_n * s->esize + 255) / 256 * 256;
     {
         int l2 = 0;
