@@ -9,7 +9,8 @@
 // L1L2StreamCore.cuh:45-690) runs one tile per cooperative launch over the
 // whole GPU: registers per cell, shared memory inside a CTA, warp shuffles
 // for +-x, an L2 swap buffer for CTA faces and a grid-wide barrier per step.
-// Here a tile is small enough for one cluster (at most 16 CTAs), so:
+// Here a tile is small enough for one cluster (at most 16 CTAs of 512
+// threads, one thread per cell), so:
 //   * the CTA-face exchange goes through DSMEM instead of an L2 buffer, and
 //     the per-step barrier is the cluster's hardware barrier instead of a
 //     grid-wide one (no spin-wait of our own);
@@ -32,6 +33,13 @@ namespace cg = cooperative_groups;
 
 // Most CTAs in one cluster (B200 allows 16 with the non-portable attribute).
 constexpr int kClusterMaxCtas = 16;
+// Most threads (cells) per CTA.  The kernel needs 128 registers per thread
+// to keep 27 populations, the exchange and the cell update free of spills;
+// capped at 64 (1024-thread CTAs) it spilled about 200 bytes per thread, and
+// the spill stores went out to L2 and stalled every cluster barrier's release
+// fence (ncu: 22.8M local store sectors per launch, membar and barrier the
+// top stall reasons, 6.8k MLUPS).
+constexpr int kClusterMaxThreads = 512;
 
 template <typename S, typename R>
 struct ClusterTileArgs {
@@ -61,11 +69,14 @@ __device__ __forceinline__ int cluster_valid_start(int idx, int blk, int num, in
 }
 
 // The round's k steps over one tile per cluster.  Shared memory: two slots
-// of 9 directions x (threads of the CTA) populations in storage format S;
-// groups of 9 directions alternate between the slots, so a slot is rewritten
-// only after the barrier that follows every read of its previous contents.
+// of 27 directions x (threads of the CTA) populations in storage format S,
+// one per exchange, alternating; one cluster barrier per exchange.  A slot is
+// rewritten two exchanges later, after the barrier of the exchange between,
+// which every thread of the cluster reaches only once it has read the slot.
+// (Three barriers per exchange, over groups of 9 directions in smaller
+// slots, measured slower.)
 template <typename S, typename R, bool HINT>
-__global__ void __launch_bounds__(1024, 1) k_tile_cluster_pull(const __grid_constant__ ClusterTileArgs<S, R> a)
+__global__ void __launch_bounds__(kClusterMaxThreads, 1) k_tile_cluster_pull(const __grid_constant__ ClusterTileArgs<S, R> a)
 {
     extern __shared__ __align__(16) unsigned char cluster_smem[];
     S* slots = reinterpret_cast<S*>(cluster_smem);
@@ -115,50 +126,60 @@ __global__ void __launch_bounds__(1024, 1) k_tile_cluster_pull(const __grid_cons
     }
     cell_update_for<S, true>(op, a.inv_tau, a.rho, a.vx, a.vy, a.vz, gi, f);
 
-    // CTA of the cluster (linear rank, x fastest) and cell inside it that
-    // hold tile cell s, for the exchange
-    auto rank_of = [&](const int* s) {
-        return (s[0] / bdim[0]) + a.cdim[0] * ((s[1] / bdim[1]) + a.cdim[1] * (s[2] / bdim[2]));
-    };
-    auto local_of = [&](const int* s) {
-        return (s[0] % bdim[0]) + bdim[0] * ((s[1] % bdim[1]) + bdim[1] * (s[2] % bdim[2]));
-    };
-
-    int group = 0;   // running count of exchanged groups (selects the slot)
+    // Where the pull of this cell reads, per axis, for the source offsets
+    // c = +1 and -1 (source p - c, or p where the domain clamp applies): the
+    // step of the source's CTA rank and of its cell index inside that CTA,
+    // relative to this cell and packed as (rank step << 16) + index step, and
+    // whether the source lies in the tile.  A direction's source is this
+    // cell's packed (rank, index) plus the sum over its axes; rank steps and
+    // index steps may be negative, the resulting index lies in [0, 512).
+    const int me = static_cast<int>(cl.block_rank());
+    int dl[3][2];           // [axis][c == -1]
+    unsigned inmask = 0;    // bit 3*axis + (1 - c): the source lies in the tile
+    {
+        const int rstride[3] = {1, a.cdim[0], a.cdim[0] * a.cdim[1]};
+        const int lstride[3] = {1, bdim[0], bdim[0] * bdim[1]};
+#pragma unroll
+        for (int ax = 0; ax < 3; ++ax) {
+            inmask |= 1u << (3 * ax + 1);
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+                int c = j == 0 ? 1 : -1;
+                if ((unsigned)(gc[ax] - c) >= (unsigned)dn[ax]) c = 0;   // domain clamp
+                const int t = tidx[ax] - c;
+                const int step = t < 0 ? -1 : (t >= bdim[ax] ? 1 : 0);
+                dl[ax][j] = step * rstride[ax] * 65536 + (step * -bdim[ax] - c) * lstride[ax];
+                if ((unsigned)(p[ax] - c) < (unsigned)a.B[ax]) inmask |= 1u << (3 * ax + (j == 0 ? 0 : 2));
+            }
+        }
+    }
+    const int own = me * 65536 + lt;
     for (int m = 1; m < a.k; ++m) {
         // post-collision populations of step m - 1 in storage format S
         // (the same rounding as a stored step, stochastic bits included)
         S q[27];
         put27_raw<S>(f, cell_hash(static_cast<uint32_t>(gi), step_seed(step0 + static_cast<uint32_t>(m - 1))),
                      [&](int d) { return &q[d]; });
+        S* slot = slots + (m & 1) * 27 * nthr;
 #pragma unroll
-        for (int grp = 0; grp < 3; ++grp, ++group) {
-            S* slot = slots + (group & 1) * 9 * nthr;
+        for (int d = 0; d < 27; ++d) slot[d * nthr + lt] = q[d];
+        cl.sync();   // barrier.cluster arrive (release) + wait (acquire)
 #pragma unroll
-            for (int e = 0; e < 9; ++e) slot[e * nthr + lt] = q[grp * 9 + e];
-            cl.sync();   // barrier.cluster arrive (release) + wait (acquire)
-#pragma unroll
-            for (int e = 0; e < 9; ++e) {
-                const int d = grp * 9 + e;
-                R v = R(0);
-                if (op & OP_LOAD) {
-                    const int c[3] = {cx_of(d), cy_of(d), cz_of(d)};
-                    int s[3];
-                    bool in = true;
-#pragma unroll
-                    for (int ax = 0; ax < 3; ++ax) {
-                        // domain clamp per axis, then the tile bound (halo: 0)
-                        const int cc = (unsigned)(gc[ax] - c[ax]) >= (unsigned)dn[ax] ? 0 : c[ax];
-                        s[ax] = p[ax] - cc;
-                        in = in && (unsigned)s[ax] < (unsigned)a.B[ax];
-                    }
-                    if (in) {
-                        const S* src = cl.map_shared_rank(slot + e * nthr + local_of(s), rank_of(s));
-                        v = ld_raw<S, R>(src);
-                    }
-                }
-                f[d] = v;
+        for (int d = 0; d < 27; ++d) {
+            const int jx = 1 - cx_of(d), jy = 1 - cy_of(d), jz = 1 - cz_of(d);
+            const unsigned need = (1u << jx) | (1u << (3 + jy)) | (1u << (6 + jz));
+            R v = R(0);
+            if ((op & OP_LOAD) && (inmask & need) == need) {
+                int packed = own;
+                if (jx != 1) packed += dl[0][jx >> 1];
+                if (jy != 1) packed += dl[1][jy >> 1];
+                if (jz != 1) packed += dl[2][jz >> 1];
+                const int r = packed >> 16;
+                // own CTA: plain shared-memory load; another CTA: DSMEM
+                const S* src = slot + d * nthr + (packed & 0xFFFF);
+                v = r == me ? ld_raw<S, R>(src) : ld_raw<S, R>(cl.map_shared_rank(src, r));
             }
+            f[d] = v;
         }
         cell_update_for<S, true>(op, a.inv_tau, a.rho, a.vx, a.vy, a.vz, gi, f);
     }

@@ -381,16 +381,20 @@ __global__ void k_fill_dirs(S* base, long long stride, typename ArithOf<S>::type
 }
 
 // CTA shape and cluster shape for the cluster engine: one thread per tile
-// cell, at most 1024 threads per CTA and kClusterMaxCtas CTAs per tile.
+// cell, at most kClusterMaxThreads threads per CTA and kClusterMaxCtas CTAs
+// per tile; CTA widths are multiples of 32 or the tile's own width.
 // Preferred: portable clusters (at most 8 CTAs), then the fewest idle
 // threads, then the fewest CTAs.  False if no shape covers the tile.
 bool cluster_shape(const int B[3], int cta[3], int cdim[3])
 {
     const long long cells = 1ll * B[0] * B[1] * B[2];
     long long best = LLONG_MAX;
-    for (int tx = 32; tx <= 1024 && tx - 32 < B[0]; tx += 32)
-        for (int ty = 1; tx * ty <= 1024 && ty <= B[1]; ++ty)
-            for (int tz = 1; tx * ty * tz <= 1024 && tz <= B[2]; ++tz) {
+    std::vector<int> widths;
+    for (int tx = 32; tx <= kClusterMaxThreads && tx - 32 < B[0]; tx += 32) widths.push_back(tx);
+    if (B[0] % 32 != 0 && B[0] <= kClusterMaxThreads) widths.push_back(B[0]);
+    for (const int tx : widths)
+        for (int ty = 1; tx * ty <= kClusterMaxThreads && ty <= B[1]; ++ty)
+            for (int tz = 1; tx * ty * tz <= kClusterMaxThreads && tz <= B[2]; ++tz) {
                 const int n[3] = {(B[0] + tx - 1) / tx, (B[1] + ty - 1) / ty, (B[2] + tz - 1) / tz};
                 const long long ctas = 1ll * n[0] * n[1] * n[2];
                 if (ctas > kClusterMaxCtas) continue;
@@ -414,13 +418,26 @@ template <typename S>
 culbm_status cluster_plan(culbm_sim* s, TileState* ts)
 {
     using R = typename ArithOf<S>::type;
+    // The reference's split when it fits (blockDim is the CTA, gridDim the
+    // tile's CTAs: HaloBlockingL1L2D3Q27PullKernel's launch,
+    // simulator_expt_platform.cu:608-650), else a shape of our own.
+    const culbm_config& c = s->cfg;
     int cta[3], cdim[3];
-    if (!cluster_shape(ts->B, cta, cdim)) return CULBM_OK;
+    const unsigned long long user_threads = 1ull * c.block_dim[0] * c.block_dim[1] * c.block_dim[2];
+    const unsigned long long user_ctas = 1ull * c.grid_dim[0] * c.grid_dim[1] * c.grid_dim[2];
+    if (user_threads >= 32 && user_threads <= kClusterMaxThreads && user_ctas <= kClusterMaxCtas) {
+        for (int q = 0; q < 3; ++q) {
+            cta[q] = static_cast<int>(c.block_dim[q]);
+            cdim[q] = static_cast<int>(c.grid_dim[q]);
+        }
+    } else if (!cluster_shape(ts->B, cta, cdim)) {
+        return CULBM_OK;
+    }
     for (int q = 0; q < 3; ++q)
         if (1ll * cdim[q] * ts->nt[q] > (q == 0 ? INT_MAX : 65535)) return CULBM_OK;
     const int nthr = cta[0] * cta[1] * cta[2];
     const int ctas = cdim[0] * cdim[1] * cdim[2];
-    const size_t smem = 2ull * 9 * nthr * sizeof(S);
+    const size_t smem = 2ull * 27 * nthr * sizeof(S);
     void (*kernels[2])(ClusterTileArgs<S, R>) = {k_tile_cluster_pull<S, R, true>, k_tile_cluster_pull<S, R, false>};
     for (auto kern : kernels) {
         CULBM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));

@@ -17,8 +17,24 @@ from test_gpu_blocked import _valid_axis, bits, oracle_pulled, run_blocked
 
 pytestmark = pytest.mark.gpu
 
-# Most cells a tile may hold for the cluster engine: 16 CTAs of 1024 threads.
-CLUSTER_CELLS = 16 * 1024
+# The cluster engine's limits: 16 CTAs of at most 512 threads, one per cell.
+MAX_CTAS, MAX_THREADS = 16, 512
+
+
+def fits_cluster(tile):
+    """Whether the engine finds a CTA shape for `tile`: CTA widths that are
+    multiples of 32 or the tile's own width, at most MAX_THREADS threads per
+    CTA and MAX_CTAS CTAs."""
+    bx, by, bz = tile
+    widths = [t for t in range(32, MAX_THREADS + 1, 32) if t - 32 < bx]
+    if bx % 32 and bx <= MAX_THREADS:
+        widths.append(bx)
+    for tx in widths:
+        for ty in range(1, min(by, MAX_THREADS // tx) + 1):
+            for tz in range(1, min(bz, MAX_THREADS // (tx * ty)) + 1):
+                if -(-bx // tx) * -(-by // ty) * -(-bz // tz) <= MAX_CTAS:
+                    return True
+    return False
 
 
 def rounds(nsteps, inner):
@@ -38,7 +54,7 @@ def test_cluster_random_geometries(culbm, orc, seed):
         dims = tuple(int(v) for v in rng.integers(14, 45, size=3))
         inner = int(rng.integers(2, 6))
         tile = tuple(int(rng.integers(max(2 * inner, 6), max(2 * inner + 1, d // 2 + 3))) for d in dims)
-        if all(_valid_axis(d, b, inner) for d, b in zip(dims, tile)) and np.prod(tile) <= CLUSTER_CELLS:
+        if all(_valid_axis(d, b, inner) for d, b in zip(dims, tile)) and fits_cluster(tile):
             break
     sc = S.reference_channel_cube(*dims, 0.05)
     nsteps = 2 * inner + int(rng.integers(1, inner + 1))
@@ -94,11 +110,14 @@ def test_cluster_without_cache_hints(culbm, orc):
 
 
 def test_cluster_user_grid_and_large_tile(culbm, orc):
-    """The tile is blockDim * gridDim whatever the split; a tile above one
-    cluster's 16 * 1024 cells runs on the L2 tile engine, with the same bits."""
+    """The tile is blockDim * gridDim whatever the split.  The reference's
+    split is kept when it fits a cluster (blockDim at most 512 threads,
+    gridDim at most 16 CTAs), else the engine picks its own; a tile no
+    cluster holds runs on the L2 tile engine, with the same bits."""
     sc = S.reference_channel_cube(70, 44, 30, 0.05)
     want = oracle_pulled(orc, sc, 0.6, 7)
-    for block, grid, cluster in (((16, 4, 2), (2, 5, 9), True), ((32, 8, 2), (2, 5, 15), False)):
+    for block, grid, cluster in (((32, 4, 4), (1, 4, 4), True), ((16, 4, 2), (2, 4, 4), True),
+                                 ((32, 8, 2), (2, 5, 15), False)):
         with culbm.Simulation(sc.shape, stream_policy=0, opt_policy=2, inv_tau=0.6, inner_loop=3, block_dim=block,
                               grid_dim=grid) as sim:
             sim.load_state(*sc.arrays())
@@ -107,7 +126,7 @@ def test_cluster_user_grid_and_large_tile(culbm, orc):
             info = sim.info()
         assert np.array_equal(bits(got), bits(want)), (block, grid)
         tile = tuple(b * g for b, g in zip(block, grid))
-        assert (np.prod(tile) <= CLUSTER_CELLS) == cluster
+        assert fits_cluster(tile) == cluster
         if cluster:
             assert_cluster_engine(info, 7, 3)
         else:
