@@ -190,10 +190,15 @@ def traffic_from_profiles(kernel_key):
 
 # ------------------------------------------------------------------- ours ---
 
-def measure(culbm, scene, sp, op, storage, steps, warmup, tile=None, inner=5, ring=False, clocks=None):
+def measure(culbm, scene, sp, op, storage, steps, warmup, tile=None, inner=5, ring=False, clocks=None, split=None):
+    """MLUPS of one policy.  `tile` is the tile extent (blockDim = tile,
+    gridDim = 1); `split` = (blockDim, gridDim) gives the tile as the
+    reference's launch split instead (for optPolicy 2 the CTA and cluster shape)."""
     arrs = scene.arrays()
     kw = {"dev_id": int(os.environ.get("LOCAL_RANK", "0"))}
-    if op:
+    if op and split is not None:
+        kw.update(block_dim=split[0], grid_dim=split[1], inner_loop=inner, use_ring=ring)
+    elif op:
         kw.update(tile=tile, inner_loop=inner, use_ring=ring)
     with culbm.Simulation(scene.shape, stream_policy=sp, opt_policy=op, storage=storage, inv_tau=0.5, **kw) as sim:
         sim.load_state(*arrs)
@@ -557,13 +562,21 @@ def run_ours(args):
         # (0,3): pull L2 tiles, the same two tiles
         "blocked_pull_fp32_readme_tile": (0, 3, "fp32", (64, 96, 76), 5),
         "blocked_pull_fp32_selected_tile": (0, 3, "fp32", tuple(sel["tile"]), sel["inner_loop"]),
+        # (0,2): the cluster engine, tile 32x8x16 as 16 CTAs of 32x4x2 cells
+        "blocked_pull_fp32_l1l2_cluster": (0, 2, "fp32", ((32, 4, 2), (1, 2, 8)), 2),
     }.items():
         try:
-            mlups, mps, inf = measure(culbm_b200, sc, sp, op, st, k2, 3, tile=tile, inner=inner, clocks=clocks)
+            split = tile if op == 2 else None
+            mlups, mps, inf = measure(culbm_b200, sc, sp, op, st, k2, 3, tile=None if split else tile, inner=inner,
+                                      clocks=clocks, split=split)
+            if split:
+                tile = tuple(b * g for b, g in zip(*split))
             extra[name] = {"mlups": round(mlups, 1), "ms_per_step": round(mps, 4),
                            "hbm_frac_of_measured": round(mlups * 1e6 * BYTES_PER_LUP[st] / 1e9 / peak, 4),
                            "policy": f"streamPolicy {sp}, optPolicy {op}" +
-                                     (f", tile {tile}, innerLoop {inner}" if op else ""),
+                                     (f", tile {tile}, innerLoop {inner}" if op else "") +
+                                     (f", CTA {split[0]} x cluster {split[1]}" if split else ""),
+                           "launches_per_step": inf.get("launches_per_step"),
                            "clocks": inf.get("clocks")}
         except Exception as e:   # report, do not hide
             extra[name] = {"error": str(e)}

@@ -45,7 +45,12 @@ typedef enum culbm_status {
 /* --streamPolicy, simulator_expt_platform.cu:37-41 */
 typedef enum culbm_stream_policy { CULBM_STREAM_PULL = 0, CULBM_STREAM_INPLACE = 1 } culbm_stream_policy;
 
-/* --optPolicy, simulator_expt_platform.cu:43-49 */
+/* --optPolicy, simulator_expt_platform.cu:43-49.  Every policy gives the
+ * plain step's results bit for bit.  CULBM_OPT_L1L2 with pull streaming runs
+ * each tile (blockDim*gridDim) as one thread-block cluster (blockDim as the
+ * CTA and gridDim as the cluster's CTAs when they fit: at most 512 threads,
+ * 16 CTAs); tiles no cluster holds, in-place streaming and the other blocked
+ * policies run on the L2 tile engine. */
 typedef enum culbm_opt_policy {
     CULBM_OPT_NONE = 0,
     CULBM_OPT_STATIC_L2 = 1,
