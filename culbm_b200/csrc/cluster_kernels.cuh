@@ -24,6 +24,7 @@
 #pragma once
 
 #include <cooperative_groups.h>
+#include <cstring>
 
 #include "tile_kernels.cuh"
 
@@ -58,6 +59,25 @@ struct ClusterTileArgs {
     GlobalPops<S> g;   // double-buffered global state (no ring buffer)
     const RoundState* rs;
 };
+
+// Warp shuffle of a stored population (any storage format) from the lane
+// `delta` below (UP) or above this one.
+template <bool UP, typename S>
+__device__ __forceinline__ S shfl_pop(S v, int delta)
+{
+    if constexpr (sizeof(S) == 2) {
+        unsigned short b;
+        memcpy(&b, &v, 2);
+        unsigned w = b;
+        w = UP ? __shfl_up_sync(0xFFFFFFFFu, w, delta) : __shfl_down_sync(0xFFFFFFFFu, w, delta);
+        b = static_cast<unsigned short>(w);
+        S r;
+        memcpy(&r, &b, 2);
+        return r;
+    } else {
+        return UP ? __shfl_up_sync(0xFFFFFFFFu, v, delta) : __shfl_down_sync(0xFFFFFFFFu, v, delta);
+    }
+}
 
 // First valid index of tile `idx` along one axis: calcValidPrev
 // (blocking_alogrithm.hpp:34-41), as valid_prev in tile_runtime.cu.
@@ -154,12 +174,29 @@ __global__ void __launch_bounds__(kClusterMaxThreads, 1) k_tile_cluster_pull(con
         }
     }
     const int own = me * 65536 + lt;
+    // warp shuffles for d = 14 / 12: a warp is one row of the CTA, and the
+    // source (x - 1 / x + 1, unclamped) is in the same warp
+    const bool row_warp = bdim[0] == 32;
+    const bool xlo_shfl = tidx[0] > 0 && gc[0] > 0;
+    const bool xhi_shfl = tidx[0] < 31 && gc[0] < D.nx - 1;
     for (int m = 1; m < a.k; ++m) {
         // post-collision populations of step m - 1 in storage format S
         // (the same rounding as a stored step, stochastic bits included)
         S q[27];
         put27_raw<S>(f, cell_hash(static_cast<uint32_t>(gi), step_seed(step0 + static_cast<uint32_t>(m - 1))),
                      [&](int d) { return &q[d]; });
+        // The pure +-x directions (d = 14: source x - 1; d = 12: source x + 1)
+        // come from the neighbouring lane by a warp shuffle where a warp is
+        // one 32-cell row of the CTA and the source lane lies in the warp (the
+        // reference's L1/L2 kernel shuffles the same two directions); their
+        // edge lanes and clamped cells read shared memory like the rest.  The
+        // shuffle runs only where every warp is a full row (a CTA-uniform
+        // test), so no partial warp executes the full-mask shuffle.
+        S from_lo = q[14], from_hi = q[12];
+        if (row_warp) {
+            from_lo = shfl_pop<true>(q[14], 1);
+            from_hi = shfl_pop<false>(q[12], 1);
+        }
         S* slot = slots + (m & 1) * 27 * nthr;
 #pragma unroll
         for (int d = 0; d < 27; ++d) slot[d * nthr + lt] = q[d];
@@ -169,7 +206,11 @@ __global__ void __launch_bounds__(kClusterMaxThreads, 1) k_tile_cluster_pull(con
             const int jx = 1 - cx_of(d), jy = 1 - cy_of(d), jz = 1 - cz_of(d);
             const unsigned need = (1u << jx) | (1u << (3 + jy)) | (1u << (6 + jz));
             R v = R(0);
-            if ((op & OP_LOAD) && (inmask & need) == need) {
+            if ((d == 12 || d == 14) && row_warp && (op & OP_LOAD) && (inmask & need) == need &&
+                (d == 14 ? xlo_shfl : xhi_shfl)) {
+                const S w = d == 14 ? from_lo : from_hi;
+                v = ld_raw<S, R>(&w);
+            } else if ((op & OP_LOAD) && (inmask & need) == need) {
                 int packed = own;
                 if (jx != 1) packed += dl[0][jx >> 1];
                 if (jy != 1) packed += dl[1][jy >> 1];
